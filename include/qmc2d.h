@@ -1,0 +1,239 @@
+/*
+ * qmc2d.h - C-ABI of the B200 walker-propagation library for the 2D
+ * electron-gas QMC code 2degas (Slater-Jastrow-backflow VMC/DMC/RQMC).
+ *
+ * The reference has no formal plugin API: its hot path is a set of Fortran
+ * subroutines without arguments that talk through COMMON blocks (ewald.h).
+ * Every entry point below replaces one of those subroutines (or a loop of
+ * them) and takes the COMMON-block arrays as plain pointers, in the same
+ * Fortran column-major layout, so that a Fortran iso_c_binding shim can pass
+ * x_new(mdim,mnp), g_new(mdim,mnp), h_new(mtypes), p_new(m_props) directly.
+ *
+ * Conventions
+ *   - Positions/drifts are x(2,N): interleaved (x,y) per electron, electrons
+ *     ordered type by type (all "up" then all "down"), as ewald.h's x_new.
+ *   - Property vectors follow the reference's p_new index map (input,
+ *     reptation.f:577-637), 0-based here: see QMC2D_J* below.
+ *   - All pointers are HOST pointers unless the name ends in _dev.
+ *   - Every call returns an int status (QMC2D_OK == 0); nothing throws
+ *     across the ABI. Device-side failures (singular Slater matrix,
+ *     non-finite energy) are reported through status words read after
+ *     each launch.
+ *   - One handle per host thread; each handle owns one CUDA stream.
+ */
+#ifndef QMC2D_H
+#define QMC2D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum qmc2d_status {
+  QMC2D_OK = 0,
+  QMC2D_ERR_ARG = 1,          /* bad argument / size */
+  QMC2D_ERR_IO = 2,           /* input file missing or unreadable */
+  QMC2D_ERR_PARSE = 3,        /* malformed keyword record or table */
+  QMC2D_ERR_UNSUPPORTED = 4,  /* keyword/feature outside the walker path */
+  QMC2D_ERR_CUDA = 5,         /* CUDA runtime error (message in qmc2d_last_error) */
+  QMC2D_ERR_NOMEM = 6,        /* device or host allocation failed */
+  QMC2D_ERR_SINGULAR = 7,     /* zero pivot in a Slater matrix
+                                 (reference: stop 'slater_bckflw_orbitals', reptation.f:10318) */
+  QMC2D_ERR_NONFINITE = 8,    /* NaN/Inf local energy or weight */
+  QMC2D_ERR_POPULATION = 9,   /* population outside the handle's capacity */
+  QMC2D_ERR_LIMIT = 10,       /* size beyond a compiled limit */
+  QMC2D_ERR_STACK = 11        /* walker stack empty/full (reptation.f:2374, 2416) */
+};
+
+/* Compiled limits. The reference's ewald.h limits (mnp=166, morbit=42,
+ * mgrid=901, mnk=196) are dropped where the device code does not need them. */
+#define QMC2D_MAX_TYPES 2
+#define QMC2D_MAX_TABLES 16
+#define QMC2D_MAX_NP 162          /* electrons per walker */
+#define QMC2D_MAX_ORB 81          /* orbitals (electrons) per spin determinant */
+#define QMC2D_MAX_NK 512          /* half-space k vectors */
+#define QMC2D_NAME_LEN 64
+
+/* ------------------------------------------------------- property layout
+ * Scalar properties, reference names and 1-based indices from
+ * reptation.f:577-628 (jetot=1, jltf=2, jacc=3, jpot(0)=4, jkin(0)=5, je2=6,
+ * jgg=7, then pot_<t>, kin_<t>, un_<t> per type, then efp), followed by
+ * rhok (2*nk doubles per type that has 'rhok'). Here 0-based. */
+#define QMC2D_JETOT 0
+#define QMC2D_JLTF 1
+#define QMC2D_JACC 2
+#define QMC2D_JPOT0 3
+#define QMC2D_JKIN0 4
+#define QMC2D_JE2 5
+#define QMC2D_JGG 6
+#define QMC2D_JPOT(nt, it) (7 + (it))
+#define QMC2D_JKIN(nt, it) (7 + (nt) + (it))
+#define QMC2D_JUN(nt, it) (7 + 2 * (nt) + (it))
+#define QMC2D_JEFP(nt) (7 + 3 * (nt))
+#define QMC2D_NSCALAR(nt) (8 + 3 * (nt))
+
+/* ------------------------------------------------------------- the system
+ * What the reference's `input` (reptation.f:12-710) leaves in COMMON for the
+ * walker path: particle types, box, k vectors, orbital wave vectors, spline
+ * tables and option flags. Filled by qmc2d_system_read() or by the caller. */
+typedef struct qmc2d_table {
+  char name[QMC2D_NAME_LEN];
+  int ngrid;        /* knots 0..ngrid (t_read, reptation.f:4701-4704) */
+  double *ut;       /* (ngrid+1)*4: ut[4*i+c] == ut(i,c+1,table) */
+  double tail;      /* v2 tail constant (reptation.f:250) */
+  int iexp;         /* getf_0 multiplies by (1/r)**iexp (reptation.f:4110) */
+  int nk_ewald;     /* number of k-space v_k after the knots, 0 if none */
+  double *vk;       /* nk_ewald+1: v_k (k=1..nk_ewald) then v_k0 (reptation.f:4714-4720) */
+} qmc2d_table;
+
+typedef struct qmc2d_system {
+  int ndim;                                /* must be 2 */
+  int ntypes;                              /* 1 or 2 */
+  char type_name[QMC2D_MAX_TYPES][QMC2D_NAME_LEN];
+  char x_file[QMC2D_MAX_TYPES][QMC2D_NAME_LEN];
+  int np[QMC2D_MAX_TYPES];                 /* particles per type */
+  int ipfrst[QMC2D_MAX_TYPES];             /* 0-based first particle of the type */
+  int nptot;
+  int npnorm;                              /* moving particles (hbs2m != 0) */
+  double hbs2m[QMC2D_MAX_TYPES];           /* hbar^2/2m per type */
+  double el[2], eli[2];                    /* box sides and inverses ('pbc') */
+  int nk;                                  /* k vectors read by kread */
+  double *kvec;                            /* 2*nk */
+  int ngvec;                               /* 2*nk+1 orbital wave vectors */
+  double *gvec;                            /* 2*ngvec, in the order the determinant uses */
+  double drt, drti, drti2;                 /* knot spacing (shared by all tables) */
+  int ntables;
+  qmc2d_table tables[QMC2D_MAX_TABLES];
+  int iu2[QMC2D_MAX_TYPES][QMC2D_MAX_TYPES];   /* table index, -1 if none */
+  int iu3[QMC2D_MAX_TYPES][QMC2D_MAX_TYPES];
+  int iub[QMC2D_MAX_TYPES][QMC2D_MAX_TYPES];   /* backflow eta tables */
+  int iv2[QMC2D_MAX_TYPES][QMC2D_MAX_TYPES];   /* pair potential tables */
+  int irhok[QMC2D_MAX_TYPES];              /* 1-based rhok slot, 0 if not requested */
+  int nrhok;
+  double v0;                               /* constant potential (Madelung) */
+  double adrift;                           /* drift cutoff parameter */
+  double delta;                            /* time step of the current run (COMMON /c_sim/);
+                                              kinetic's adrift cutoff reads it */
+  int ecut;                                /* cut E_L in the RQMC action (fgg) */
+  double value_ecut;
+  int ntheta;                              /* twists per direction; efp added when != 0 */
+  int ith, jth;                            /* current twist (1-based), 0 at Gamma */
+  int ibckf;
+  int gstorto, wpiu, nodalaction, rejection;
+  int seed[4];                             /* 'seed' file / keyword */
+  int n_scalar_props;
+  int n_props;                             /* scalars + rhok */
+  int jrhok;                               /* first rhok index (0-based) */
+  int ref_underflow_return;                /* 1: keep the reference's early return when
+                                              exp(-2*(-ln psi)) underflows (reptation.f:10087) */
+} qmc2d_system;
+
+/* Read <dir>/<runid>.sy and every table it names (input, t_read, kread:
+ * reptation.f:12-710, 4689-4769). The orbital wave vectors are built at the
+ * Gamma point (reptation.f:674-708) or, when 'ntwists' is present, for twist
+ * (1,1) (tabc, reptation.f:9559). Unsupported keywords give
+ * QMC2D_ERR_UNSUPPORTED with the keyword in qmc2d_last_error(). */
+int qmc2d_system_read(const char *dir, const char *runid, qmc2d_system **out);
+void qmc2d_system_free(qmc2d_system *sys);
+
+/* Rebuild gvec for twist (ith, jth) of an ntheta x ntheta grid: +-k + theta,
+ * sorted by |g|^2 with the reference's heapsort (twistg, reptation.f:9818;
+ * SORTTF, reptation.f:9514). ith = jth = 0 restores the Gamma-point list. */
+int qmc2d_system_set_twist(qmc2d_system *sys, int ith, int jth);
+
+/* Read `count` configurations of all types starting at configuration `first`
+ * (0-based) from the per-type files <dir>/<x_file><suffix> (read_conf,
+ * reptation.f:2452-2491). x receives count*2*nptot doubles. Returns the
+ * number of configurations read in *nread. */
+int qmc2d_read_configs(const qmc2d_system *sys, const char *dir, const char *suffix,
+                       int first, int count, double *x, int *nread);
+
+const char *qmc2d_last_error(void);
+const char *qmc2d_version(void);
+
+/* ------------------------------------------------------------ the handle */
+typedef struct qmc2d_handle qmc2d_handle;
+
+typedef struct qmc2d_options {
+  int capacity;          /* walkers (or reptile beads) the handle can hold */
+  int device;            /* CUDA device ordinal */
+  uint64_t seed;         /* Philox key for the device random streams */
+} qmc2d_options;
+
+/* Copy the system's tables to the device and allocate walker storage. */
+int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt, qmc2d_handle **out);
+int qmc2d_destroy(qmc2d_handle *h);
+
+/* compute_properties (reptation.f:2661): for nw configurations x (2*nptot
+ * each) compute g = -grad ln psi (2*nptot), hlap = -lap ln psi per type
+ * (ntypes), props (n_props) and the sign s. Host buffers, synchronous. */
+int qmc2d_compute_properties(qmc2d_handle *h, int nw, const double *x,
+                             double *g, double *hlap, double *props, double *s);
+
+/* Same on device-resident buffers, asynchronous on `stream` (a cudaStream_t,
+ * or NULL for the handle's stream). */
+int qmc2d_compute_properties_dev(qmc2d_handle *h, int nw, const double *x_dev,
+                                 double *g_dev, double *hlap_dev, double *props_dev,
+                                 double *s_dev, void *stream);
+
+/* ---------------------------------------------------------- populations
+ * A population is the reference's walker stack (x_stack, g_stack, h_stack,
+ * s_stack, age_stack, p_stack; ewald.h:166-173) held in HBM. */
+
+/* read_conf (reptation.f:2452): evaluate nw configurations and make them the
+ * population (x_old = x, g_old = g, p_old = props, age = 0, p_old(jacc)=1). */
+int qmc2d_population_set(qmc2d_handle *h, int nw, const double *x);
+int qmc2d_population_size(qmc2d_handle *h, int *nw);
+/* Copy the population out (any pointer may be NULL). */
+int qmc2d_population_get(qmc2d_handle *h, double *x, double *g, double *props,
+                         double *age);
+
+/* Block accumulators (averages(1/2), reptation.f:4283-4304): weighted sums
+ * of p_old over all walkers and steps since the last reset. */
+int qmc2d_block_reset(qmc2d_handle *h);
+int qmc2d_block_get(qmc2d_handle *h, double *blk_av /* n_props */, double *blk_norm);
+
+/* Counters of the last run: accepted moves, proposed moves, forced moves. */
+typedef struct qmc2d_counters {
+  double accepted, proposed, forced, sign_changes;
+  double max_weight_capped;   /* branch2 wmult caps (reptation.f:2175) */
+} qmc2d_counters;
+int qmc2d_counters_get(qmc2d_handle *h, qmc2d_counters *c);
+
+/* VMC: nstp steps of move + metropolis_test + averages(2) on every walker
+ * (vmc loop body, reptation.f:995-1003; move :4617; metropolis_test :2622).
+ * mage forces a move after that many consecutive rejections (<=0: never). */
+int qmc2d_vmc(qmc2d_handle *h, int nstp, double delta, int mage);
+
+/* DMC: nstp generations; each walker makes mmstep moves, its weight is
+ * multiplied by min(mmult, exp(-npnorm*(E_L-etrial)*delta)) after each, and
+ * the population is resampled with branch2's fixed-population comb
+ * (dmc, reptation.f:872-922; branch2 :2162-2273). */
+int qmc2d_dmc(qmc2d_handle *h, int nstp, int mmstep, double delta, double etrial,
+              double mmult, int mage);
+
+/* ------------------------------------------------------------- reptation */
+typedef struct qmc2d_rmc_params {
+  int ntau, ntauskip, mdelta;
+  double delta, etrial;
+  int mage, mage_r;
+} qmc2d_rmc_params;
+
+/* read_path (reptation.f:1775): set up one reptile per slot from
+ * nrep*ntau configurations (reptile-major, bead order). */
+int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params *prm,
+                   const double *x);
+/* nstp reptation moves (reptation_move + reptation_metropolis_test,
+ * reptation.f:1897-1895) on every reptile, accumulating p_old into the
+ * block sums. */
+int qmc2d_rmc(qmc2d_handle *h, int nstp);
+/* Copy reptile r's path (ntau beads, x then props) out. */
+int qmc2d_rmc_get_path(qmc2d_handle *h, int r, double *x, double *props);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QMC2D_H */
