@@ -1,0 +1,188 @@
+"""qmc2d-b200: the walker-propagation path of 2degas on B200 (sm_100a).
+
+Python view of the C-ABI in include/qmc2d.h. The heavy lifting is in
+lib/libqmc2d.so (CUDA kernels + C++ host); this module only marshals
+arrays. There is no CPU fallback: if the library or a GPU is missing, the
+calls raise.
+
+    import importlib
+    q = importlib.import_module("2degas_b200")
+    sys_ = q.System.read("tests/golden/n26", "n26")
+    with q.Handle(sys_, capacity=256, seed=1) as h:
+        g, hl, props, s = h.compute_properties(x)
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi
+
+__all__ = ["System", "Handle", "QMCError", "load_library", "_capi"]
+
+QMCError = _capi.QMCError
+
+
+def load_library():
+    return _capi.load()
+
+
+def _pd(a):
+    return a.ctypes.data_as(_capi.PD)
+
+
+class System:
+    """A qmc2d_system read from a reference run directory (input, t_read, kread)."""
+
+    def __init__(self, ptr, lib):
+        self.ptr = ptr
+        self.lib = lib
+
+    @classmethod
+    def read(cls, directory, runid):
+        lib = _capi.load()
+        sp = _capi.SYSP()
+        _capi.check(lib, lib.qmc2d_system_read(str(directory).encode(), runid.encode(),
+                                               ctypes.byref(sp)))
+        return cls(sp, lib)
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                self.lib.qmc2d_system_free(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+    @property
+    def s(self):
+        return self.ptr.contents
+
+    @property
+    def N(self):
+        return self.s.nptot
+
+    @property
+    def ntypes(self):
+        return self.s.ntypes
+
+    @property
+    def nprops(self):
+        return self.s.n_props
+
+    def set_twist(self, ith, jth):
+        _capi.check(self.lib, self.lib.qmc2d_system_set_twist(self.ptr, ith, jth))
+
+    def gvec(self):
+        s = self.s
+        return np.ctypeslib.as_array(s.gvec, shape=(2 * s.ngvec,)).reshape(-1, 2).copy()
+
+    def read_configs(self, directory, suffix, first, count):
+        x = np.zeros((count, 2 * self.N))
+        n = ctypes.c_int(0)
+        _capi.check(self.lib, self.lib.qmc2d_read_configs(self.ptr, str(directory).encode(),
+                                                          suffix.encode(), first, count, _pd(x),
+                                                          ctypes.byref(n)))
+        return x[: n.value]
+
+
+class Handle:
+    """Device-resident state for one system (qmc2d_create .. qmc2d_destroy)."""
+
+    def __init__(self, system, capacity, seed=1, device=0):
+        self.system = system
+        self.lib = system.lib
+        self.cap = capacity
+        self.h = ctypes.c_void_p()
+        opt = _capi.Options(capacity, device, seed)
+        _capi.check(self.lib, self.lib.qmc2d_create(system.ptr, ctypes.byref(opt),
+                                                    ctypes.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            self.lib.qmc2d_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, code):
+        return _capi.check(self.lib, code)
+
+    # compute_properties (reptation.f:2661)
+    def compute_properties(self, x):
+        x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float64)
+        nw, N, nt, np_ = x.shape[0], self.system.N, self.system.ntypes, self.system.nprops
+        g = np.zeros((nw, 2 * N))
+        hl = np.zeros((nw, nt))
+        p = np.zeros((nw, np_))
+        s = np.zeros(nw)
+        self._chk(self.lib.qmc2d_compute_properties(self.h, nw, _pd(x), _pd(g), _pd(hl), _pd(p),
+                                                    _pd(s)))
+        return g, hl, p, s
+
+    def compute_properties_dev(self, nw, x_ptr, g_ptr, h_ptr, p_ptr, s_ptr, stream=None):
+        self._chk(self.lib.qmc2d_compute_properties_dev(self.h, nw, x_ptr, g_ptr, h_ptr, p_ptr,
+                                                        s_ptr, stream))
+
+    def population_set(self, x):
+        x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float64)
+        self._chk(self.lib.qmc2d_population_set(self.h, x.shape[0], _pd(x)))
+
+    def population_size(self):
+        n = ctypes.c_int()
+        self._chk(self.lib.qmc2d_population_size(self.h, ctypes.byref(n)))
+        return n.value
+
+    def population_get(self):
+        nw, N, np_ = self.population_size(), self.system.N, self.system.nprops
+        x = np.zeros((nw, 2 * N))
+        g = np.zeros((nw, 2 * N))
+        p = np.zeros((nw, np_))
+        age = np.zeros(nw)
+        self._chk(self.lib.qmc2d_population_get(self.h, _pd(x), _pd(g), _pd(p), _pd(age)))
+        return dict(x=x, g=g, p=p, age=age)
+
+    def block_reset(self):
+        self._chk(self.lib.qmc2d_block_reset(self.h))
+
+    def block_get(self):
+        b = np.zeros(self.system.nprops)
+        n = ctypes.c_double()
+        self._chk(self.lib.qmc2d_block_get(self.h, _pd(b), ctypes.byref(n)))
+        return b, n.value
+
+    def counters(self):
+        c = _capi.Counters()
+        self._chk(self.lib.qmc2d_counters_get(self.h, ctypes.byref(c)))
+        return dict(accepted=c.accepted, proposed=c.proposed, forced=c.forced,
+                    capped=c.max_weight_capped)
+
+    def vmc(self, nstp, delta, mage):
+        self._chk(self.lib.qmc2d_vmc(self.h, nstp, delta, mage))
+
+    def dmc(self, nstp, mmstep, delta, etrial, mmult, mage):
+        self._chk(self.lib.qmc2d_dmc(self.h, nstp, mmstep, delta, etrial, mmult, mage))
+
+    def rmc_init(self, nrep, x, ntau, ntauskip, mdelta, delta, etrial, mage, mage_r):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        prm = _capi.RmcParams(ntau, ntauskip, mdelta, delta, etrial, mage, mage_r)
+        self._chk(self.lib.qmc2d_rmc_init(self.h, nrep, ctypes.byref(prm), _pd(x)))
+
+    def rmc(self, nstp):
+        self._chk(self.lib.qmc2d_rmc(self.h, nstp))
+
+    def rmc_get_path(self, rep, ntau):
+        N, np_ = self.system.N, self.system.nprops
+        x = np.zeros((ntau, 2 * N))
+        p = np.zeros((ntau, np_))
+        self._chk(self.lib.qmc2d_rmc_get_path(self.h, rep, _pd(x), _pd(p)))
+        return x, p

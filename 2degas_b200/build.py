@@ -1,0 +1,68 @@
+"""Build libqmc2d.so in-tree for sm_100a (B200).
+
+    python 2degas_b200/build.py [--verbose]
+
+Every CUDA and host source under csrc/ goes into one shared library,
+2degas_b200/lib/libqmc2d.so, exporting the C-ABI of include/qmc2d.h.
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "lib")
+OUT = os.path.join(LIBDIR, "libqmc2d.so")
+
+SOURCES = ["input.cpp", "system.cpp", "kernels.cu", "capi.cu", "rmc.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc():
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def newest_input():
+    paths = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
+    paths.append(os.path.join(os.path.dirname(HERE), "include", "qmc2d.h"))
+    paths.append(os.path.abspath(__file__))
+    return max(os.path.getmtime(p) for p in paths)
+
+
+def build(verbose=False, force=False):
+    if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= newest_input():
+        return OUT
+    os.makedirs(LIBDIR, exist_ok=True)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, src + ".o")
+        cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+               "-Xcompiler", "-fvisibility=hidden", "-rdc=false", "-c",
+               os.path.join(CSRC, src), "-o", obj]
+        if src.endswith(".cu"):
+            cmd[1:1] = ["-Xptxas", "-v"] if verbose else []
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if verbose or r.returncode:
+            sys.stdout.write(r.stdout)
+            sys.stderr.write(r.stderr)
+        if r.returncode:
+            raise RuntimeError(f"nvcc failed on {src}")
+        objs.append(obj)
+    cmd = [nvcc(), *ARCH, "-shared", "-o", OUT, *objs, "-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("link failed")
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(verbose="--verbose" in sys.argv, force="--force" in sys.argv))

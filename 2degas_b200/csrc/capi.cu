@@ -1,0 +1,433 @@
+// capi.cu - the C-ABI of include/qmc2d.h: handle lifetime, device copies of
+// the system, populations in HBM and the drivers that replace the
+// reference's compute_properties / vmc / dmc loops.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/qmc2d.h"
+#include "common.h"
+#include "devsys.h"
+#include "kernels.cuh"
+#include "rmc.cuh"
+#include "handle.h"
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char *what) {
+  q2d::set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return QMC2D_ERR_CUDA;
+}
+
+#define CK(call)                                      \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t n) {
+  return cudaMalloc((void **)p, sizeof(T) * (n > 0 ? n : 1));
+}
+
+int build_devsys(const qmc2d_system *sys, q2d::DevSys *hs, std::vector<double> *coef) {
+  q2d::DevSys s{};
+  s.N = sys->nptot;
+  s.nt = sys->ntypes;
+  s.npnorm = sys->npnorm;
+  s.nprops = sys->n_props;
+  s.nscalar = sys->n_scalar_props;
+  s.jrhok = sys->jrhok;
+  s.nk = sys->nk;
+  s.ngvec = sys->ngvec;
+  s.nrhok = sys->nrhok;
+  s.nmax = 0;
+  for (int t = 0; t < 2; t++) {
+    s.np[t] = t < sys->ntypes ? sys->np[t] : 0;
+    s.ipfrst[t] = t < sys->ntypes ? sys->ipfrst[t] : sys->nptot;
+    s.irhok[t] = t < sys->ntypes ? sys->irhok[t] : 0;
+    s.hbs2m[t] = t < sys->ntypes ? sys->hbs2m[t] : 0.0;
+    if (t < sys->ntypes) s.nmax = std::max(s.nmax, sys->np[t]);
+  }
+  for (int d = 0; d < 2; d++) {
+    s.el[d] = sys->el[d];
+    s.eli[d] = sys->eli[d];
+  }
+  s.drt = sys->drt;
+  s.drti = sys->drti;
+  s.drti2 = sys->drti2;
+  s.v0 = sys->v0;
+  s.adrift = sys->adrift;
+  s.delta = sys->delta;
+  s.ntheta = sys->ntheta;
+  s.ref_underflow = sys->ref_underflow_return;
+  s.ecut = sys->ecut;
+  s.value_ecut = sys->value_ecut;
+  s.rejection = sys->rejection;
+  s.wpiu = sys->wpiu;
+  s.gstorto = sys->gstorto;
+  s.nodalaction = sys->nodalaction;
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 2; b++) {
+      bool in = a < sys->ntypes && b < sys->ntypes;
+      s.iu2[a][b] = in ? sys->iu2[a][b] : -1;
+      s.iu3[a][b] = in ? sys->iu3[a][b] : -1;
+      s.iub[a][b] = in ? sys->iub[a][b] : -1;
+      s.iv2[a][b] = in ? sys->iv2[a][b] : -1;
+    }
+  s.has_u2 = s.iu2[0][0] >= 0;
+  s.has_u3 = s.iu3[0][0] >= 0;
+  s.has_bf = s.iub[0][0] >= 0;
+  s.has_v2 = s.iv2[0][0] >= 0;
+  coef->clear();
+  for (int t = 0; t < sys->ntables; t++) {
+    const qmc2d_table &tb = sys->tables[t];
+    while (coef->size() % 2) coef->push_back(0.0);  // 16-byte rows
+    s.tab_off[t] = (int)coef->size();
+    s.tab_ngrid[t] = tb.ngrid;
+    s.tab_iexp[t] = tb.iexp;
+    s.tab_tail[t] = tb.tail;
+    coef->insert(coef->end(), tb.ut, tb.ut + 4 * (size_t)(tb.ngrid + 1));
+    s.tab_nkew[t] = tb.nk_ewald;
+    s.tab_vkoff[t] = (int)coef->size();
+    if (tb.nk_ewald > 0) coef->insert(coef->end(), tb.vk, tb.vk + tb.nk_ewald + 1);
+  }
+  *hs = s;
+  return QMC2D_OK;
+}
+
+int alloc_pop(q2d::DevPop *p, int cap, int N, int nt, int np) {
+  CK(dalloc(&p->x, (size_t)cap * 2 * N));
+  CK(dalloc(&p->g, (size_t)cap * 2 * N));
+  CK(dalloc(&p->h, (size_t)cap * nt));
+  CK(dalloc(&p->p, (size_t)cap * np));
+  CK(dalloc(&p->s, (size_t)cap));
+  CK(dalloc(&p->age, (size_t)cap));
+  return QMC2D_OK;
+}
+
+void free_pop(q2d::DevPop *p) {
+  cudaFree(p->x);
+  cudaFree(p->g);
+  cudaFree(p->h);
+  cudaFree(p->p);
+  cudaFree(p->s);
+  cudaFree(p->age);
+  *p = q2d::DevPop{};
+}
+
+int sync_status(qmc2d_handle *h, int nw) {
+  CK(cudaStreamSynchronize(h->stream));
+  std::vector<int> st(nw > 0 ? nw : 1);
+  if (nw > 0) CK(cudaMemcpy(st.data(), h->d_status, sizeof(int) * nw, cudaMemcpyDeviceToHost));
+  int any = 0;
+  for (int i = 0; i < nw; i++) any |= st[i];
+  if (any & q2d::ST_SINGULAR) {
+    q2d::set_error("zero pivot in a Slater matrix");
+    return QMC2D_ERR_SINGULAR;
+  }
+  if (any & q2d::ST_NONFINITE) {
+    q2d::set_error("non-finite local energy or -ln psi");
+    return QMC2D_ERR_NONFINITE;
+  }
+  return QMC2D_OK;
+}
+
+}  // namespace
+
+int q2d_sync_status(qmc2d_handle *h, int n) { return sync_status(h, n); }
+
+extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
+                            qmc2d_handle **out) {
+  if (!sys || !opt || !out || opt->capacity <= 0) {
+    q2d::set_error("qmc2d_create: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  *out = nullptr;
+  if (sys->ndim != 2 || sys->ntypes < 1 || sys->ntypes > 2 || sys->nptot > QMC2D_MAX_NP) {
+    q2d::set_error("qmc2d_create: unsupported system size");
+    return QMC2D_ERR_LIMIT;
+  }
+  qmc2d_handle *h = new qmc2d_handle();
+  h->device = opt->device;
+  h->seed = opt->seed;
+  h->cap = opt->capacity;
+  std::vector<double> coef;
+  build_devsys(sys, &h->hs, &coef);
+  h->nt = sys->ntypes;
+  h->N = sys->nptot;
+  h->nprops = sys->n_props;
+  auto fail = [&](int code) {
+    qmc2d_destroy(h);
+    return code;
+  };
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return fail(cuda_fail(e, "cudaSetDevice"));
+  int smem_max = 0;
+  cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+  size_t need = std::max(q2d::move_smem_bytes(h->hs), q2d::eval_smem_bytes(h->hs));
+  if (need + sizeof(q2d::DevSys) > (size_t)smem_max) {
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "walker needs %zu bytes of shared memory, device has %d",
+                  need, smem_max);
+    q2d::set_error(buf);
+    return fail(QMC2D_ERR_LIMIT);
+  }
+  if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return fail(cuda_fail(e, "cudaStreamCreate"));
+  int st;
+  if ((e = dalloc(&h->d_coef, coef.size())) != cudaSuccess) return fail(cuda_fail(e, "alloc"));
+  if ((e = dalloc(&h->d_kvec, 2 * (size_t)std::max(1, sys->nk))) != cudaSuccess)
+    return fail(cuda_fail(e, "alloc"));
+  if ((e = dalloc(&h->d_gvec, 2 * (size_t)std::max(1, sys->ngvec))) != cudaSuccess)
+    return fail(cuda_fail(e, "alloc"));
+  cudaMemcpy(h->d_coef, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice);
+  if (sys->nk > 0)
+    cudaMemcpy(h->d_kvec, sys->kvec, sizeof(double) * 2 * sys->nk, cudaMemcpyHostToDevice);
+  if (sys->ngvec > 0 && sys->gvec)
+    cudaMemcpy(h->d_gvec, sys->gvec, sizeof(double) * 2 * sys->ngvec, cudaMemcpyHostToDevice);
+  h->hs.coef = h->d_coef;
+  h->hs.kvec = h->d_kvec;
+  h->hs.gvec = h->d_gvec;
+  if ((e = dalloc(&h->ds, 1)) != cudaSuccess) return fail(cuda_fail(e, "alloc"));
+  cudaMemcpy(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice);
+  int cap = h->cap, N = h->N, nt = h->nt, np = h->nprops;
+  for (int k = 0; k < 2; k++)
+    if ((st = alloc_pop(&h->pop[k], cap, N, nt, np))) return fail(st);
+  if ((e = dalloc(&h->d_blk, (size_t)cap * np)) != cudaSuccess ||
+      (e = dalloc(&h->d_norm, (size_t)cap)) != cudaSuccess ||
+      (e = dalloc(&h->d_cnt, (size_t)cap * 4)) != cudaSuccess ||
+      (e = dalloc(&h->d_wate, (size_t)cap)) != cudaSuccess ||
+      (e = dalloc(&h->d_status, (size_t)cap)) != cudaSuccess ||
+      (e = dalloc(&h->br.delt, (size_t)cap)) != cudaSuccess ||
+      (e = dalloc(&h->br.csum, (size_t)cap)) != cudaSuccess ||
+      (e = dalloc(&h->br.mult, (size_t)cap)) != cudaSuccess ||
+      (e = dalloc(&h->br.src, (size_t)cap)) != cudaSuccess ||
+      (e = dalloc(&h->br.ecum, (size_t)cap)) != cudaSuccess ||
+      (e = dalloc(&h->br.zrank, (size_t)cap)) != cudaSuccess ||
+      (e = dalloc(&h->br.ncapped, 1)) != cudaSuccess ||
+      (e = dalloc(&h->d_x, (size_t)cap * 2 * N)) != cudaSuccess ||
+      (e = dalloc(&h->d_g, (size_t)cap * 2 * N)) != cudaSuccess ||
+      (e = dalloc(&h->d_h, (size_t)cap * nt)) != cudaSuccess ||
+      (e = dalloc(&h->d_p, (size_t)cap * np)) != cudaSuccess ||
+      (e = dalloc(&h->d_s, (size_t)cap)) != cudaSuccess)
+    return fail(cuda_fail(e, "cudaMalloc"));
+  cudaMemset(h->d_blk, 0, sizeof(double) * cap * np);
+  cudaMemset(h->d_norm, 0, sizeof(double) * cap);
+  cudaMemset(h->d_cnt, 0, sizeof(double) * cap * 4);
+  cudaMemset(h->d_status, 0, sizeof(int) * cap);
+  cudaMemset(h->br.ncapped, 0, sizeof(int));
+  if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(cuda_fail(e, "create"));
+  *out = h;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_destroy(qmc2d_handle *h) {
+  if (!h) return QMC2D_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  q2d::rmc_free(&h->rmc);
+  for (int k = 0; k < 2; k++) free_pop(&h->pop[k]);
+  void *bufs[] = {h->ds, h->d_coef, h->d_kvec, h->d_gvec, h->d_blk, h->d_norm, h->d_cnt,
+                  h->d_wate, h->d_status, h->br.delt, h->br.csum, h->br.mult, h->br.src,
+                  h->br.ecum, h->br.zrank, h->br.ncapped, h->d_x, h->d_g, h->d_h, h->d_p,
+                  h->d_s};
+  for (void *b : bufs) cudaFree(b);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_compute_properties_dev(qmc2d_handle *h, int nw, const double *x_dev,
+                                            double *g_dev, double *hl_dev, double *props_dev,
+                                            double *s_dev, void *stream) {
+  if (!h || nw < 0 || nw > h->cap) {
+    q2d::set_error("qmc2d_compute_properties_dev: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  CK(cudaSetDevice(h->device));
+  CK(q2d::launch_eval(h->hs, h->ds, nw, x_dev, g_dev, hl_dev, props_dev, s_dev, h->d_status,
+                      st));
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_compute_properties(qmc2d_handle *h, int nw, const double *x, double *g,
+                                        double *hl, double *props, double *s) {
+  if (!h || !x || nw < 0 || nw > h->cap) {
+    q2d::set_error("qmc2d_compute_properties: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  if (nw == 0) return QMC2D_OK;
+  CK(cudaSetDevice(h->device));
+  size_t N2 = 2 * (size_t)h->N;
+  CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * nw, h->stream));
+  CK(cudaMemcpyAsync(h->d_x, x, sizeof(double) * N2 * nw, cudaMemcpyHostToDevice, h->stream));
+  CK(q2d::launch_eval(h->hs, h->ds, nw, h->d_x, h->d_g, h->d_h, h->d_p, h->d_s, h->d_status,
+                      h->stream));
+  if (g) CK(cudaMemcpyAsync(g, h->d_g, sizeof(double) * N2 * nw, cudaMemcpyDeviceToHost, h->stream));
+  if (hl)
+    CK(cudaMemcpyAsync(hl, h->d_h, sizeof(double) * h->nt * nw, cudaMemcpyDeviceToHost,
+                       h->stream));
+  if (props)
+    CK(cudaMemcpyAsync(props, h->d_p, sizeof(double) * h->nprops * nw, cudaMemcpyDeviceToHost,
+                       h->stream));
+  if (s) CK(cudaMemcpyAsync(s, h->d_s, sizeof(double) * nw, cudaMemcpyDeviceToHost, h->stream));
+  return sync_status(h, nw);
+}
+
+extern "C" int qmc2d_population_set(qmc2d_handle *h, int nw, const double *x) {
+  if (!h || !x || nw <= 0 || nw > h->cap) {
+    q2d::set_error("qmc2d_population_set: population outside capacity");
+    return QMC2D_ERR_POPULATION;
+  }
+  CK(cudaSetDevice(h->device));
+  q2d::DevPop &p = h->pop[h->cur];
+  size_t N2 = 2 * (size_t)h->N;
+  CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * nw, h->stream));
+  CK(cudaMemcpyAsync(p.x, x, sizeof(double) * N2 * nw, cudaMemcpyHostToDevice, h->stream));
+  CK(q2d::launch_eval(h->hs, h->ds, nw, p.x, p.g, p.h, p.p, p.s, h->d_status, h->stream));
+  // read_conf's metropolis_test(1): accepted, p_old(jacc) = 1, age = 0
+  std::vector<double> one(nw, 1.0), zero(nw, 0.0);
+  CK(cudaMemcpy2DAsync(p.p + QMC2D_JACC, sizeof(double) * h->nprops, one.data(), sizeof(double),
+                       sizeof(double), nw, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(p.age, zero.data(), sizeof(double) * nw, cudaMemcpyHostToDevice,
+                     h->stream));
+  h->nw = nw;
+  return sync_status(h, nw);
+}
+
+extern "C" int qmc2d_population_size(qmc2d_handle *h, int *nw) {
+  if (!h || !nw) return QMC2D_ERR_ARG;
+  *nw = h->nw;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_population_get(qmc2d_handle *h, double *x, double *g, double *props,
+                                    double *age) {
+  if (!h) return QMC2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  q2d::DevPop &p = h->pop[h->cur];
+  size_t N2 = 2 * (size_t)h->N, nw = h->nw;
+  if (x) CK(cudaMemcpy(x, p.x, sizeof(double) * N2 * nw, cudaMemcpyDeviceToHost));
+  if (g) CK(cudaMemcpy(g, p.g, sizeof(double) * N2 * nw, cudaMemcpyDeviceToHost));
+  if (props) CK(cudaMemcpy(props, p.p, sizeof(double) * h->nprops * nw, cudaMemcpyDeviceToHost));
+  if (age) CK(cudaMemcpy(age, p.age, sizeof(double) * nw, cudaMemcpyDeviceToHost));
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_block_reset(qmc2d_handle *h) {
+  if (!h) return QMC2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemsetAsync(h->d_blk, 0, sizeof(double) * h->cap * h->nprops, h->stream));
+  CK(cudaMemsetAsync(h->d_norm, 0, sizeof(double) * h->cap, h->stream));
+  CK(cudaMemsetAsync(h->d_cnt, 0, sizeof(double) * h->cap * 4, h->stream));
+  CK(cudaMemsetAsync(h->br.ncapped, 0, sizeof(int), h->stream));
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_block_get(qmc2d_handle *h, double *blk_av, double *blk_norm) {
+  if (!h) return QMC2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  int np = h->nprops, n = std::max(h->nw, h->rmc.nrep);
+  std::vector<double> b((size_t)n * np), nn(n);
+  CK(cudaMemcpy(b.data(), h->d_blk, sizeof(double) * b.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(nn.data(), h->d_norm, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (blk_av)
+    for (int j = 0; j < np; j++) {
+      double t = 0.0;
+      for (int w = 0; w < n; w++) t += b[(size_t)w * np + j];
+      blk_av[j] = t;
+    }
+  if (blk_norm) {
+    double t = 0.0;
+    for (int w = 0; w < n; w++) t += nn[w];
+    *blk_norm = t;
+  }
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_counters_get(qmc2d_handle *h, qmc2d_counters *c) {
+  if (!h || !c) return QMC2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  int n = std::max(h->nw, h->rmc.nrep);
+  std::vector<double> v((size_t)n * 4);
+  int ncap = 0;
+  CK(cudaMemcpy(v.data(), h->d_cnt, sizeof(double) * v.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&ncap, h->br.ncapped, sizeof(int), cudaMemcpyDeviceToHost));
+  std::memset(c, 0, sizeof(*c));
+  for (int w = 0; w < n; w++) {
+    c->accepted += v[4 * w];
+    c->proposed += v[4 * w + 1];
+    c->forced += v[4 * w + 2];
+  }
+  c->max_weight_capped = ncap;
+  return QMC2D_OK;
+}
+
+static int run_moves(qmc2d_handle *h, int nstp, int dmc, double delta, double etrial,
+                     double mmult, int mage) {
+  q2d::MoveArgs a{};
+  a.nw = h->nw;
+  a.nstp = nstp;
+  a.dmc = dmc;
+  a.delta = delta;
+  a.mage = mage;
+  a.etrial = etrial;
+  a.mmult = mmult;
+  a.seed = h->seed;
+  a.step0 = h->move_counter;
+  a.blk = h->d_blk;
+  a.blk_norm = h->d_norm;
+  a.cnt = h->d_cnt;
+  a.wate = dmc ? h->d_wate : nullptr;
+  a.status = h->d_status;
+  if (h->hs.delta != delta && h->hs.adrift != 0.0) {
+    h->hs.delta = delta;
+    CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
+  }
+  CK(q2d::launch_moves(h->hs, h->ds, h->pop[h->cur], a, h->stream));
+  h->move_counter += (uint32_t)nstp;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_vmc(qmc2d_handle *h, int nstp, double delta, int mage) {
+  if (!h || nstp < 0 || !(delta > 0.0)) return QMC2D_ERR_ARG;
+  if (h->nw <= 0) {
+    q2d::set_error("qmc2d_vmc: empty population");
+    return QMC2D_ERR_STACK;
+  }
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * h->nw, h->stream));
+  int st = run_moves(h, nstp, 0, delta, 0.0, 0.0, mage);
+  if (st) return st;
+  return sync_status(h, h->nw);
+}
+
+extern "C" int qmc2d_dmc(qmc2d_handle *h, int nstp, int mmstep, double delta, double etrial,
+                         double mmult, int mage) {
+  if (!h || nstp < 0 || mmstep <= 0 || !(delta > 0.0)) return QMC2D_ERR_ARG;
+  if (h->nw <= 0) {
+    q2d::set_error("qmc2d_dmc: empty population");
+    return QMC2D_ERR_STACK;
+  }
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * h->nw, h->stream));
+  for (int gen = 0; gen < nstp; gen++) {
+    int st = run_moves(h, mmstep, 1, delta, etrial, mmult, mage);
+    if (st) return st;
+    CK(q2d::launch_branch(h->nw, h->d_wate, h->seed, h->gen_counter, h->br, h->stream));
+    int nxt = 1 - h->cur;
+    CK(q2d::launch_gather(h->hs, h->pop[h->cur], h->pop[nxt], h->br.src, h->nw, h->stream));
+    h->cur = nxt;
+    h->gen_counter++;
+  }
+  return sync_status(h, h->nw);
+}

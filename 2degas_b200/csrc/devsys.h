@@ -1,0 +1,53 @@
+// devsys.h - device-side view of a qmc2d_system and of a walker population.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/qmc2d.h"
+
+namespace q2d {
+
+constexpr int kThreads = 256;  // threads per walker CTA
+constexpr int kGroup = 8;      // threads cooperating on one particle's pair sums
+constexpr int kChunk = 32;     // (electron, direction) columns per backflow quadratic-form tile
+
+// Per-walker status word bits written by the kernels.
+enum : int { ST_OK = 0, ST_SINGULAR = 1, ST_NONFINITE = 2, ST_UNDERFLOW = 4 };
+
+// Flattened system for kernels (passed by value as a kernel parameter).
+struct DevSys {
+  int N, nt, npnorm, nprops, nscalar, jrhok, nk, ngvec, nrhok;
+  int np[2], ipfrst[2], irhok[2];
+  int nmax;  // largest spin block
+  double hbs2m[2], el[2], eli[2];
+  double drt, drti, drti2, v0, adrift, delta;
+  int ntheta, ref_underflow;
+  int has_u2, has_u3, has_bf, has_v2;
+  // reptation options (input keywords ecut, rejection, wpiu, gstorto, nodalaction)
+  int ecut, rejection, wpiu, gstorto, nodalaction;
+  double value_ecut;
+  // table slots per type pair (into the packed coefficient buffer), -1 if none
+  int iu2[2][2], iu3[2][2], iub[2][2], iv2[2][2];
+  int tab_off[QMC2D_MAX_TABLES];   // offset (doubles) of ut(0,1) of table t
+  int tab_ngrid[QMC2D_MAX_TABLES];
+  int tab_iexp[QMC2D_MAX_TABLES];
+  int tab_nkew[QMC2D_MAX_TABLES];
+  int tab_vkoff[QMC2D_MAX_TABLES];  // offset of v_k in the packed buffer
+  double tab_tail[QMC2D_MAX_TABLES];
+  const double *coef;  // packed tables: ut rows (4 doubles each) and v_k lists
+  const double *kvec;  // 2*nk
+  const double *gvec;  // 2*ngvec
+};
+
+// Walker population in HBM: one block of each field per walker slot
+// (walker-major; inside a walker the reference's x(2,N) order).
+struct DevPop {
+  double *x, *g, *h, *p, *s, *age;  // 2N, 2N, nt, nprops, 1, 1 per walker
+};
+
+// Shared-memory footprint (bytes) of the walker evaluation for this system.
+size_t eval_smem_bytes(const DevSys &s);
+// Extra shared memory a move kernel adds for the walker's own state.
+size_t move_smem_bytes(const DevSys &s);
+
+}  // namespace q2d

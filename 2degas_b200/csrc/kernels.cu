@@ -1,0 +1,445 @@
+// kernels.cu - walker kernels for sm_100a: batched evaluation
+// (compute_properties), the fused VMC/DMC move (move + compute_properties +
+// metropolis_test + averages(2), reptation.f:4617, 2661, 2622, 4275), the
+// fixed-population comb of branch2 (reptation.f:2162) and the slot gather
+// that replaces its send/receive/prov_dest copies.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "walker_eval.cuh"
+
+namespace q2d {
+
+// ------------------------------------------------------------------ Philox
+// Philox4x32-10 (Salmon et al., SC'11): 10 rounds, Weyl key schedule.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// 53 random bits, offset by half an ulp: u in (0,1).
+__device__ __forceinline__ double open01(uint32_t a, uint32_t b) {
+  unsigned long long k = ((unsigned long long)(a >> 5) << 26) | (unsigned long long)(b >> 6);
+  return ((double)k + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+__device__ __forceinline__ double2 uniform2(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c2,
+                                            uint32_t c3) {
+  uint4 o = philox4x32_10(make_uint4(c0, c1, c2, c3),
+                          make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+  return make_double2(open01(o.x, o.y), open01(o.z, o.w));
+}
+
+__device__ __forceinline__ void load_sys(DevSys &S, const DevSys *sp) {
+  const int *src = reinterpret_cast<const int *>(sp);
+  int *dst = reinterpret_cast<int *>(&S);
+  for (int i = threadIdx.x; i < (int)(sizeof(DevSys) / sizeof(int)); i += blockDim.x)
+    dst[i] = src[i];
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------- eval
+__global__ void __launch_bounds__(kThreads) eval_kernel(const DevSys *sp, int nw,
+                                                        const double *__restrict__ x, double *g,
+                                                        double *hl, double *props, double *s,
+                                                        int *status) {
+  __shared__ DevSys S;
+  extern __shared__ __align__(16) char smem[];
+  load_sys(S, sp);
+  EvalSmem m;
+  size_t off = eval_carve(S, smem, &m);
+  double *pn = reinterpret_cast<double *>(smem + off);
+  double *hn = pn + S.nprops;
+  double *sn = hn + 2;
+  const int w = blockIdx.x;
+  if (w >= nw) return;
+  const int N2 = 2 * S.N;
+  for (int j = threadIdx.x; j < N2; j += blockDim.x) m.x[j] = x[(size_t)w * N2 + j];
+  __syncthreads();
+  int st = eval_walker(S, m, hn, pn, sn);
+  for (int j = threadIdx.x; j < N2; j += blockDim.x) g[(size_t)w * N2 + j] = m.g[j];
+  for (int j = threadIdx.x; j < S.nprops; j += blockDim.x)
+    props[(size_t)w * S.nprops + j] = pn[j];
+  if (threadIdx.x == 0) {
+    for (int t = 0; t < S.nt; t++) hl[(size_t)w * S.nt + t] = hn[t];
+    s[w] = *sn;
+    status[w] = st;
+  }
+}
+
+size_t eval_smem_bytes(const DevSys &s) {
+  return eval_carve(s, nullptr, nullptr) + align16(sizeof(double) * (s.nprops + 3));
+}
+
+// ------------------------------------------------------------- the move
+// Walker state kept in shared memory across the CTA's steps.
+struct MoveSmem {
+  double *xo, *go, *po, *pn, *blk, *ho, *hn, *sc;
+};
+
+__host__ __device__ inline size_t move_carve(const DevSys &s, char *base, MoveSmem *m) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) -> char * {
+    char *p = base ? base + off : nullptr;
+    off += align16(bytes);
+    return p;
+  };
+  MoveSmem t;
+  t.xo = (double *)take(sizeof(double) * 2 * s.N);
+  t.go = (double *)take(sizeof(double) * 2 * s.N);
+  t.po = (double *)take(sizeof(double) * s.nprops);
+  t.pn = (double *)take(sizeof(double) * s.nprops);
+  t.blk = (double *)take(sizeof(double) * s.nprops);
+  t.ho = (double *)take(sizeof(double) * 2);
+  t.hn = (double *)take(sizeof(double) * 2);
+  t.sc = (double *)take(sizeof(double) * 8);
+  if (m) *m = t;
+  return off;
+}
+
+size_t move_smem_bytes(const DevSys &s) {
+  return eval_carve(s, nullptr, nullptr) + move_carve(s, nullptr, nullptr);
+}
+
+__global__ void __launch_bounds__(kThreads) move_kernel(const DevSys *sp, DevPop pop, MoveArgs a) {
+  __shared__ DevSys S;
+  extern __shared__ __align__(16) char smem[];
+  load_sys(S, sp);
+  EvalSmem m;
+  size_t off = eval_carve(S, smem, &m);
+  MoveSmem v;
+  move_carve(S, smem + off, &v);
+  const int w = blockIdx.x, tid = threadIdx.x;
+  if (w >= a.nw) return;
+  const int N2 = 2 * S.N, np = S.nprops, nt = S.nt;
+  for (int j = tid; j < N2; j += kThreads) {
+    v.xo[j] = pop.x[(size_t)w * N2 + j];
+    v.go[j] = pop.g[(size_t)w * N2 + j];
+  }
+  for (int j = tid; j < np; j += kThreads) {
+    v.po[j] = pop.p[(size_t)w * np + j];
+    v.blk[j] = a.blk[(size_t)w * np + j];
+  }
+  if (tid < nt) v.ho[tid] = pop.h[(size_t)w * nt + tid];
+  __syncthreads();
+  double so = pop.s[w];
+  double age = pop.age[w];
+  double norm = a.blk_norm[w];
+  double wate = 1.0;
+  double nacc = 0.0, nforced = 0.0;
+  int status = 0;
+  const uint64_t seed = a.seed;
+  const double pi = 3.141592653589793;
+  for (int istp = 0; istp < a.nstp; istp++) {
+    const uint32_t step = a.step0 + (uint32_t)istp;
+    // proposal (move, reptation.f:4631-4646)
+    double wo = 0.0;
+    for (int j = tid; j < N2; j += kThreads) {
+      int ti = type_of(S, j >> 1);
+      double var = 2.0 * S.hbs2m[ti] * a.delta, vari = 1.0 / var;
+      double2 u = uniform2(seed, (uint32_t)j, (uint32_t)w, step, 0u);
+      double chi = cos(pi * u.x) * sqrt(-2.0 * var * log(u.y));
+      wo -= chi * chi * vari;
+      m.x[j] = chi + (-var * v.go[j]) + v.xo[j];
+    }
+    double wold = block_sum(wo, m.red);
+    double sn = 1.0;
+    status |= eval_walker(S, m, v.hn, v.pn, &v.sc[0]);
+    sn = v.sc[0];
+    // reverse move (reptation.f:4660-4674)
+    double wn = 0.0;
+    for (int j = tid; j < N2; j += kThreads) {
+      int ti = type_of(S, j >> 1);
+      double var = 2.0 * S.hbs2m[ti] * a.delta, vari = 1.0 / var;
+      double chi = v.xo[j] - m.x[j] - (-var * m.g[j]);
+      wn -= chi * chi * vari;
+    }
+    double wnew = block_sum(wn, m.red);
+    double p;
+    if (age == a.mage) {
+      p = 1.0;
+      nforced += 1.0;
+    } else {
+      p = (v.po[QMC2D_JLTF] - v.pn[QMC2D_JLTF]) * 2.0 + 0.5 * (wnew - wold);
+      p = fmin(0.0, fmax(-50.0, p));
+      p = exp(p);
+    }
+    // metropolis_test (reptation.f:2622-2659)
+    double xr = 1.0;
+    if (p < 1.0) xr = uniform2(seed, 0xFFFFFFFEu, (uint32_t)w, step, 0u).x;
+    bool acc = p >= xr;
+    double elocal = acc ? 0.5 * (v.pn[QMC2D_JETOT] + v.po[QMC2D_JETOT]) : v.po[QMC2D_JETOT];
+    __syncthreads();
+    if (acc) {
+      for (int j = tid; j < N2; j += kThreads) {
+        v.xo[j] = m.x[j];
+        v.go[j] = m.g[j];
+      }
+      for (int j = tid; j < np; j += kThreads) v.po[j] = v.pn[j];
+      if (tid < nt) v.ho[tid] = v.hn[tid];
+      so = sn;
+      age = 0.0;
+      nacc += 1.0;
+    } else {
+      age += 1.0;
+    }
+    __syncthreads();
+    if (tid == 0) v.po[QMC2D_JACC] = p;
+    double wgt = 1.0;
+    if (a.dmc) {
+      // dmc weight (reptation.f:898-903)
+      double peso = exp(-S.npnorm * (elocal - a.etrial) * a.delta);
+      if (peso > a.mmult) peso = a.mmult;
+      wate *= peso;
+      wgt = wate;
+    }
+    __syncthreads();
+    for (int j = tid; j < np; j += kThreads) v.blk[j] += v.po[j] * wgt;
+    norm += wgt;
+  }
+  __syncthreads();
+  for (int j = tid; j < N2; j += kThreads) {
+    pop.x[(size_t)w * N2 + j] = v.xo[j];
+    pop.g[(size_t)w * N2 + j] = v.go[j];
+  }
+  for (int j = tid; j < np; j += kThreads) {
+    pop.p[(size_t)w * np + j] = v.po[j];
+    a.blk[(size_t)w * np + j] = v.blk[j];
+  }
+  if (tid < nt) pop.h[(size_t)w * nt + tid] = v.ho[tid];
+  if (tid == 0) {
+    pop.s[w] = so;
+    pop.age[w] = age;
+    a.blk_norm[w] = norm;
+    a.cnt[4 * w + 0] += nacc;
+    a.cnt[4 * w + 1] += a.nstp;
+    a.cnt[4 * w + 2] += nforced;
+    if (status) a.cnt[4 * w + 3] += 1.0;
+    if (a.wate) a.wate[w] = wate;
+    a.status[w] |= status;
+  }
+}
+
+// ------------------------------------------------------------- branch2
+// One block. Population-wide steps of branch2 (reptation.f:2174-2212) and
+// prov_dest's in-rank assignment (reptation.f:2260-2271) on global scratch.
+__device__ void block_exclusive_scan_partials(double *part, int n) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double run = 0.0;
+    for (int i = 0; i < n; i++) {
+      double t = part[i];
+      part[i] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+}
+
+__device__ void block_exclusive_scan_ipartials(int *part, int n) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int i = 0; i < n; i++) {
+      int t = part[i];
+      part[i] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+}
+
+constexpr int kBranchThreads = 1024;
+
+__global__ void __launch_bounds__(kBranchThreads) branch_kernel(int nw, double *wate,
+                                                                uint64_t seed, uint32_t gen,
+                                                                BranchScratch b) {
+  __shared__ double dpart[kBranchThreads];
+  __shared__ int ipart[kBranchThreads];
+  __shared__ int ipart2[kBranchThreads];
+  __shared__ double red[32];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int seg = (nw + nt - 1) / nt;
+  const int lo = min(nw, tid * seg), hi = min(nw, lo + seg);
+  // cap at wmult = 10 (reptation.f:2174-2181)
+  int ncap = 0;
+  double loc = 0.0;
+  for (int i = lo; i < hi; i++) {
+    double v = wate[i];
+    if (v > 10.0) {
+      v = 10.0;
+      wate[i] = v;
+      ncap++;
+    }
+    loc += v;
+  }
+  if (ncap) atomicAdd(b.ncapped, ncap);
+  // somma
+  for (int o = 16; o > 0; o >>= 1) loc += __shfl_xor_sync(0xffffffffu, loc, o);
+  if ((tid & 31) == 0) red[tid >> 5] = loc;
+  __syncthreads();
+  double somma = 0.0;
+  for (int k = 0; k < nt / 32; k++) somma += red[k];
+  // multiplicities and fractional parts, inclusive scan of the fractions
+  double part = 0.0;
+  for (int i = lo; i < hi; i++) {
+    double ww = nw * wate[i] / somma;
+    int tm = (int)ww;
+    b.mult[i] = tm;
+    b.delt[i] = ww - tm;
+    part += ww - tm;
+  }
+  dpart[tid] = part;
+  block_exclusive_scan_partials(dpart, nt);
+  double run = dpart[tid];
+  for (int i = lo; i < hi; i++) {
+    run += b.delt[i];
+    b.csum[i] = run;
+  }
+  __syncthreads();
+  double k0 = b.csum[nw - 1];
+  int ncomb = (int)llround(k0);
+  // systematic comb: copy c lands on the first walker whose cumulative
+  // fraction reaches c + r_c (r_c from the shared stream, as rannyu2)
+  for (int c = tid; c < ncomb; c += nt) {
+    double r = uniform2(seed, (uint32_t)c, 0xFFFFFFFFu, gen, 1u).x;
+    double target = c + r;
+    int a0 = 0, a1 = nw;  // lower_bound
+    while (a0 < a1) {
+      int mid = (a0 + a1) >> 1;
+      if (b.csum[mid] < target) a0 = mid + 1;
+      else a1 = mid;
+    }
+    if (a0 >= nw) a0 = nw - 1;
+    atomicAdd(&b.mult[a0], 1);
+  }
+  __syncthreads();
+  // slots left empty take the surplus copies in order of source slot
+  int zc = 0, ec = 0;
+  for (int i = lo; i < hi; i++) {
+    int mu = b.mult[i];
+    zc += mu == 0;
+    ec += mu > 1 ? mu - 1 : 0;
+  }
+  ipart[tid] = zc;
+  ipart2[tid] = ec;
+  block_exclusive_scan_ipartials(ipart, nt);
+  block_exclusive_scan_ipartials(ipart2, nt);
+  int zr = ipart[tid], er = ipart2[tid];
+  for (int i = lo; i < hi; i++) {
+    int mu = b.mult[i];
+    b.zrank[i] = zr;
+    b.ecum[i] = er;
+    zr += mu == 0;
+    er += mu > 1 ? mu - 1 : 0;
+  }
+  __syncthreads();
+  int etot = ipart2[nt - 1];
+  {
+    // total extras = last exclusive partial + last segment's count
+    int lo2 = min(nw, (nt - 1) * seg), hi2 = min(nw, lo2 + seg);
+    for (int i = lo2; i < hi2; i++) {
+      int mu = b.mult[i];
+      etot += mu > 1 ? mu - 1 : 0;
+    }
+  }
+  for (int j = lo; j < hi; j++) {
+    int src = j;
+    if (b.mult[j] == 0) {
+      int z = b.zrank[j];
+      if (z < etot) {
+        int a0 = 0, a1 = nw;  // upper_bound(ecum, z) - 1
+        while (a0 < a1) {
+          int mid = (a0 + a1) >> 1;
+          if (b.ecum[mid] <= z) a0 = mid + 1;
+          else a1 = mid;
+        }
+        src = a0 - 1;
+      }
+    }
+    b.src[j] = src;
+  }
+}
+
+__global__ void gather_kernel(DevPop from, DevPop to, const int *src, int N2, int nt, int np) {
+  const int j = blockIdx.x, i = src[j];
+  for (int e = threadIdx.x; e < N2; e += blockDim.x) {
+    to.x[(size_t)j * N2 + e] = from.x[(size_t)i * N2 + e];
+    to.g[(size_t)j * N2 + e] = from.g[(size_t)i * N2 + e];
+  }
+  for (int e = threadIdx.x; e < np; e += blockDim.x)
+    to.p[(size_t)j * np + e] = from.p[(size_t)i * np + e];
+  if (threadIdx.x < nt) to.h[(size_t)j * nt + threadIdx.x] = from.h[(size_t)i * nt + threadIdx.x];
+  if (threadIdx.x == 0) {
+    to.s[j] = from.s[i];
+    to.age[j] = from.age[i];
+  }
+}
+
+__global__ void philox_probe_kernel(uint64_t seed, const uint32_t *ctr, uint32_t *out, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint4 o = philox4x32_10(make_uint4(ctr[4 * i], ctr[4 * i + 1], ctr[4 * i + 2], ctr[4 * i + 3]),
+                          make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+  out[4 * i] = o.x;
+  out[4 * i + 1] = o.y;
+  out[4 * i + 2] = o.z;
+  out[4 * i + 3] = o.w;
+}
+
+// ------------------------------------------------------------ launchers
+static cudaError_t set_smem(const void *fn, size_t bytes) {
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t launch_eval(const DevSys &hs, const DevSys *ds, int nw, const double *x, double *g,
+                        double *hl, double *props, double *s, int *status, cudaStream_t st) {
+  if (nw <= 0) return cudaSuccess;
+  size_t sm = eval_smem_bytes(hs);
+  cudaError_t e = set_smem((const void *)eval_kernel, sm);
+  if (e != cudaSuccess) return e;
+  eval_kernel<<<nw, kThreads, sm, st>>>(ds, nw, x, g, hl, props, s, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_moves(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
+                         cudaStream_t st) {
+  if (a.nw <= 0 || a.nstp <= 0) return cudaSuccess;
+  size_t sm = move_smem_bytes(hs);
+  cudaError_t e = set_smem((const void *)move_kernel, sm);
+  if (e != cudaSuccess) return e;
+  move_kernel<<<a.nw, kThreads, sm, st>>>(ds, pop, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_branch(int nw, double *wate, uint64_t seed, uint32_t gen, BranchScratch b,
+                          cudaStream_t st) {
+  if (nw <= 0) return cudaSuccess;
+  branch_kernel<<<1, kBranchThreads, 0, st>>>(nw, wate, seed, gen, b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather(const DevSys &hs, DevPop from, DevPop to, const int *src, int nw,
+                          cudaStream_t st) {
+  if (nw <= 0) return cudaSuccess;
+  gather_kernel<<<nw, 128, 0, st>>>(from, to, src, 2 * hs.N, hs.nt, hs.nprops);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_philox_probe(uint64_t seed, const uint32_t *ctr, uint32_t *out, int n,
+                                cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  philox_probe_kernel<<<(n + 127) / 128, 128, 0, st>>>(seed, ctr, out, n);
+  return cudaGetLastError();
+}
+
+}  // namespace q2d

@@ -1,0 +1,52 @@
+// kernels.cuh - launchers of the walker kernels (kernels.cu).
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "devsys.h"
+
+namespace q2d {
+
+struct MoveArgs {
+  int nw;
+  int nstp;           // VMC steps, or DMC moves per generation (mmstep)
+  int dmc;            // 0: VMC averages (weight 1), 1: DMC weights
+  double delta;
+  double mage;        // forced-move age (compared with ==, as the reference)
+  double etrial, mmult;
+  uint64_t seed;
+  uint32_t step0;     // Philox c2 of the first move
+  double *blk;        // nw * nprops block sums of p_old (* weight)
+  double *blk_norm;   // nw
+  double *cnt;        // nw * 4: accepted, proposed, forced, nonzero status
+  double *wate;       // nw DMC weights (out)
+  int *status;        // nw status words (OR-ed)
+};
+
+// Evaluate nw configurations x (2N each) -> g, hl, props, s.
+cudaError_t launch_eval(const DevSys &hs, const DevSys *ds, int nw, const double *x, double *g,
+                        double *hl, double *props, double *s, int *status, cudaStream_t st);
+
+// VMC steps or one DMC generation's moves on a resident population.
+cudaError_t launch_moves(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
+                         cudaStream_t st);
+
+// branch2's comb: wate -> src (new slot j copies old slot src[j]).
+struct BranchScratch {
+  double *delt, *csum;
+  int *mult, *src, *ecum, *zrank;
+  int *ncapped;
+};
+cudaError_t launch_branch(int nw, double *wate, uint64_t seed, uint32_t gen, BranchScratch b,
+                          cudaStream_t st);
+// new[j] = old[src[j]] for every walker field.
+cudaError_t launch_gather(const DevSys &hs, DevPop from, DevPop to, const int *src, int nw,
+                          cudaStream_t st);
+
+// Device Philox4x32-10 check: out[4*i..] = philox(ctr_i, key) for testing.
+cudaError_t launch_philox_probe(uint64_t seed, const uint32_t *ctr, uint32_t *out, int n,
+                                cudaStream_t st);
+
+}  // namespace q2d

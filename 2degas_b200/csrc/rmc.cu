@@ -1,0 +1,580 @@
+// rmc.cu - reptation QMC on the device: one CTA per reptile, the path ring
+// in HBM. Restates read_path (reptation.f:1775), get_w_stack (:1804), fgg
+// (:1853), reptation_metropolis_test (:1865), reptation_move (:1897) and
+// the scalar part of path_props (:1567-1577). Random draws follow the
+// Philox stream layout documented in include/qmc2d.h's RMC section.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/qmc2d.h"
+#include "common.h"
+#include "kernels.cuh"
+#include "rmc.cuh"
+#include "walker_eval.cuh"
+
+namespace q2d {
+
+namespace {
+
+enum { JBRA = 0, JDTP = 1, JITP = 2, JLNG = 3, JNDS = 4 };
+
+__device__ __forceinline__ uint4 philox(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+__device__ __forceinline__ double2 u2(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c2,
+                                      uint32_t c3) {
+  uint4 o = philox(make_uint4(c0, c1, c2, c3), make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+  auto cv = [](uint32_t a, uint32_t b) {
+    unsigned long long k = ((unsigned long long)(a >> 5) << 26) | (unsigned long long)(b >> 6);
+    return ((double)k + 0.5) * (1.0 / 9007199254740992.0);
+  };
+  return make_double2(cv(o.x, o.y), cv(o.z, o.w));
+}
+
+struct RmcArgs {
+  int nrep, ntau, ntauskip, mdelta, nbuf, nstp;
+  double delta, etrial, mage, mage_r;
+  uint64_t seed;
+  uint32_t step0;
+  int ecut, rejection, wpiu, gstorto, nodalaction;
+  double value_ecut;
+  double *x, *g, *p, *h, *s, *age_stack, *w, *pp_old, *age;
+  int *ends;
+  double *blk, *blk_norm, *cnt;
+  int *status;
+};
+
+__device__ __forceinline__ void load_sys(DevSys &S, const DevSys *sp) {
+  const int *src = reinterpret_cast<const int *>(sp);
+  int *dst = reinterpret_cast<int *>(&S);
+  for (int i = threadIdx.x; i < (int)(sizeof(DevSys) / sizeof(int)); i += blockDim.x)
+    dst[i] = src[i];
+  __syncthreads();
+}
+
+__device__ __forceinline__ double fgg(const RmcArgs &a, double e, double gg) {
+  return a.ecut == 0 ? e : a.value_ecut + (e - a.value_ecut) * gg;
+}
+
+// Bead pointers of reptile r, ring slot j.
+struct Bead {
+  double *x, *g, *p, *h, *s, *age, *w;
+};
+__device__ __forceinline__ Bead bead(const DevSys &S, const RmcArgs &a, int r, int j) {
+  size_t b = (size_t)r * a.nbuf + j;
+  Bead o;
+  o.x = a.x + b * 2 * S.N;
+  o.g = a.g + b * 2 * S.N;
+  o.p = a.p + b * S.nprops;
+  o.h = a.h + b * S.nt;
+  o.s = a.s + b;
+  o.age = a.age_stack + b;
+  o.w = a.w + b * 5;
+  return o;
+}
+
+// path_props scalar part: mean over beads 1+ntauskip..ntau-ntauskip from
+// kfirst; E_L is the mixed estimator of the two ends.
+__device__ void path_props(const DevSys &S, const RmcArgs &a, int r, int kfirst, int klast,
+                           double *pp) {
+  for (int ip = threadIdx.x; ip < S.nprops; ip += blockDim.x) {
+    double t = 0.0;
+    for (int i = 1 + a.ntauskip; i <= a.ntau - a.ntauskip; i++) {
+      int j = (kfirst + i - 1) % a.nbuf;
+      t += bead(S, a, r, j).p[ip];
+    }
+    pp[ip] = t / (a.ntau - 2 * a.ntauskip);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    pp[QMC2D_JETOT] =
+        0.5 * (bead(S, a, r, klast).p[QMC2D_JETOT] + bead(S, a, r, kfirst).p[QMC2D_JETOT]);
+  __syncthreads();
+}
+
+// get_w_stack (reptation.f:1804-1851) for beads j -> jn; returns wnew/wold.
+__device__ void get_w_stack(const DevSys &S, const RmcArgs &a, int r, int j, int jn, double *red,
+                            double *wnew_out, double *wold_out) {
+  Bead bj = bead(S, a, r, j), bn = bead(S, a, r, jn);
+  double wf = 0, wb = 0, wg = 0;
+  for (int k = threadIdx.x; k < 2 * S.N; k += blockDim.x) {
+    int t = type_of(S, k >> 1);
+    double var = 2.0 * S.hbs2m[t] * a.delta, vari = 1.0 / var;
+    double d0 = bj.x[k] - bn.x[k];
+    wg -= d0 * d0 * vari;
+    double df = -var * bj.g[k];
+    double d1 = bj.x[k] + df - bn.x[k];
+    wf -= d1 * d1 * vari;
+    double db = -var * bn.g[k];
+    double d2 = bj.x[k] - db - bn.x[k];
+    wb -= d2 * d2 * vari;
+  }
+  double wnew = block_sum(wb, red), wold = block_sum(wf, red), lng = block_sum(wg, red);
+  if (threadIdx.x == 0) {
+    lng += a.delta * S.npnorm * (bj.p[QMC2D_JKIN0] + bn.p[QMC2D_JKIN0]);
+    bj.w[JLNG] = 0.5 * lng;
+    bj.w[JDTP] = 0.5 * wold;
+    bj.w[JBRA] = -.5 * a.delta * S.npnorm *
+                 (fgg(a, bj.p[QMC2D_JETOT], bj.p[QMC2D_JGG]) +
+                  fgg(a, bn.p[QMC2D_JETOT], bn.p[QMC2D_JGG]) - 2.0 * a.etrial);
+    bn.w[JITP] = 0.5 * wnew;
+    double nds = 0.0;
+    for (int t = 0; t < S.nt; t++) {
+      int ju = QMC2D_JUN(S.nt, t);
+      double var = 2.0 * S.hbs2m[t] * a.delta;
+      nds -= log(1.0 - exp(-bj.p[ju] * bn.p[ju] / (0.5 * var)));
+    }
+    bj.w[JNDS] = nds;
+  }
+  __syncthreads();
+  *wnew_out = wnew;
+  *wold_out = wold;
+}
+
+// read_path after the beads are evaluated: w_stack, bead acceptances,
+// path properties, ends.
+__global__ void rmc_init_kernel(const DevSys *sp, RmcArgs a) {
+  __shared__ DevSys S;
+  __shared__ double red[32];
+  extern __shared__ __align__(16) char smem[];
+  load_sys(S, sp);
+  double *pp = reinterpret_cast<double *>(smem);
+  const int r = blockIdx.x;
+  if (r >= a.nrep) return;
+  for (int i = 0; i < a.ntau; i++) {
+    Bead b = bead(S, a, r, i);
+    if (threadIdx.x == 0) {
+      b.p[QMC2D_JACC] = 1.0;
+      *b.age = 0.0;
+    }
+  }
+  __syncthreads();
+  path_props(S, a, r, 0, a.ntau - 1, pp);
+  for (int i = 1; i <= a.ntau - 1; i++) {
+    int j = i - 1, jn = i;
+    double wnew, wold;
+    get_w_stack(S, a, r, j, jn, red, &wnew, &wold);
+    if (threadIdx.x == 0) {
+      Bead bj = bead(S, a, r, j), bn = bead(S, a, r, jn);
+      double p = 2 * (bj.p[QMC2D_JLTF] - bn.p[QMC2D_JLTF]) + 0.5 * (wnew - wold);
+      p = fmin(0.0, fmax(-50.0, p));
+      bn.p[QMC2D_JACC] = exp(p);
+    }
+    __syncthreads();
+  }
+  for (int ip = threadIdx.x; ip < S.nprops; ip += blockDim.x)
+    a.pp_old[(size_t)r * S.nprops + ip] = pp[ip];
+  if (threadIdx.x == 0) {
+    a.ends[2 * r] = 0;
+    a.ends[2 * r + 1] = a.ntau - 1;
+    a.age[r] = 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) rmc_eval_beads_kernel(const DevSys *sp, RmcArgs a,
+                                                                  const double *x) {
+  __shared__ DevSys S;
+  extern __shared__ __align__(16) char smem[];
+  load_sys(S, sp);
+  EvalSmem m;
+  size_t off = eval_carve(S, smem, &m);
+  double *pn = reinterpret_cast<double *>(smem + off);
+  double *hn = pn + S.nprops;
+  double *sn = hn + 2;
+  const int r = blockIdx.x / a.ntau, i = blockIdx.x % a.ntau;
+  const int N2 = 2 * S.N;
+  Bead b = bead(S, a, r, i);
+  for (int k = threadIdx.x; k < N2; k += blockDim.x) {
+    double v = x[((size_t)r * a.ntau + i) * N2 + k];
+    m.x[k] = v;
+    b.x[k] = v;
+  }
+  __syncthreads();
+  int st = eval_walker(S, m, hn, pn, sn);
+  for (int k = threadIdx.x; k < N2; k += blockDim.x) b.g[k] = m.g[k];
+  for (int k = threadIdx.x; k < S.nprops; k += blockDim.x) b.p[k] = pn[k];
+  if (threadIdx.x == 0) {
+    for (int t = 0; t < S.nt; t++) b.h[t] = hn[t];
+    *b.s = *sn;
+    if (st) atomicOr(&a.status[r], st);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) rmc_move_kernel(const DevSys *sp, RmcArgs a) {
+  __shared__ DevSys S;
+  extern __shared__ __align__(16) char smem[];
+  load_sys(S, sp);
+  EvalSmem m;
+  size_t off = eval_carve(S, smem, &m);
+  double *pn = reinterpret_cast<double *>(smem + off);
+  double *pp = pn + S.nprops;   // p_p_new
+  double *ppo = pp + S.nprops;  // p_p_old
+  double *blk = ppo + S.nprops;
+  double *hn = blk + S.nprops;
+  double *sc = hn + 2;
+  const int r = blockIdx.x, tid = threadIdx.x;
+  if (r >= a.nrep) return;
+  const int N2 = 2 * S.N, nt = S.nt, nb = a.nbuf;
+  for (int ip = tid; ip < S.nprops; ip += blockDim.x) {
+    ppo[ip] = a.pp_old[(size_t)r * S.nprops + ip];
+    blk[ip] = a.blk[(size_t)r * S.nprops + ip];
+  }
+  int jfirst = a.ends[2 * r], jlast = a.ends[2 * r + 1];
+  double age = a.age[r];
+  double norm = a.blk_norm[r];
+  double nacc = 0.0;
+  int status = 0;
+  double half = 0.5, one = 0.0, one_nds = 0.0, mezzo = 0.0;
+  if (a.wpiu != 0) {
+    mezzo = 0.5;
+  } else if (a.gstorto != 0) {
+    half = 0.0;
+    one = 1.0;
+    if (a.nodalaction != 0) one_nds = 1.0;
+  }
+  const double pi = 3.141592653589793;
+  __syncthreads();
+  for (int istp = 0; istp < a.nstp; istp++) {
+    const uint32_t t = a.step0 + (uint32_t)istp;
+    double2 dl = u2(a.seed, 0xFFFFFFF0u, (uint32_t)r, t, 2u);
+    int idir = (dl.x - 0.5) >= 0.0 ? 1 : -1;
+    int ndelta = 1 + (int)(dl.y * a.mdelta);
+    int jstart = idir == 1 ? jlast : jfirst;
+    for (int idelta = 1; idelta <= ndelta; idelta++) {
+      int j = (jstart + idir * (idelta - 1) + nb) % nb;
+      int jn = (jstart + idir * idelta + nb) % nb;
+      uint32_t c3 = 3u + (uint32_t)(idelta - 1);
+      Bead bj = bead(S, a, r, j), bn = bead(S, a, r, jn);
+      double ww = 0, wg = 0, dd = 0;
+      for (int k = tid; k < N2; k += blockDim.x) {
+        int ti = type_of(S, k >> 1);
+        double var = 2.0 * S.hbs2m[ti] * a.delta, vari = 1.0 / var;
+        double drift = -var * bj.g[k];
+        dd += drift * drift * vari;
+        double2 u = u2(a.seed, (uint32_t)k, (uint32_t)r, t, c3);
+        double chi = cos(pi * u.x) * sqrt(-2.0 * var * log(u.y));
+        ww -= chi * chi * vari;
+        m.x[k] = chi + drift + bj.x[k];
+        wg -= (chi + drift) * (chi + drift) * vari;
+      }
+      double wold = block_sum(ww, m.red), dold = block_sum(dd, m.red);
+      double lng = block_sum(wg, m.red);
+      status |= eval_walker(S, m, hn, pn, sc);
+      double sn = sc[0];
+      double wn = 0.0;
+      for (int k = tid; k < N2; k += blockDim.x) {
+        int ti = type_of(S, k >> 1);
+        double var = 2.0 * S.hbs2m[ti] * a.delta, vari = 1.0 / var;
+        double chi = bj.x[k] - m.x[k] - (-var * m.g[k]);
+        wn -= chi * chi * vari;
+      }
+      double wnew = block_sum(wn, m.red);
+      double p = 2 * (bj.p[QMC2D_JLTF] - pn[QMC2D_JLTF]) + 0.5 * (wnew - wold);
+      p = exp(fmin(0.0, fmax(-50.0, p)));
+      if (a.rejection == 0) p = 1.0;
+      else if (*bj.age == a.mage) p = 1.0;
+      if (*bj.s * sn < 0.0) p = 0.0;
+      double wg2 = a.delta * S.npnorm * (bj.p[QMC2D_JKIN0] + pn[QMC2D_JKIN0]);
+      double ua = u2(a.seed, 0xFFFFFFFEu, (uint32_t)r, t, c3).x;
+      bool rej = p < ua;
+      __syncthreads();
+      Bead ba = idir == 1 ? bj : bn, bb = idir == 1 ? bn : bj;
+      if (rej) {
+        if (tid == 0) {
+          ba.w[JDTP] = 0.5 * dold;
+          ba.w[JBRA] = -a.delta * S.npnorm * (fgg(a, bj.p[QMC2D_JETOT], bj.p[QMC2D_JGG]) - a.etrial);
+          bb.w[JITP] = 0.5 * dold;
+          ba.w[JLNG] = 0.5 * wg2;
+          double nds = 0.0;
+          for (int tt = 0; tt < nt; tt++) {
+            int ju = QMC2D_JUN(nt, tt);
+            double var = 2.0 * S.hbs2m[tt] * a.delta;
+            nds -= log(1.0 - exp(-bj.p[ju] * bj.p[ju] / (0.5 * var)));
+          }
+          ba.w[JNDS] = nds;
+          *bn.age = *bj.age + 1.0;
+          *bn.s = *bj.s;
+          for (int tt = 0; tt < nt; tt++) bn.h[tt] = bj.h[tt];
+        }
+        for (int k = tid; k < N2; k += blockDim.x) {
+          bn.x[k] = bj.x[k];
+          bn.g[k] = bj.g[k];
+        }
+        for (int k = tid; k < S.nprops; k += blockDim.x) bn.p[k] = bj.p[k];
+      } else {
+        lng += wg2;
+        if (tid == 0) {
+          ba.w[JDTP] = idir == 1 ? 0.5 * wold : 0.5 * wnew;
+          ba.w[JBRA] = -0.5 * a.delta * S.npnorm *
+                       ((fgg(a, bj.p[QMC2D_JETOT], bj.p[QMC2D_JGG]) +
+                         fgg(a, pn[QMC2D_JETOT], pn[QMC2D_JGG])) -
+                        2.0 * a.etrial);
+          bb.w[JITP] = idir == 1 ? 0.5 * wnew : 0.5 * wold;
+          ba.w[JLNG] = 0.5 * lng;
+          double nds = 0.0;
+          for (int tt = 0; tt < nt; tt++) {
+            int ju = QMC2D_JUN(nt, tt);
+            double var = 2.0 * S.hbs2m[tt] * a.delta;
+            nds -= log(1.0 - exp(-bj.p[ju] * pn[ju] / (0.5 * var)));
+          }
+          ba.w[JNDS] = nds;
+          *bn.age = 0.0;
+          *bn.s = sn;
+          for (int tt = 0; tt < nt; tt++) bn.h[tt] = hn[tt];
+        }
+        for (int k = tid; k < N2; k += blockDim.x) {
+          bn.x[k] = m.x[k];
+          bn.g[k] = m.g[k];
+        }
+        for (int k = tid; k < S.nprops; k += blockDim.x) bn.p[k] = pn[k];
+      }
+      __syncthreads();
+      if (tid == 0) bn.p[QMC2D_JACC] = p;
+      __syncthreads();
+    }
+    int kfirst = (jfirst + idir * ndelta + nb) % nb;
+    int klast = (jlast + idir * ndelta + nb) % nb;
+    path_props(S, a, r, kfirst, klast, pp);
+    double wnew = 0.0;
+    if (tid == 0) {
+      auto P = [&](int j) { return bead(S, a, r, j); };
+      wnew = (-P(kfirst).p[QMC2D_JLTF] * (1 + 2 * mezzo) - P(klast).p[QMC2D_JLTF] * (1 - 2 * mezzo) +
+              P(jfirst).p[QMC2D_JLTF] * (1 + 2 * mezzo) + P(jlast).p[QMC2D_JLTF] * (1 - 2 * mezzo));
+      if (idir == 1) {
+        for (int idelta = 1; idelta <= ndelta; idelta++) {
+          int j = (jfirst + idir * (idelta - 1) + nb) % nb;
+          int jn = (jfirst + idir * idelta + nb) % nb;
+          double *wj = P(j).w, *wn = P(jn).w;
+          wnew = wnew - wj[JBRA] - wj[JDTP] * (half + mezzo) + wn[JITP] * (one + half + mezzo) -
+                 wj[JLNG] * one + wj[JNDS] * one_nds;
+        }
+        for (int idelta = 1; idelta <= ndelta; idelta++) {
+          int j = (jlast + idir * (idelta - 1) + nb) % nb;
+          int jn = (jlast + idir * idelta + nb) % nb;
+          double *wj = P(j).w, *wn = P(jn).w;
+          wnew = wnew + wj[JBRA] - wj[JDTP] * (one + half - mezzo) + wn[JITP] * (half - mezzo) +
+                 wj[JLNG] * one - wj[JNDS] * one_nds;
+        }
+      } else {
+        for (int idelta = 1; idelta <= ndelta; idelta++) {
+          int j = (jlast + idir * (idelta - 1) + nb) % nb;
+          int jn = (jlast + idir * idelta + nb) % nb;
+          double *wj = P(j).w, *wn = P(jn).w;
+          wnew = wnew - wn[JBRA] + wn[JDTP] * (one + half - mezzo) - wj[JITP] * (half - mezzo) -
+                 wn[JLNG] * one + wn[JNDS] * one_nds;
+        }
+        for (int idelta = 1; idelta <= ndelta; idelta++) {
+          int j = (jfirst + idir * (idelta - 1) + nb) % nb;
+          int jn = (jfirst + idir * idelta + nb) % nb;
+          double *wj = P(j).w, *wn = P(jn).w;
+          wnew = wnew + wn[JBRA] + wn[JDTP] * (half + mezzo) - wj[JITP] * (one + half + mezzo) +
+                 wn[JLNG] * one - wn[JNDS] * one_nds;
+        }
+      }
+      sc[1] = wnew;
+    }
+    __syncthreads();
+    wnew = sc[1];
+    // reptation_metropolis_test (reptation.f:1865-1895)
+    double p = (age == a.mage_r) ? 1.0 : exp(fmin(0.0, fmax(-50.0, wnew)));
+    double ua = u2(a.seed, 0xFFFFFFFDu, (uint32_t)r, t, 2u).x;
+    if (p >= ua) {
+      jfirst = kfirst;
+      jlast = klast;
+      for (int ip = tid; ip < S.nprops; ip += blockDim.x) ppo[ip] = pp[ip];
+      age = 0.0;
+      nacc += 1.0;
+    } else {
+      age += 1.0;
+    }
+    __syncthreads();
+    for (int ip = tid; ip < S.nprops; ip += blockDim.x) blk[ip] += ppo[ip];
+    norm += 1.0;
+    __syncthreads();
+  }
+  for (int ip = tid; ip < S.nprops; ip += blockDim.x) {
+    a.pp_old[(size_t)r * S.nprops + ip] = ppo[ip];
+    a.blk[(size_t)r * S.nprops + ip] = blk[ip];
+  }
+  if (tid == 0) {
+    a.ends[2 * r] = jfirst;
+    a.ends[2 * r + 1] = jlast;
+    a.age[r] = age;
+    a.blk_norm[r] = norm;
+    a.cnt[4 * r] += nacc;
+    a.cnt[4 * r + 1] += a.nstp;
+    a.status[r] |= status;
+  }
+}
+
+}  // namespace
+
+void rmc_free(RmcState *r) {
+  void *b[] = {r->x, r->g, r->p, r->h, r->s, r->age_stack, r->w, r->ends, r->pp_old, r->age};
+  for (void *p : b) cudaFree(p);
+  *r = RmcState{};
+}
+
+}  // namespace q2d
+
+// ----------------------------------------------------------------- C-ABI
+#include <string>
+#include <vector>
+
+#include "handle.h"
+
+namespace {
+
+int rfail(cudaError_t e, const char *what) {
+  q2d::set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return QMC2D_ERR_CUDA;
+}
+
+#define RCK(call)                                   \
+  do {                                              \
+    cudaError_t e_ = (call);                        \
+    if (e_ != cudaSuccess) return rfail(e_, #call); \
+  } while (0)
+
+q2d::RmcArgs rmc_args(qmc2d_handle *h, int nstp) {
+  q2d::RmcState &r = h->rmc;
+  q2d::RmcArgs a{};
+  a.nrep = r.nrep;
+  a.ntau = r.ntau;
+  a.ntauskip = r.ntauskip;
+  a.mdelta = r.mdelta;
+  a.nbuf = r.nbuf;
+  a.nstp = nstp;
+  a.delta = r.delta;
+  a.etrial = r.etrial;
+  a.mage = r.mage;
+  a.mage_r = r.mage_r;
+  a.seed = h->seed;
+  a.step0 = r.step;
+  a.ecut = h->hs.ecut;
+  a.value_ecut = h->hs.value_ecut;
+  a.rejection = h->hs.rejection;
+  a.wpiu = h->hs.wpiu;
+  a.gstorto = h->hs.gstorto;
+  a.nodalaction = h->hs.nodalaction;
+  a.x = r.x;
+  a.g = r.g;
+  a.p = r.p;
+  a.h = r.h;
+  a.s = r.s;
+  a.age_stack = r.age_stack;
+  a.w = r.w;
+  a.pp_old = r.pp_old;
+  a.age = r.age;
+  a.ends = r.ends;
+  a.blk = h->d_blk;
+  a.blk_norm = h->d_norm;
+  a.cnt = h->d_cnt;
+  a.status = h->d_status;
+  return a;
+}
+
+size_t rmc_move_smem(const q2d::DevSys &s) {
+  return q2d::eval_carve(s, nullptr, nullptr) + sizeof(double) * (4 * (size_t)s.nprops + 16);
+}
+
+}  // namespace
+
+extern "C" int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params *prm,
+                              const double *x) {
+  if (!h || !prm || !x || nrep <= 0 || nrep > h->cap || prm->ntau < 2 || prm->mdelta < 1 ||
+      prm->ntau - 2 * prm->ntauskip < 1 || !(prm->delta > 0.0)) {
+    q2d::set_error("qmc2d_rmc_init: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  RCK(cudaSetDevice(h->device));
+  RCK(cudaStreamSynchronize(h->stream));
+  q2d::rmc_free(&h->rmc);
+  q2d::RmcState &r = h->rmc;
+  r.nrep = nrep;
+  r.ntau = prm->ntau;
+  r.ntauskip = prm->ntauskip;
+  r.mdelta = prm->mdelta;
+  r.nbuf = prm->ntau + prm->mdelta;
+  r.delta = prm->delta;
+  r.etrial = prm->etrial;
+  r.mage = prm->mage;
+  r.mage_r = prm->mage_r;
+  r.step = 0;
+  size_t nb = (size_t)nrep * r.nbuf;
+  int N = h->N, nt = h->nt, np = h->nprops;
+  RCK(cudaMalloc(&r.x, sizeof(double) * nb * 2 * N));
+  RCK(cudaMalloc(&r.g, sizeof(double) * nb * 2 * N));
+  RCK(cudaMalloc(&r.p, sizeof(double) * nb * np));
+  RCK(cudaMalloc(&r.h, sizeof(double) * nb * nt));
+  RCK(cudaMalloc(&r.s, sizeof(double) * nb));
+  RCK(cudaMalloc(&r.age_stack, sizeof(double) * nb));
+  RCK(cudaMalloc(&r.w, sizeof(double) * nb * 5));
+  RCK(cudaMalloc(&r.ends, sizeof(int) * 2 * nrep));
+  RCK(cudaMalloc(&r.pp_old, sizeof(double) * nrep * np));
+  RCK(cudaMalloc(&r.age, sizeof(double) * nrep));
+  RCK(cudaMemsetAsync(r.w, 0, sizeof(double) * nb * 5, h->stream));
+  RCK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * h->cap, h->stream));
+  double *dx = nullptr;
+  size_t nx = (size_t)nrep * r.ntau * 2 * N;
+  RCK(cudaMalloc(&dx, sizeof(double) * nx));
+  RCK(cudaMemcpyAsync(dx, x, sizeof(double) * nx, cudaMemcpyHostToDevice, h->stream));
+  q2d::RmcArgs a = rmc_args(h, 0);
+  size_t sm = q2d::eval_smem_bytes(h->hs);
+  RCK(cudaFuncSetAttribute((const void *)q2d::rmc_eval_beads_kernel,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  q2d::rmc_eval_beads_kernel<<<nrep * r.ntau, q2d::kThreads, sm, h->stream>>>(h->ds, a, dx);
+  RCK(cudaGetLastError());
+  q2d::rmc_init_kernel<<<nrep, q2d::kThreads, sizeof(double) * np, h->stream>>>(h->ds, a);
+  RCK(cudaGetLastError());
+  RCK(cudaStreamSynchronize(h->stream));
+  cudaFree(dx);
+  h->nw = 0;
+  return q2d_sync_status(h, nrep);
+}
+
+extern "C" int qmc2d_rmc(qmc2d_handle *h, int nstp) {
+  if (!h || nstp < 0) return QMC2D_ERR_ARG;
+  if (h->rmc.nrep <= 0) {
+    q2d::set_error("qmc2d_rmc: no reptiles (call qmc2d_rmc_init)");
+    return QMC2D_ERR_STACK;
+  }
+  if (nstp == 0) return QMC2D_OK;
+  RCK(cudaSetDevice(h->device));
+  RCK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * h->rmc.nrep, h->stream));
+  q2d::RmcArgs a = rmc_args(h, nstp);
+  size_t sm = rmc_move_smem(h->hs);
+  RCK(cudaFuncSetAttribute((const void *)q2d::rmc_move_kernel,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  q2d::rmc_move_kernel<<<h->rmc.nrep, q2d::kThreads, sm, h->stream>>>(h->ds, a);
+  RCK(cudaGetLastError());
+  h->rmc.step += (uint32_t)nstp;
+  return q2d_sync_status(h, h->rmc.nrep);
+}
+
+extern "C" int qmc2d_rmc_get_path(qmc2d_handle *h, int rep, double *x, double *props) {
+  if (!h || rep < 0 || rep >= h->rmc.nrep) return QMC2D_ERR_ARG;
+  RCK(cudaSetDevice(h->device));
+  RCK(cudaStreamSynchronize(h->stream));
+  q2d::RmcState &r = h->rmc;
+  int ends[2];
+  RCK(cudaMemcpy(ends, r.ends + 2 * rep, sizeof(int) * 2, cudaMemcpyDeviceToHost));
+  size_t N2 = 2 * (size_t)h->N, np = h->nprops;
+  for (int i = 0; i < r.ntau; i++) {
+    size_t b = (size_t)rep * r.nbuf + (ends[0] + i) % r.nbuf;
+    if (x) RCK(cudaMemcpy(x + i * N2, r.x + b * N2, sizeof(double) * N2, cudaMemcpyDeviceToHost));
+    if (props)
+      RCK(cudaMemcpy(props + i * np, r.p + b * np, sizeof(double) * np, cudaMemcpyDeviceToHost));
+  }
+  return QMC2D_OK;
+}

@@ -31,6 +31,10 @@
 extern "C" {
 #endif
 
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
 /* ---------------------------------------------------------------- status */
 enum qmc2d_status {
   QMC2D_OK = 0,
@@ -232,6 +236,10 @@ int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params *prm,
 int qmc2d_rmc(qmc2d_handle *h, int nstp);
 /* Copy reptile r's path (ntau beads, x then props) out. */
 int qmc2d_rmc_get_path(qmc2d_handle *h, int r, double *x, double *props);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 
 #ifdef __cplusplus
 }
