@@ -146,10 +146,49 @@ class Handle:
         nw, N, np_ = self.population_size(), self.system.N, self.system.nprops
         x = np.zeros((nw, 2 * N))
         g = np.zeros((nw, 2 * N))
+        hl = np.zeros((nw, self.system.ntypes))
         p = np.zeros((nw, np_))
+        s = np.zeros(nw)
         age = np.zeros(nw)
-        self._chk(self.lib.qmc2d_population_get(self.h, _pd(x), _pd(g), _pd(p), _pd(age)))
-        return dict(x=x, g=g, p=p, age=age)
+        self._chk(self.lib.qmc2d_population_get(self.h, _pd(x), _pd(g), _pd(hl), _pd(p), _pd(s),
+                                                _pd(age)))
+        return dict(x=x, g=g, h=hl, p=p, s=s, age=age)
+
+    def population_get_ptr(self, x, g, hl, p, s, age):
+        """Copy out into caller buffers given as raw addresses (e.g. pinned memory)."""
+        c = ctypes.cast
+        self._chk(self.lib.qmc2d_population_get(self.h, c(x, _capi.PD), c(g, _capi.PD),
+                                                c(hl, _capi.PD), c(p, _capi.PD),
+                                                c(s, _capi.PD), c(age, _capi.PD)))
+
+    def population_load_ptr(self, nw, x, g, hl, p, s, age):
+        """Load walker records from raw host addresses (putconf for a population)."""
+        self._chk(self.lib.qmc2d_population_load(self.h, nw, x, g, hl, p, s, age))
+
+    def stream(self):
+        st = ctypes.c_void_p()
+        self._chk(self.lib.qmc2d_stream(self.h, ctypes.byref(st)))
+        return st.value
+
+    def profile(self, enable=True):
+        self._chk(self.lib.qmc2d_profile(self.h, 1 if enable else 0))
+
+    PHASES = ("propose", "pairs", "rhok", "u3", "orbitals", "invert", "fmat", "drift",
+              "mbuild", "cross", "assemble", "accept")
+
+    def phase_timers(self, enable=True):
+        """Start (enable) or stop and return {phase: SM cycles summed over CTAs}."""
+        buf = (ctypes.c_ulonglong * 16)()
+        self._chk(self.lib.qmc2d_phase_timers(self.h, 1 if enable else 0, buf))
+        if enable:
+            return None
+        return {name: int(buf[i]) for i, name in enumerate(self.PHASES)}
+
+    def profile_get(self, kernel):
+        ms = ctypes.c_double()
+        n = ctypes.c_long()
+        self._chk(self.lib.qmc2d_profile_get(self.h, kernel, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
 
     def block_reset(self):
         self._chk(self.lib.qmc2d_block_reset(self.h))

@@ -28,6 +28,9 @@ ERR_POPULATION = 9
 ERR_LIMIT = 10
 ERR_STACK = 11
 
+# kernels for qmc2d_profile_get
+KERNEL_MOVE, KERNEL_BRANCH, KERNEL_GATHER, KERNEL_EVAL, KERNEL_RMC = range(5)
+
 # property indices (0-based; reptation.f:577-637)
 JETOT, JLTF, JACC, JPOT0, JKIN0, JE2, JGG = range(7)
 
@@ -157,7 +160,13 @@ SIGNATURES = {
                                              c_void_p, c_void_p, c_void_p]),
     "qmc2d_population_set": (c_int, [c_void_p, c_int, PD]),
     "qmc2d_population_size": (c_int, [c_void_p, POINTER(c_int)]),
-    "qmc2d_population_get": (c_int, [c_void_p, PD, PD, PD, PD]),
+    "qmc2d_population_get": (c_int, [c_void_p, PD, PD, PD, PD, PD, PD]),
+    "qmc2d_population_load": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                      c_void_p, c_void_p]),
+    "qmc2d_stream": (c_int, [c_void_p, POINTER(c_void_p)]),
+    "qmc2d_profile": (c_int, [c_void_p, c_int]),
+    "qmc2d_profile_get": (c_int, [c_void_p, c_int, PD, POINTER(ctypes.c_long)]),
+    "qmc2d_phase_timers": (c_int, [c_void_p, c_int, POINTER(ctypes.c_ulonglong)]),
     "qmc2d_block_reset": (c_int, [c_void_p]),
     "qmc2d_block_get": (c_int, [c_void_p, PD, PD]),
     "qmc2d_counters_get": (c_int, [c_void_p, POINTER(Counters)]),

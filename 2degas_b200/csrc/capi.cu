@@ -235,10 +235,65 @@ extern "C" int qmc2d_destroy(qmc2d_handle *h) {
   void *bufs[] = {h->ds, h->d_coef, h->d_kvec, h->d_gvec, h->d_blk, h->d_norm, h->d_cnt,
                   h->d_wate, h->d_status, h->br.delt, h->br.csum, h->br.mult, h->br.src,
                   h->br.ecum, h->br.zrank, h->br.ncapped, h->d_x, h->d_g, h->d_h, h->d_p,
-                  h->d_s};
+                  h->d_s, h->hs.phase};
   for (void *b : bufs) cudaFree(b);
+  for (int k = 0; k < QMC2D_NKERNELS; k++)
+    for (cudaEvent_t e : h->ev[k]) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_stream(qmc2d_handle *h, void **stream) {
+  if (!h || !stream) return QMC2D_ERR_ARG;
+  *stream = (void *)h->stream;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_profile(qmc2d_handle *h, int enable) {
+  if (!h) return QMC2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  h->prof = enable != 0;
+  for (int k = 0; k < QMC2D_NKERNELS; k++) {
+    h->ev_used[k] = 0;
+    h->prof_ms[k] = 0.0;
+    h->prof_n[k] = 0;
+  }
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_phase_timers(qmc2d_handle *h, int enable, unsigned long long *cycles) {
+  if (!h) return QMC2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  if (enable) {
+    if (!h->hs.phase) CK(dalloc(&h->hs.phase, q2d::PH_COUNT));
+    CK(cudaMemset(h->hs.phase, 0, sizeof(unsigned long long) * q2d::PH_COUNT));
+  } else if (h->hs.phase) {
+    if (cycles)
+      CK(cudaMemcpy(cycles, h->hs.phase, sizeof(unsigned long long) * q2d::PH_COUNT,
+                    cudaMemcpyDeviceToHost));
+    cudaFree(h->hs.phase);
+    h->hs.phase = nullptr;
+  }
+  CK(cudaMemcpy(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice));
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_profile_get(qmc2d_handle *h, int kernel, double *ms, long *launches) {
+  if (!h || kernel < 0 || kernel >= QMC2D_NKERNELS) return QMC2D_ERR_ARG;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int i = 0; i < h->ev_used[kernel]; i++) {
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, h->ev[kernel][2 * i], h->ev[kernel][2 * i + 1]));
+    h->prof_ms[kernel] += t;
+    h->prof_n[kernel]++;
+  }
+  h->ev_used[kernel] = 0;
+  if (ms) *ms = h->prof_ms[kernel];
+  if (launches) *launches = h->prof_n[kernel];
   return QMC2D_OK;
 }
 
@@ -251,6 +306,7 @@ extern "C" int qmc2d_compute_properties_dev(qmc2d_handle *h, int nw, const doubl
   }
   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
   CK(cudaSetDevice(h->device));
+  ProfScope ps(h, QMC2D_KERNEL_EVAL, st);
   CK(q2d::launch_eval(h->hs, h->ds, nw, x_dev, g_dev, hl_dev, props_dev, s_dev, h->d_status,
                       st));
   return QMC2D_OK;
@@ -267,8 +323,11 @@ extern "C" int qmc2d_compute_properties(qmc2d_handle *h, int nw, const double *x
   size_t N2 = 2 * (size_t)h->N;
   CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * nw, h->stream));
   CK(cudaMemcpyAsync(h->d_x, x, sizeof(double) * N2 * nw, cudaMemcpyHostToDevice, h->stream));
-  CK(q2d::launch_eval(h->hs, h->ds, nw, h->d_x, h->d_g, h->d_h, h->d_p, h->d_s, h->d_status,
-                      h->stream));
+  {
+    ProfScope ps(h, QMC2D_KERNEL_EVAL, h->stream);
+    CK(q2d::launch_eval(h->hs, h->ds, nw, h->d_x, h->d_g, h->d_h, h->d_p, h->d_s, h->d_status,
+                        h->stream));
+  }
   if (g) CK(cudaMemcpyAsync(g, h->d_g, sizeof(double) * N2 * nw, cudaMemcpyDeviceToHost, h->stream));
   if (hl)
     CK(cudaMemcpyAsync(hl, h->d_h, sizeof(double) * h->nt * nw, cudaMemcpyDeviceToHost,
@@ -307,17 +366,43 @@ extern "C" int qmc2d_population_size(qmc2d_handle *h, int *nw) {
   return QMC2D_OK;
 }
 
-extern "C" int qmc2d_population_get(qmc2d_handle *h, double *x, double *g, double *props,
-                                    double *age) {
+extern "C" int qmc2d_population_get(qmc2d_handle *h, double *x, double *g, double *hl,
+                                    double *props, double *s, double *age) {
   if (!h) return QMC2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
-  CK(cudaStreamSynchronize(h->stream));
   q2d::DevPop &p = h->pop[h->cur];
   size_t N2 = 2 * (size_t)h->N, nw = h->nw;
-  if (x) CK(cudaMemcpy(x, p.x, sizeof(double) * N2 * nw, cudaMemcpyDeviceToHost));
-  if (g) CK(cudaMemcpy(g, p.g, sizeof(double) * N2 * nw, cudaMemcpyDeviceToHost));
-  if (props) CK(cudaMemcpy(props, p.p, sizeof(double) * h->nprops * nw, cudaMemcpyDeviceToHost));
-  if (age) CK(cudaMemcpy(age, p.age, sizeof(double) * nw, cudaMemcpyDeviceToHost));
+  cudaStream_t st = h->stream;
+  if (x) CK(cudaMemcpyAsync(x, p.x, sizeof(double) * N2 * nw, cudaMemcpyDeviceToHost, st));
+  if (g) CK(cudaMemcpyAsync(g, p.g, sizeof(double) * N2 * nw, cudaMemcpyDeviceToHost, st));
+  if (hl) CK(cudaMemcpyAsync(hl, p.h, sizeof(double) * h->nt * nw, cudaMemcpyDeviceToHost, st));
+  if (props)
+    CK(cudaMemcpyAsync(props, p.p, sizeof(double) * h->nprops * nw, cudaMemcpyDeviceToHost, st));
+  if (s) CK(cudaMemcpyAsync(s, p.s, sizeof(double) * nw, cudaMemcpyDeviceToHost, st));
+  if (age) CK(cudaMemcpyAsync(age, p.age, sizeof(double) * nw, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_population_load(qmc2d_handle *h, int nw, const double *x, const double *g,
+                                     const double *hl, const double *props, const double *s,
+                                     const double *age) {
+  if (!h || !x || !g || !hl || !props || !s || !age || nw <= 0 || nw > h->cap) {
+    q2d::set_error("qmc2d_population_load: bad argument or population outside capacity");
+    return QMC2D_ERR_POPULATION;
+  }
+  CK(cudaSetDevice(h->device));
+  q2d::DevPop &p = h->pop[h->cur];
+  size_t N2 = 2 * (size_t)h->N;
+  cudaStream_t st = h->stream;
+  CK(cudaMemcpyAsync(p.x, x, sizeof(double) * N2 * nw, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(p.g, g, sizeof(double) * N2 * nw, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(p.h, hl, sizeof(double) * h->nt * nw, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(p.p, props, sizeof(double) * h->nprops * nw, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(p.s, s, sizeof(double) * nw, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(p.age, age, sizeof(double) * nw, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));  // the caller may reuse its buffers on return
+  h->nw = nw;
   return QMC2D_OK;
 }
 
@@ -393,7 +478,10 @@ static int run_moves(qmc2d_handle *h, int nstp, int dmc, double delta, double et
     h->hs.delta = delta;
     CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
   }
-  CK(q2d::launch_moves(h->hs, h->ds, h->pop[h->cur], a, h->stream));
+  {
+    ProfScope ps(h, QMC2D_KERNEL_MOVE, h->stream);
+    CK(q2d::launch_moves(h->hs, h->ds, h->pop[h->cur], a, h->stream));
+  }
   h->move_counter += (uint32_t)nstp;
   return QMC2D_OK;
 }
@@ -423,9 +511,15 @@ extern "C" int qmc2d_dmc(qmc2d_handle *h, int nstp, int mmstep, double delta, do
   for (int gen = 0; gen < nstp; gen++) {
     int st = run_moves(h, mmstep, 1, delta, etrial, mmult, mage);
     if (st) return st;
-    CK(q2d::launch_branch(h->nw, h->d_wate, h->seed, h->gen_counter, h->br, h->stream));
+    {
+      ProfScope ps(h, QMC2D_KERNEL_BRANCH, h->stream);
+      CK(q2d::launch_branch(h->nw, h->d_wate, h->seed, h->gen_counter, h->br, h->stream));
+    }
     int nxt = 1 - h->cur;
-    CK(q2d::launch_gather(h->hs, h->pop[h->cur], h->pop[nxt], h->br.src, h->nw, h->stream));
+    {
+      ProfScope ps(h, QMC2D_KERNEL_GATHER, h->stream);
+      CK(q2d::launch_gather(h->hs, h->pop[h->cur], h->pop[nxt], h->br.src, h->nw, h->stream));
+    }
     h->cur = nxt;
     h->gen_counter++;
   }

@@ -37,6 +37,14 @@ struct DevSys {
   const double *coef;  // packed tables: ut rows (4 doubles each) and v_k lists
   const double *kvec;  // 2*nk
   const double *gvec;  // 2*ngvec
+  unsigned long long *phase;  // per-phase SM cycles (qmc2d_phase_timers), null when off
+};
+
+// Phases of one walker move timed by qmc2d_phase_timers.
+enum : int {
+  PH_PROPOSE = 0, PH_PAIRS = 1, PH_RHOK = 2, PH_U3 = 3, PH_ORBITALS = 4, PH_INVERT = 5,
+  PH_FMAT = 6, PH_DRIFT = 7, PH_MBUILD = 8, PH_CROSS = 9, PH_ASSEMBLE = 10, PH_ACCEPT = 11,
+  PH_COUNT = 16
 };
 
 // Walker population in HBM: one block of each field per walker slot

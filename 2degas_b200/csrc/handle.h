@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "../../include/qmc2d.h"
 #include "devsys.h"
@@ -27,6 +28,32 @@ struct qmc2d_handle {
   uint64_t seed = 0;
   uint32_t move_counter = 0, gen_counter = 0;
   q2d::RmcState rmc{};
+  // per-kernel CUDA-event timing (qmc2d_profile)
+  bool prof = false;
+  std::vector<cudaEvent_t> ev[QMC2D_NKERNELS];  // event pairs, reused
+  int ev_used[QMC2D_NKERNELS] = {0};
+  double prof_ms[QMC2D_NKERNELS] = {0};
+  long prof_n[QMC2D_NKERNELS] = {0};
+};
+
+// Bracket one launch of kernel k with an event pair when profiling is on.
+struct ProfScope {
+  qmc2d_handle *h;
+  int k, idx = -1;
+  cudaStream_t st;
+  ProfScope(qmc2d_handle *h_, int k_, cudaStream_t s) : h(h_), k(k_), st(s) {
+    if (!h->prof) return;
+    idx = h->ev_used[k]++;
+    while ((int)h->ev[k].size() < 2 * (idx + 1)) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      h->ev[k].push_back(e);
+    }
+    cudaEventRecord(h->ev[k][2 * idx], st);
+  }
+  ~ProfScope() {
+    if (idx >= 0) cudaEventRecord(h->ev[k][2 * idx + 1], st);
+  }
 };
 
 // Reads the per-walker status words of the first n slots; maps them to a

@@ -48,7 +48,7 @@ __device__ __forceinline__ void load_sys(DevSys &S, const DevSys *sp) {
 }
 
 // ---------------------------------------------------------------- eval
-__global__ void __launch_bounds__(kThreads) eval_kernel(const DevSys *sp, int nw,
+__global__ void __launch_bounds__(kThreads, 2) eval_kernel(const DevSys *sp, int nw,
                                                         const double *__restrict__ x, double *g,
                                                         double *hl, double *props, double *s,
                                                         int *status) {
@@ -65,7 +65,8 @@ __global__ void __launch_bounds__(kThreads) eval_kernel(const DevSys *sp, int nw
   const int N2 = 2 * S.N;
   for (int j = threadIdx.x; j < N2; j += blockDim.x) m.x[j] = x[(size_t)w * N2 + j];
   __syncthreads();
-  int st = eval_walker(S, m, hn, pn, sn);
+  long long tph = clock64();
+  int st = eval_walker(S, m, hn, pn, sn, tph);
   for (int j = threadIdx.x; j < N2; j += blockDim.x) g[(size_t)w * N2 + j] = m.g[j];
   for (int j = threadIdx.x; j < S.nprops; j += blockDim.x)
     props[(size_t)w * S.nprops + j] = pn[j];
@@ -110,7 +111,8 @@ size_t move_smem_bytes(const DevSys &s) {
   return eval_carve(s, nullptr, nullptr) + move_carve(s, nullptr, nullptr);
 }
 
-__global__ void __launch_bounds__(kThreads) move_kernel(const DevSys *sp, DevPop pop, MoveArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, DevPop pop,
+                                                           MoveArgs a) {
   __shared__ DevSys S;
   extern __shared__ __align__(16) char smem[];
   load_sys(S, sp);
@@ -139,6 +141,7 @@ __global__ void __launch_bounds__(kThreads) move_kernel(const DevSys *sp, DevPop
   int status = 0;
   const uint64_t seed = a.seed;
   const double pi = 3.141592653589793;
+  long long tph = clock64();
   for (int istp = 0; istp < a.nstp; istp++) {
     const uint32_t step = a.step0 + (uint32_t)istp;
     // proposal (move, reptation.f:4631-4646)
@@ -152,8 +155,9 @@ __global__ void __launch_bounds__(kThreads) move_kernel(const DevSys *sp, DevPop
       m.x[j] = chi + (-var * v.go[j]) + v.xo[j];
     }
     double wold = block_sum(wo, m.red);
+    phase_mark(S, PH_PROPOSE, tph);
     double sn = 1.0;
-    status |= eval_walker(S, m, v.hn, v.pn, &v.sc[0]);
+    status |= eval_walker(S, m, v.hn, v.pn, &v.sc[0], tph);
     sn = v.sc[0];
     // reverse move (reptation.f:4660-4674)
     double wn = 0.0;
@@ -205,6 +209,7 @@ __global__ void __launch_bounds__(kThreads) move_kernel(const DevSys *sp, DevPop
     __syncthreads();
     for (int j = tid; j < np; j += kThreads) v.blk[j] += v.po[j] * wgt;
     norm += wgt;
+    phase_mark(S, PH_ACCEPT, tph);
   }
   __syncthreads();
   for (int j = tid; j < N2; j += kThreads) {

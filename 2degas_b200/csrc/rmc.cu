@@ -181,7 +181,7 @@ __global__ void rmc_init_kernel(const DevSys *sp, RmcArgs a) {
   }
 }
 
-__global__ void __launch_bounds__(kThreads) rmc_eval_beads_kernel(const DevSys *sp, RmcArgs a,
+__global__ void __launch_bounds__(kThreads, 2) rmc_eval_beads_kernel(const DevSys *sp, RmcArgs a,
                                                                   const double *x) {
   __shared__ DevSys S;
   extern __shared__ __align__(16) char smem[];
@@ -200,7 +200,8 @@ __global__ void __launch_bounds__(kThreads) rmc_eval_beads_kernel(const DevSys *
     b.x[k] = v;
   }
   __syncthreads();
-  int st = eval_walker(S, m, hn, pn, sn);
+  long long tph = clock64();
+  int st = eval_walker(S, m, hn, pn, sn, tph);
   for (int k = threadIdx.x; k < N2; k += blockDim.x) b.g[k] = m.g[k];
   for (int k = threadIdx.x; k < S.nprops; k += blockDim.x) b.p[k] = pn[k];
   if (threadIdx.x == 0) {
@@ -210,7 +211,7 @@ __global__ void __launch_bounds__(kThreads) rmc_eval_beads_kernel(const DevSys *
   }
 }
 
-__global__ void __launch_bounds__(kThreads) rmc_move_kernel(const DevSys *sp, RmcArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp, RmcArgs a) {
   __shared__ DevSys S;
   extern __shared__ __align__(16) char smem[];
   load_sys(S, sp);
@@ -269,7 +270,8 @@ __global__ void __launch_bounds__(kThreads) rmc_move_kernel(const DevSys *sp, Rm
       }
       double wold = block_sum(ww, m.red), dold = block_sum(dd, m.red);
       double lng = block_sum(wg, m.red);
-      status |= eval_walker(S, m, hn, pn, sc);
+      long long tph = clock64();
+      status |= eval_walker(S, m, hn, pn, sc, tph);
       double sn = sc[0];
       double wn = 0.0;
       for (int k = tid; k < N2; k += blockDim.x) {
@@ -556,7 +558,10 @@ extern "C" int qmc2d_rmc(qmc2d_handle *h, int nstp) {
   size_t sm = rmc_move_smem(h->hs);
   RCK(cudaFuncSetAttribute((const void *)q2d::rmc_move_kernel,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  q2d::rmc_move_kernel<<<h->rmc.nrep, q2d::kThreads, sm, h->stream>>>(h->ds, a);
+  {
+    ProfScope ps(h, QMC2D_KERNEL_RMC, h->stream);
+    q2d::rmc_move_kernel<<<h->rmc.nrep, q2d::kThreads, sm, h->stream>>>(h->ds, a);
+  }
   RCK(cudaGetLastError());
   h->rmc.step += (uint32_t)nstp;
   return q2d_sync_status(h, h->rmc.nrep);

@@ -18,12 +18,12 @@
 
 namespace {
 
-// Split one record into blank-separated words; only the first 80 columns
-// count, as in readwords (character*80 record).
+// Split one record of a table or k-vector file into blank-separated words.
+// List-directed reads see the whole record (only the keyword file's
+// readwords is limited to 80 columns).
 std::vector<std::string> words_of(const std::string &rec) {
-  std::string r = rec.substr(0, 80);
   std::vector<std::string> w;
-  std::istringstream is(r);
+  std::istringstream is(rec);
   std::string s;
   while (is >> s) w.push_back(s);
   return w;

@@ -13,12 +13,15 @@
 //     sum_j M_kj (G_k - G_j) and its Laplacian is
 //     sum_j (xi'' + 3 xi'/r) r_kj.(G_k - G_j) - tr(S_k^2) - sum_j tr(M_kj^2),
 //     S_k = sum_j M_kj: the dense dg/ddg of makeg/dotg are never formed.
-//   * determinant per spin: A(k,j) = exp(i g_k.q_j) in shared memory,
-//     Gauss-Jordan inversion with partial pivoting (log|det| from the
-//     pivots), F_a = A^-1 diag(i g_a) A, and the backflow cross term
-//     sum_{j,k} Re[(J_j.F(k,j))(J_k.F(j,k))] as the quadratic form of the
-//     symmetric 2n x 2n matrix M_ac(j,k) = Re[F_a(k,j) F_c(j,k)] against the
-//     Jacobian columns of every electron.
+//   * determinants: A(k,j) = exp(i g_k.q_j) for both spins at once; each
+//     spin's matrix is inverted by its own group of warps (Gauss-Jordan with
+//     partial pivoting, rows chosen in place instead of swapped, warp-level
+//     synchronisation only), while the remaining warps compute rho_k.
+//     Then, per spin, F_a = A^-1 diag(i g_a) A (register-tiled complex
+//     GEMM), the drift and the first two Laplacian terms, and the backflow
+//     cross term sum_{j,k} Re[(J_j.F(k,j))(J_k.F(j,k))] as the quadratic
+//     form of the symmetric 2n x 2n matrix M_ac(j,k) = Re[F_a(k,j) F_c(j,k)]
+//     against the Jacobian columns of every electron (register-tiled GEMM).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -31,13 +34,17 @@ struct EvalSmem {
   double *x, *g, *q, *G3, *S3, *Sb, *qbd, *lap, *ltf, *vp, *ph2;
   double *gd, *lapd, *ph2d;  // determinant contributions (added unless underflow)
   double *rhok;              // 2*nk per rhok slot
-  double2 *A, *Ai, *F0, *F1;
-  double *D2, *U, *red, *colk;
-  int *perm, *iscal;
-  double *dscal;
+  double2 *A[2], *W[2];      // per spin: orbitals (column-major) and the inversion workspace
+  double2 *F0, *F1;          // F_a of the spin being processed, column-major
+  double *D2, *U, *part, *red, *gsh, *dk[2];
+  int *perm[2], *used[2], *iscal, *gidx;
+  double *gval;
 };
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
+// Row stride of the inversion workspace: odd, so the rows that the lanes of
+// a warp own fall on distinct 16-byte bank groups.
+__host__ __device__ inline int ws_ld(int n) { return n | 1; }
 
 // Carve the dynamic shared memory; returns bytes used.
 __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSmem *m) {
@@ -47,7 +54,8 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
     off += align16(bytes);
     return p;
   };
-  int N = s.N, n = s.nmax > 0 ? s.nmax : 1;
+  int N = s.N, n = s.nmax > 0 ? s.nmax : 1, ld = ws_ld(n);
+  int nsp = s.nt;
   EvalSmem t;
   t.x = (double *)take(sizeof(double) * 2 * N);
   t.g = (double *)take(sizeof(double) * 2 * N);
@@ -64,19 +72,38 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
   t.lapd = (double *)take(sizeof(double) * N);
   t.ph2d = (double *)take(sizeof(double) * N);
   t.rhok = (double *)take(sizeof(double) * 2 * (s.nk > 0 ? s.nk : 1) * 2);
-  // A and Ai are contiguous so the 2n x 2n real matrix of the cross term can
-  // overlay them once F0/F1 are formed.
-  t.A = (double2 *)take(sizeof(double2) * 2 * n * n);
-  t.Ai = t.A ? t.A + n * n : nullptr;
-  t.F0 = (double2 *)take(sizeof(double2) * n * n);
-  t.F1 = (double2 *)take(sizeof(double2) * n * n);
-  t.D2 = (double *)take(sizeof(double) * 3 * n);
-  t.U = (double *)take(sizeof(double) * 2 * n * kChunk);
+  t.A[0] = t.A[1] = t.W[0] = t.W[1] = nullptr;
+  t.F0 = t.F1 = nullptr;
+  t.D2 = t.U = t.part = t.gsh = nullptr;
+  t.dk[0] = t.dk[1] = nullptr;
+  t.perm[0] = t.perm[1] = t.used[0] = t.used[1] = nullptr;
+  if (s.has_bf) {
+    // A[s] and W[s] are adjacent: the 2n x 2n real cross-term matrix of spin
+    // s overlays them once F0/F1 are formed.
+#pragma unroll
+    for (int sp = 0; sp < 2; sp++) {
+      if (sp >= nsp) continue;
+      t.A[sp] = (double2 *)take(sizeof(double2) * (n * n + n * ld));
+      t.W[sp] = t.A[sp] ? t.A[sp] + n * n : nullptr;
+      t.dk[sp] = (double *)take(sizeof(double) * n);
+      t.perm[sp] = (int *)take(sizeof(int) * n);
+      t.used[sp] = (int *)take(sizeof(int) * n);
+    }
+    // F0/F1 are dead once the cross-term matrix is built, so the cross
+    // term's Jacobian columns U and partial sums share their space.
+    size_t fbytes = sizeof(double2) * 2 * n * n;
+    size_t ubytes = sizeof(double) * (2 * n * kChunk + (n + 1) * kChunk);
+    t.F0 = (double2 *)take(fbytes > ubytes ? fbytes : ubytes);
+    t.F1 = t.F0 ? t.F0 + n * n : nullptr;
+    t.U = reinterpret_cast<double *>(t.F0);
+    t.part = t.U ? t.U + 2 * n * kChunk : nullptr;
+    t.D2 = (double *)take(sizeof(double) * 3 * n);
+    t.gsh = (double *)take(sizeof(double) * 2 * n);
+  }
   t.red = (double *)take(sizeof(double) * kThreads);
-  t.colk = (double *)take(sizeof(double2) * n);
-  t.perm = (int *)take(sizeof(int) * n);
   t.iscal = (int *)take(sizeof(int) * 8);
-  t.dscal = (double *)take(sizeof(double) * 16);
+  t.gidx = (int *)take(sizeof(int) * 16);
+  t.gval = (double *)take(sizeof(double) * 16);
   if (m) *m = t;
   return off;
 }
@@ -125,6 +152,25 @@ __device__ __forceinline__ void pair_geom(const DevSys &S, const double *x, int 
   byr = 1.0 / r;
 }
 
+// Backflow Jacobian dq_j/dx_i (2x2, symmetric) for j != i (qa of
+// slater_excitations, reptation.f:10093-10168): -(eta I + eta'/r r r^T).
+__device__ __forceinline__ void bf_offdiag(const DevSys &S, const double *x, int i, int j,
+                                           int tab, double &jxx, double &jxy, double &jyy,
+                                           double &qbx, double &qby) {
+  double rx, ry, r, byr, rem;
+  int ind;
+  pair_geom(S, x, i, j, rx, ry, r, byr, ind, rem);
+  double t, dt, ddt;
+  spline3(S, tab, ind, rem, t, dt, ddt);
+  double c = dt * byr;
+  jxx = -(t + c * rx * rx);
+  jxy = -(c * rx * ry);
+  jyy = -(t + c * ry * ry);
+  double w2 = c * 3.0 + ddt;  // div grad of eta(r) r, the qb term
+  qbx = -w2 * rx;
+  qby = -w2 * ry;
+}
+
 // Sum within aligned groups of 8 lanes; every lane of the warp must call it.
 __device__ __forceinline__ double group8_sum(double v) {
   v += __shfl_xor_sync(0xffffffffu, v, 4);
@@ -133,17 +179,41 @@ __device__ __forceinline__ double group8_sum(double v) {
   return v;
 }
 
-// Deterministic block sum; result valid in every thread. Uses red[0..8].
-__device__ __forceinline__ double block_sum(double v, double *red) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+// Deterministic block sum of K values at once; results valid in every
+// thread. Uses red[0 .. K*8).
+template <int K>
+__device__ __forceinline__ void block_sum_n(double (&v)[K], double *red) {
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
   int w = threadIdx.x >> 5, l = threadIdx.x & 31;
   __syncthreads();
-  if (l == 0) red[w] = v;
+  if (l == 0)
+#pragma unroll
+    for (int k = 0; k < K; k++) red[k * 8 + w] = v[k];
   __syncthreads();
-  double t = 0.0;
-  for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += red[k];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    double t = 0.0;
+    for (int ww = 0; ww < kThreads / 32; ww++) t += red[k * 8 + ww];
+    v[k] = t;
+  }
   __syncthreads();
-  return t;
+}
+
+__device__ __forceinline__ double block_sum(double v, double *red) {
+  double a[1] = {v};
+  block_sum_n<1>(a, red);
+  return a[0];
+}
+
+// Adds the SM cycles since t to phase k (thread 0 only, when timers are on).
+__device__ __forceinline__ void phase_mark(const DevSys &S, int k, long long &t) {
+  if (S.phase != nullptr && threadIdx.x == 0) {
+    long long now = clock64();
+    atomicAdd(&S.phase[k], (unsigned long long)(now - t));
+    t = now;
+  }
 }
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -151,13 +221,159 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 }
 __device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
 
+// ------------------------------------------------- Gauss-Jordan inversion
+//
+// In-place inversion of the n x n complex matrix W (row-major, row stride
+// ld) by a group of G warps (gt = 0 .. 32G-1 in the group). Step k pivots
+// on column k at the unused row p of largest |re|+|im| (izamax/dcabs1,
+// reptation.f:9079, 9219; ties go to the lowest row); the row is marked used
+// instead of swapped. With pi(k) the pivot row of step k, the inverse is
+//     A^-1(k, pi(c)) = W(pi(k), c),
+// and |det A| = prod_k |pivot_k|. perm[k] = pi(k), dk[k] = |pivot_k|^2.
+//
+// Work split: L lanes share a row (L = largest power of two <= 32G/n, at
+// most 8), each owning a contiguous slice of the columns; a thread owns at
+// most 4 rows. The elimination of a slice goes in register chunks of 8 so
+// the loads of a chunk are all in flight at once.
+constexpr int kGjMaxRows = 4;
+
+__device__ inline void gj_invert(double2 *W, int ld, int n, int *perm, double *dk, int *used,
+                                 int *singular, int gt, int G, int bar_id, double *gval,
+                                 int *gidx) {
+  const int nthr = 32 * G, lane = gt & 31, wg = gt >> 5;
+  int L = 1;
+  while (L < 8 && 2 * L * n <= nthr) L *= 2;
+  const int R = nthr / L;  // rows covered per pass
+  const int my_s = gt % L, my_r0 = gt / L;
+  const int h = (n + L - 1) / L;
+  const int c_lo = my_s * h, c_hi = min(n, c_lo + h);
+  auto gsync = [&]() {
+    if (G == 1) __syncwarp();
+    else asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthr) : "memory");
+  };
+  for (int r = gt; r < n; r += nthr) used[r] = 0;
+  gsync();
+  for (int k = 0; k < n; k++) {
+    // pivot search over the unused rows (slice-0 lanes)
+    double best = -1.0;
+    int bi = n;
+    if (my_s == 0)
+#pragma unroll
+      for (int i = 0; i < kGjMaxRows; i++) {
+        int r = my_r0 + i * R;
+        if (r < n && !used[r]) {
+          double v = cabs1(W[r * ld + k]);
+          if (v > best) {
+            best = v;
+            bi = r;
+          }
+        }
+      }
+    for (int o = 16; o > 0; o >>= 1) {
+      double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (G > 1) {
+      if (lane == 0) {
+        gval[wg] = best;
+        gidx[wg] = bi;
+      }
+      gsync();
+      best = gval[0];
+      bi = gidx[0];
+      for (int w = 1; w < G; w++)
+        if (gval[w] > best || (gval[w] == best && gidx[w] < bi)) {
+          best = gval[w];
+          bi = gidx[w];
+        }
+    }
+    const int p = bi < n ? bi : k;  // bi == n only if every candidate is NaN
+    const double2 piv = W[p * ld + k];
+    const double d = piv.x * piv.x + piv.y * piv.y;
+    const double rd = 1.0 / d;
+    const double2 inv = make_double2(piv.x * rd, -piv.y * rd);
+    // multipliers of my rows, read before anyone writes column k
+    double2 f[kGjMaxRows];
+#pragma unroll
+    for (int i = 0; i < kGjMaxRows; i++) {
+      int r = my_r0 + i * R;
+      f[i] = (r < n && r != p) ? W[r * ld + k] : make_double2(0.0, 0.0);
+    }
+    gsync();
+    if (gt == 0) {
+      perm[k] = p;
+      dk[k] = d;
+      used[p] = 1;
+      if (!(best > 0.0)) *singular = 1;
+    }
+    double2 *prow = W + p * ld;
+    for (int c = gt; c < n; c += nthr) prow[c] = (c == k) ? inv : cmul(prow[c], inv);
+    gsync();
+#pragma unroll
+    for (int i = 0; i < kGjMaxRows; i++) {
+      const int r = my_r0 + i * R;
+      if (r >= n || r == p) continue;
+      double2 *__restrict__ row = W + r * ld;
+      const double2 *__restrict__ pr = prow;
+      const double2 fi = f[i];
+      for (int c0 = c_lo; c0 < c_hi; c0 += 8) {
+        double2 a[8], v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          int c = min(c0 + u, c_hi - 1);
+          a[u] = pr[c];
+          v[u] = row[c];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          v[u].x -= fi.x * a[u].x - fi.y * a[u].y;
+          v[u].y -= fi.x * a[u].y + fi.y * a[u].x;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+          if (c0 + u < c_hi) row[c0 + u] = v[u];
+      }
+      if (k >= c_lo && k < c_hi) {
+        double2 v = cmul(fi, inv);
+        row[k] = make_double2(-v.x, -v.y);
+      }
+    }
+    gsync();
+  }
+}
+
+// rho_k per rhok slot (distances, reptation.f:4225-4243) by threads
+// t0 .. t0+nthr-1.
+__device__ inline void compute_rhok(const DevSys &S, const EvalSmem &m, int t, int nthr) {
+  for (int e = t; e < S.nt * S.nk; e += nthr) {
+    int ty = e / S.nk, k = e - ty * S.nk;
+    if (S.irhok[ty] == 0) continue;
+    double kx = __ldg(S.kvec + 2 * k), ky = __ldg(S.kvec + 2 * k + 1);
+    double c = 0.0, sn = 0.0;
+    for (int i = S.ipfrst[ty]; i < S.ipfrst[ty] + S.np[ty]; i++) {
+      double kr = kx * m.x[2 * i] + ky * m.x[2 * i + 1];
+      double sv, cv;
+      sincos(kr, &sv, &cv);
+      c += cv;
+      sn += sv;
+    }
+    int slot = S.irhok[ty] - 1;
+    m.rhok[2 * (slot * S.nk + k)] = c;
+    m.rhok[2 * (slot * S.nk + k) + 1] = sn;
+  }
+}
+
 // ---------------------------------------------------------- the evaluation
 //
 // Input: m.x holds the configuration. Output (in shared memory): m.g (drift
 // -grad ln psi), hl[nt] (-lap ln psi per type), props[nprops], *sign.
 // Returns a status word (ST_*), identical in all threads.
 __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl, double *props,
-                                  double *sign) {
+                                  double *sign, long long &tph) {
   const int tid = threadIdx.x;
   const int N = S.N, nt = S.nt;
   const int lane8 = tid & (kGroup - 1);
@@ -266,24 +482,8 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
       m.ph2d[i] = 0.0;
     }
   }
-  // ---- rho_k per rhok slot (distances, reptation.f:4225-4243)
-  for (int e = tid; e < nt * S.nk; e += kThreads) {
-    int t = e / S.nk, k = e - t * S.nk;
-    if (S.irhok[t] == 0) continue;
-    double kx = __ldg(S.kvec + 2 * k), ky = __ldg(S.kvec + 2 * k + 1);
-    double c = 0.0, sn = 0.0;
-    for (int i = S.ipfrst[t]; i < S.ipfrst[t] + S.np[t]; i++) {
-      double kr = kx * m.x[2 * i] + ky * m.x[2 * i + 1];
-      double sv, cv;
-      sincos(kr, &sv, &cv);
-      c += cv;
-      sn += sv;
-    }
-    int slot = S.irhok[t] - 1;
-    m.rhok[2 * (slot * S.nk + k)] = c;
-    m.rhok[2 * (slot * S.nk + k) + 1] = sn;
-  }
   __syncthreads();
+  phase_mark(S, PH_PAIRS, tph);
 
   // ---- pass B: u3 gradient and Laplacian from the G vectors.
   if (S.has_u3) {
@@ -322,136 +522,133 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
         m.ltf[k] -= 0.5 * (Gkx * Gkx + Gky * Gky);
       }
     }
+    __syncthreads();
+    phase_mark(S, PH_U3, tph);
   }
-  __syncthreads();
 
   // ---- backflow Slater determinants (slater_excitations, reptation.f:9967)
   int status = ST_OK;
   double logdet_sum = 0.0;
   if (S.has_bf) {
-    for (int sp = 0; sp < nt; sp++) {
-      const int n = S.np[sp], f0 = S.ipfrst[sp], nn = n * n;
-      // orbitals (paho_orbitals, reptation.f:10298-10315): A(k,j), column-major
-      for (int e = tid; e < nn; e += kThreads) {
-        int k = e % n, j = e / n;
-        double gkx = __ldg(S.gvec + 2 * k), gky = __ldg(S.gvec + 2 * k + 1);
-        double kr = m.q[2 * (f0 + j)] * gkx + m.q[2 * (f0 + j) + 1] * gky;
-        double sv, cv;
-        sincos(kr, &sv, &cv);
-        m.A[e] = make_double2(cv, sv);
-        m.Ai[e] = make_double2(cv, sv);
+    const int n = S.nmax;
+    // orbitals of both spins (paho_orbitals, reptation.f:10298-10315)
+    int tot = 0;
+    for (int sp = 0; sp < nt; sp++) tot += S.np[sp] * S.np[sp];
+    for (int e = tid; e < tot; e += kThreads) {
+      int sp = 0, ee = e;
+      if (nt > 1 && ee >= S.np[0] * S.np[0]) {
+        ee -= S.np[0] * S.np[0];
+        sp = 1;
       }
-      if (tid == 0) {
-        m.dscal[0] = 0.0;  // log|det|
-        m.iscal[1] = 0;    // singular flag
+      const int ns = S.np[sp], ld = ws_ld(ns), f0 = S.ipfrst[sp];
+      int k = ee % ns, j = ee / ns;
+      double gkx = __ldg(S.gvec + 2 * k), gky = __ldg(S.gvec + 2 * k + 1);
+      double kr = m.q[2 * (f0 + j)] * gkx + m.q[2 * (f0 + j) + 1] * gky;
+      double sv, cv;
+      sincos(kr, &sv, &cv);
+      (sp ? m.A[1] : m.A[0])[k + j * ns] = make_double2(cv, sv);
+      (sp ? m.W[1] : m.W[0])[k * ld + j] = make_double2(cv, sv);
+    }
+    for (int e = tid; e < 2 * n; e += kThreads) m.gsh[e] = __ldg(S.gvec + e);
+    if (tid < 2) m.iscal[tid] = 0;  // singular flags
+    __syncthreads();
+    phase_mark(S, PH_ORBITALS, tph);
+    // inversion by one group of warps per spin; rho_k on the other warps
+    {
+      // warps per spin: half the CTA for the inversions, the rest for rho_k
+      const int G = (kThreads / 32) / (2 * nt) > 0 ? (kThreads / 32) / (2 * nt) : 1;
+      const int w = tid >> 5;
+      if (w < G * nt) {
+        const int sp = w / G, gt = tid - sp * 32 * G;
+        const int ns = S.np[sp];
+        gj_invert(sp ? m.W[1] : m.W[0], ws_ld(ns), ns, sp ? m.perm[1] : m.perm[0],
+                  sp ? m.dk[1] : m.dk[0], sp ? m.used[1] : m.used[0], &m.iscal[sp], gt,
+                  G, 1 + sp, m.gval + 8 * sp, m.gidx + 8 * sp);
+      } else {
+        compute_rhok(S, m, tid - G * nt * 32, kThreads - G * nt * 32);
       }
       __syncthreads();
-      // Gauss-Jordan inversion with partial pivoting (pivot = first row of
-      // largest |re|+|im|, as izamax/dcabs1, reptation.f:9079, 9219).
-      for (int k = 0; k < n; k++) {
-        if (tid < 32) {
-          double best = -1.0;
-          int bi = k;
-          for (int r = k + tid; r < n; r += 32) {
-            double v = cabs1(m.Ai[r + k * n]);
-            if (v > best) {
-              best = v;
-              bi = r;
-            }
-          }
-          for (int o = 16; o > 0; o >>= 1) {
-            double ob = __shfl_xor_sync(0xffffffffu, best, o);
-            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ob > best || (ob == best && oi < bi)) {
-              best = ob;
-              bi = oi;
-            }
-          }
-          if (tid == 0) {
-            m.perm[k] = bi;
-            m.iscal[0] = bi;
-            if (!(best > 0.0)) m.iscal[1] = 1;
-          }
-        }
-        __syncthreads();
-        int p = m.iscal[0];
-        if (p != k)
-          for (int c = tid; c < n; c += kThreads) {
-            double2 a = m.Ai[k + c * n];
-            m.Ai[k + c * n] = m.Ai[p + c * n];
-            m.Ai[p + c * n] = a;
-          }
-        __syncthreads();
-        double2 piv = m.Ai[k + k * n];
-        double d = piv.x * piv.x + piv.y * piv.y;
-        double2 inv = make_double2(piv.x / d, -piv.y / d);
-        double2 *colk = reinterpret_cast<double2 *>(m.colk);
-        for (int r = tid; r < n; r += kThreads) colk[r] = m.Ai[r + k * n];
-        if (tid == 0) m.dscal[0] += 0.5 * log(d);
-        __syncthreads();
-        for (int c = tid; c < n; c += kThreads)
-          m.Ai[k + c * n] = (c == k) ? inv : cmul(m.Ai[k + c * n], inv);
-        __syncthreads();
-        for (int e = tid; e < nn; e += kThreads) {
-          int r = e % n, c = e / n;
-          if (r == k) continue;
-          double2 f = colk[r];
-          if (c == k) {
-            double2 v = cmul(f, inv);
-            m.Ai[e] = make_double2(-v.x, -v.y);
-          } else {
-            double2 a = m.Ai[k + c * n];
-            double2 v = m.Ai[e];
-            v.x -= f.x * a.x - f.y * a.y;
-            v.y -= f.x * a.y + f.y * a.x;
-            m.Ai[e] = v;
-          }
-        }
+      if (G * nt == kThreads / 32) {
+        compute_rhok(S, m, tid, kThreads);
         __syncthreads();
       }
-      // undo the row interchanges on the columns of the inverse
-      for (int k = n - 1; k >= 0; k--) {
-        int p = m.perm[k];
-        if (p != k)
-          for (int r = tid; r < n; r += kThreads) {
-            double2 a = m.Ai[r + k * n];
-            m.Ai[r + k * n] = m.Ai[r + p * n];
-            m.Ai[r + p * n] = a;
+    }
+    {
+      double ld_acc = 0.0;
+      for (int sp = 0; sp < nt; sp++)
+        for (int k = tid; k < S.np[sp]; k += kThreads)
+          ld_acc += 0.5 * log((sp ? m.dk[1] : m.dk[0])[k]);
+      logdet_sum = block_sum(ld_acc, m.red);
+      if (m.iscal[0] || m.iscal[1]) status |= ST_SINGULAR;
+    }
+    phase_mark(S, PH_INVERT, tph);
+
+    for (int sp = 0; sp < nt; sp++) {
+      const int ns = S.np[sp], ld = ws_ld(ns), f0 = S.ipfrst[sp];
+      const double2 *A = sp ? m.A[1] : m.A[0], *W = sp ? m.W[1] : m.W[0];
+      const int *pm = sp ? m.perm[1] : m.perm[0];
+      // F_a(l,j) = sum_k Ainv(l,k) (i g_k[a]) A(k,j) (zv, reptation.f:10189-10200)
+      // with Ainv(l, pi(c)) = W(pi(l), c): 2x2 (l,j) tiles per thread.
+      {
+        const int nh = (ns + 1) / 2;
+        for (int tile = tid; tile < nh * nh; tile += kThreads) {
+          const int l0 = 2 * (tile % nh), j0 = 2 * (tile / nh);
+          const bool l1ok = l0 + 1 < ns, j1ok = j0 + 1 < ns;
+          const double2 *w0 = W + pm[l0] * ld;
+          const double2 *w1 = W + pm[l1ok ? l0 + 1 : l0] * ld;
+          const double2 *a0c = A + j0 * ns;
+          const double2 *a1c = A + (j1ok ? j0 + 1 : j0) * ns;
+          double2 f0[2][2], f1[2][2];
+#pragma unroll
+          for (int u = 0; u < 2; u++)
+#pragma unroll
+            for (int v = 0; v < 2; v++) f0[u][v] = f1[u][v] = make_double2(0.0, 0.0);
+          for (int c = 0; c < ns; c++) {
+            const int pc = pm[c];
+            const double gx = m.gsh[2 * pc], gy = m.gsh[2 * pc + 1];
+            const double2 wv[2] = {w0[c], w1[c]};
+            const double2 av[2] = {a0c[pc], a1c[pc]};
+#pragma unroll
+            for (int u = 0; u < 2; u++)
+#pragma unroll
+              for (int v = 0; v < 2; v++) {
+                double2 pr = cmul(wv[u], av[v]);
+                f0[u][v].x -= gx * pr.y;
+                f0[u][v].y += gx * pr.x;
+                f1[u][v].x -= gy * pr.y;
+                f1[u][v].y += gy * pr.x;
+              }
           }
-        __syncthreads();
-      }
-      if (m.iscal[1]) status |= ST_SINGULAR;
-      logdet_sum += m.dscal[0];
-      // F_a(l,j) = sum_k Ainv(l,k) (i g_k[a]) A(k,j)  (zv, reptation.f:10189-10200)
-      for (int e = tid; e < nn; e += kThreads) {
-        int l = e % n, j = e / n;
-        double2 f0v = make_double2(0, 0), f1v = make_double2(0, 0);
-        for (int k = 0; k < n; k++) {
-          double2 pr = cmul(m.Ai[l + k * n], m.A[k + j * n]);
-          double gkx = __ldg(S.gvec + 2 * k), gky = __ldg(S.gvec + 2 * k + 1);
-          f0v.x -= gkx * pr.y;
-          f0v.y += gkx * pr.x;
-          f1v.x -= gky * pr.y;
-          f1v.y += gky * pr.x;
+#pragma unroll
+          for (int u = 0; u < 2; u++)
+#pragma unroll
+            for (int v = 0; v < 2; v++) {
+              int l = l0 + u, j = j0 + v;
+              if (l < ns && j < ns) {
+                m.F0[l + j * ns] = f0[u][v];
+                m.F1[l + j * ns] = f1[u][v];
+              }
+            }
         }
-        m.F0[e] = f0v;
-        m.F1[e] = f1v;
       }
       // D2(j)[ab] = Re sum_k Ainv(j,k) (-g_ka g_kb) A(k,j)  (ddzorb term)
-      for (int j = tid; j < n; j += kThreads) {
+      for (int j = tid; j < ns; j += kThreads) {
         double dxx = 0, dxy = 0, dyy = 0;
-        for (int k = 0; k < n; k++) {
-          double2 pr = cmul(m.Ai[j + k * n], m.A[k + j * n]);
-          double gkx = __ldg(S.gvec + 2 * k), gky = __ldg(S.gvec + 2 * k + 1);
-          dxx -= gkx * gkx * pr.x;
-          dxy -= gkx * gky * pr.x;
-          dyy -= gky * gky * pr.x;
+        const double2 *wj = W + pm[j] * ld;
+        for (int c = 0; c < ns; c++) {
+          const int pc = pm[c];
+          double pr = wj[c].x * A[pc + j * ns].x - wj[c].y * A[pc + j * ns].y;
+          double gx = m.gsh[2 * pc], gy = m.gsh[2 * pc + 1];
+          dxx -= gx * gx * pr;
+          dxy -= gx * gy * pr;
+          dyy -= gy * gy * pr;
         }
         m.D2[3 * j] = dxx;
         m.D2[3 * j + 1] = dxy;
         m.D2[3 * j + 2] = dyy;
       }
       __syncthreads();
+      phase_mark(S, PH_FMAT, tph);
       // drift, phase gradient and the first two Laplacian terms for every
       // electron i against this determinant (reptation.f:10201-10237).
       for (int base = 0; base < N; base += per_round) {
@@ -460,40 +657,26 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
         int ti = valid ? type_of(S, i) : 0;
         double zxr = 0, zxi = 0, zyr = 0, zyi = 0, t12 = 0;
         if (valid) {
-          for (int jl = lane8; jl < n; jl += kGroup) {
+          for (int jl = lane8; jl < ns; jl += kGroup) {
             int j = f0 + jl;
-            double jxx, jxy, jyx, jyy, qbx, qby;  // J[a][b] = dq_j[a]/dx_i[b]
+            double jxx, jxy, jyy, qbx, qby;  // J[a][b] = dq_j[a]/dx_i[b]
             if (j == i) {
               jxx = 1.0 + m.Sb[3 * i];
               jxy = m.Sb[3 * i + 1];
-              jyx = jxy;
               jyy = 1.0 + m.Sb[3 * i + 2];
               qbx = m.qbd[2 * i];
               qby = m.qbd[2 * i + 1];
             } else {
-              double rx, ry, r, byr, rem;
-              int ind;
-              pair_geom(S, m.x, i, j, rx, ry, r, byr, ind, rem);
-              double t, dt, ddt;
-              spline3(S, S.iub[ti][sp], ind, rem, t, dt, ddt);
-              double c = dt * byr;
-              jxx = -(t + c * rx * rx);
-              jxy = -(c * rx * ry);
-              jyx = jxy;
-              jyy = -(t + c * ry * ry);
-              double w2 = dt * byr * 3.0 + ddt;
-              qbx = -w2 * rx;
-              qby = -w2 * ry;
+              bf_offdiag(S, m.x, i, j, S.iub[ti][sp], jxx, jxy, jyy, qbx, qby);
             }
-            double2 fx = m.F0[jl + jl * n], fy = m.F1[jl + jl * n];
-            zxr += fx.x * jxx + fy.x * jyx;
-            zxi += fx.y * jxx + fy.y * jyx;
+            double2 fx = m.F0[jl + jl * ns], fy = m.F1[jl + jl * ns];
+            zxr += fx.x * jxx + fy.x * jxy;
+            zxi += fx.y * jxx + fy.y * jxy;
             zyr += fx.x * jxy + fy.x * jyy;
             zyi += fx.y * jxy + fy.y * jyy;
             t12 -= fx.x * qbx + fy.x * qby;
-            // (J^T J)[a][b]
-            double jtj_xx = jxx * jxx + jyx * jyx;
-            double jtj_xy = jxx * jxy + jyx * jyy;
+            double jtj_xx = jxx * jxx + jxy * jxy;
+            double jtj_xy = jxx * jxy + jxy * jyy;
             double jtj_yy = jxy * jxy + jyy * jyy;
             t12 -= m.D2[3 * jl] * jtj_xx + 2.0 * m.D2[3 * jl + 1] * jtj_xy +
                    m.D2[3 * jl + 2] * jtj_yy;
@@ -512,70 +695,82 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
         }
       }
       __syncthreads();
-      // cross term: M (2n x 2n, overlaying A and Ainv) then quadratic forms.
-      const int n2 = 2 * n;
-      double *M = reinterpret_cast<double *>(m.A);
+      phase_mark(S, PH_DRIFT, tph);
+      // cross term: M (2n x 2n over A[sp], W[sp]) then quadratic forms
+      const int n2 = 2 * ns;
+      double *M = reinterpret_cast<double *>(sp ? m.A[1] : m.A[0]);
       for (int e = tid; e < n2 * n2; e += kThreads) {
         int p = e % n2, qq = e / n2;
-        int a = p / n, j = p - a * n, c = qq / n, k = qq - c * n;
-        double2 fa = (a == 0 ? m.F0 : m.F1)[k + j * n];
-        double2 fc = (c == 0 ? m.F0 : m.F1)[j + k * n];
+        int a = p / ns, j = p - a * ns, c = qq / ns, k = qq - c * ns;
+        double2 fa = (a == 0 ? m.F0 : m.F1)[k + j * ns];
+        double2 fc = (c == 0 ? m.F0 : m.F1)[j + k * ns];
         M[e] = fa.x * fc.x - fa.y * fc.y;
       }
       __syncthreads();
+      phase_mark(S, PH_MBUILD, tph);
+      const int nrt = ns;  // row tiles of 2 rows over n2 = 2 ns rows
       for (int i0 = 0; i0 < N; i0 += kChunk / 2) {
         // U[(a,j)][(i,b)] = J_{j,i}[a][b] for electrons i0 .. i0+15
-        for (int e = tid; e < n * (kChunk / 2); e += kThreads) {
-          int jl = e % n, il = e / n;
+        for (int e = tid; e < ns * (kChunk / 2); e += kThreads) {
+          int jl = e % ns, il = e / ns;
           int i = i0 + il, j = f0 + jl;
-          double jxx = 0, jxy = 0, jyy = 0;
+          double jxx = 0, jxy = 0, jyy = 0, qbx, qby;
           if (i < N) {
             if (j == i) {
               jxx = 1.0 + m.Sb[3 * i];
               jxy = m.Sb[3 * i + 1];
               jyy = 1.0 + m.Sb[3 * i + 2];
             } else {
-              double rx, ry, r, byr, rem;
-              int ind;
-              pair_geom(S, m.x, i, j, rx, ry, r, byr, ind, rem);
-              double t, dt, ddt;
-              spline3(S, S.iub[type_of(S, i)][sp], ind, rem, t, dt, ddt);
-              double c = dt * byr;
-              jxx = -(t + c * rx * rx);
-              jxy = -(c * rx * ry);
-              jyy = -(t + c * ry * ry);
+              bf_offdiag(S, m.x, i, j, S.iub[type_of(S, i)][sp], jxx, jxy, jyy, qbx, qby);
             }
           }
-          m.U[(0 * n + jl) * kChunk + 2 * il + 0] = jxx;  // a=x, b=x
-          m.U[(0 * n + jl) * kChunk + 2 * il + 1] = jxy;  // a=x, b=y
-          m.U[(1 * n + jl) * kChunk + 2 * il + 0] = jxy;  // a=y, b=x
-          m.U[(1 * n + jl) * kChunk + 2 * il + 1] = jyy;  // a=y, b=y
+          m.U[(0 * ns + jl) * kChunk + 2 * il + 0] = jxx;  // a=x, b=x
+          m.U[(0 * ns + jl) * kChunk + 2 * il + 1] = jxy;  // a=x, b=y
+          m.U[(1 * ns + jl) * kChunk + 2 * il + 0] = jxy;  // a=y, b=x
+          m.U[(1 * ns + jl) * kChunk + 2 * il + 1] = jyy;  // a=y, b=y
         }
         __syncthreads();
-        {
-          int col = tid & (kChunk - 1), rg = tid / kChunk;
-          const int nrg = kThreads / kChunk;
-          double part = 0.0;
-          for (int p = rg; p < n2; p += nrg) {
-            double y = 0.0;
-            for (int qq = 0; qq < n2; qq++) y += M[p + qq * n2] * m.U[qq * kChunk + col];
-            part += m.U[p * kChunk + col] * y;
+        // Y = M U in 2-row x 4-column register tiles; each tile's rows dot
+        // their own U rows into part[row tile][column].
+        for (int tile = tid; tile < nrt * (kChunk / 4); tile += kThreads) {
+          const int p0 = 2 * (tile / (kChunk / 4)), c0 = 4 * (tile % (kChunk / 4));
+          double y0[4] = {0, 0, 0, 0}, y1[4] = {0, 0, 0, 0};
+          const double *Mp = M + p0;
+          for (int qq = 0; qq < n2; qq++) {
+            const double2 mm = *reinterpret_cast<const double2 *>(Mp + qq * n2);
+            const double2 ua = *reinterpret_cast<const double2 *>(m.U + qq * kChunk + c0);
+            const double2 ub = *reinterpret_cast<const double2 *>(m.U + qq * kChunk + c0 + 2);
+            y0[0] += mm.x * ua.x;
+            y0[1] += mm.x * ua.y;
+            y0[2] += mm.x * ub.x;
+            y0[3] += mm.x * ub.y;
+            y1[0] += mm.y * ua.x;
+            y1[1] += mm.y * ua.y;
+            y1[2] += mm.y * ub.x;
+            y1[3] += mm.y * ub.y;
           }
-          m.red[rg * kChunk + col] = part;
+          const double *u0 = m.U + p0 * kChunk + c0, *u1 = u0 + kChunk;
+#pragma unroll
+          for (int v = 0; v < 4; v++) m.part[(p0 / 2) * kChunk + c0 + v] = u0[v] * y0[v] + u1[v] * y1[v];
         }
         __syncthreads();
         if (tid < kChunk / 2) {
           int i = i0 + tid;
           if (i < N) {
             double t3 = 0.0;
-            for (int rg = 0; rg < kThreads / kChunk; rg++)
-              t3 += m.red[rg * kChunk + 2 * tid] + m.red[rg * kChunk + 2 * tid + 1];
+            for (int rt = 0; rt < nrt; rt++)
+              t3 += m.part[rt * kChunk + 2 * tid] + m.part[rt * kChunk + 2 * tid + 1];
             m.lapd[i] += t3;
           }
         }
         __syncthreads();
       }
+      phase_mark(S, PH_CROSS, tph);
     }
+  } else {
+    compute_rhok(S, m, tid, kThreads);
+    __syncthreads();
+    phase_mark(S, PH_RHOK, tph);
   }
 
   // ---- assemble: -ln psi, kinetic (reptation.f:2729), potential (:3986)
@@ -586,85 +781,110 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
   bool underflow = false;
   if (S.has_bf && S.ref_underflow) underflow = exp(-ltf * 2.0) <= 0.0;
   if (underflow) status |= ST_UNDERFLOW;
-  if (S.has_bf && !underflow) {
-    for (int i = tid; i < N; i += kThreads) {
-      m.g[2 * i] += m.gd[2 * i];
-      m.g[2 * i + 1] += m.gd[2 * i + 1];
-      m.lap[i] += m.lapd[i];
-      m.ph2[i] = m.ph2d[i];
+  // determinant terms and the drift cutoff (kinetic, reptation.f:2748-2763)
+  double gga = 0.0;
+  for (int i = tid; i < N; i += kThreads) {
+    double gx = m.g[2 * i], gy = m.g[2 * i + 1], lp = m.lap[i], ph = 0.0;
+    if (S.has_bf && !underflow) {
+      gx += m.gd[2 * i];
+      gy += m.gd[2 * i + 1];
+      lp += m.lapd[i];
+      ph = m.ph2d[i];
     }
-  }
-  __syncthreads();
-  // drift cutoff (kinetic, reptation.f:2748-2763)
-  double ngg = 0.0, ggsum = 0.0;
-  if (S.adrift != 0.0) {
-    for (int i = tid; i < N; i += kThreads) {
+    double x2 = gx * gx + gy * gy;
+    if (S.adrift != 0.0) {
       int ti = type_of(S, i);
       double vari = 1.0 / (2.0 * S.hbs2m[ti] * S.delta);
-      double x2 = m.g[2 * i] * m.g[2 * i] + m.g[2 * i + 1] * m.g[2 * i + 1];
       double gg = x2 * S.adrift * S.delta * S.delta * vari;
       gg = (-1.0 + sqrt(1.0 + 2.0 * gg)) / gg;
-      ggsum += gg;
-      m.ph2d[i] = x2;  // raw |g|^2 for the kinetic energy
-      m.g[2 * i] *= gg;
-      m.g[2 * i + 1] *= gg;
+      gga += gg;
+      gx *= gg;
+      gy *= gg;
     }
-    ggsum = block_sum(ggsum, m.red);
-    ngg = N;
+    m.g[2 * i] = gx;
+    m.g[2 * i + 1] = gy;
+    m.lap[i] = lp;
+    m.ph2[i] = ph;
+    m.ph2d[i] = x2;  // |g|^2 before the cutoff, for the kinetic energy
   }
+  __syncthreads();
+  // per-type sums: Laplacian, |g|^2, pair potential, phase gradient^2
+  // (register arrays with compile-time indices only: nt <= 2)
+  double sums[9] = {0, 0, 0, 0, 0, 0, 0, 0, gga};
+  for (int i = tid; i < N; i += kThreads) {
+    const bool t1 = type_of(S, i) == 1;
+    const double l = m.lap[i], g2 = m.ph2d[i], v = m.vp[i], p = m.ph2[i];
+    sums[0] += t1 ? 0.0 : l;
+    sums[1] += t1 ? 0.0 : g2;
+    sums[2] += t1 ? 0.0 : v;
+    sums[3] += t1 ? 0.0 : p;
+    sums[4] += t1 ? l : 0.0;
+    sums[5] += t1 ? g2 : 0.0;
+    sums[6] += t1 ? v : 0.0;
+    sums[7] += t1 ? p : 0.0;
+  }
+  block_sum_n<9>(sums, m.red);
   double kin0 = 0.0, pot0 = 0.0, efp = 0.0;
   double kin_t[2] = {0, 0}, un_t[2] = {0, 0}, pot_t[2] = {0, 0};
-  for (int t = 0; t < nt; t++) {
-    double hs = 0.0, g2 = 0.0, vs = 0.0, ph = 0.0;
-    for (int i = S.ipfrst[t] + tid; i < S.ipfrst[t] + S.np[t]; i += kThreads) {
-      hs += m.lap[i];
-      g2 += S.adrift != 0.0 ? m.ph2d[i]
-                            : m.g[2 * i] * m.g[2 * i] + m.g[2 * i + 1] * m.g[2 * i + 1];
-      vs += m.vp[i];
-      ph += m.ph2[i];
-    }
-    hs = block_sum(hs, m.red);
-    g2 = block_sum(g2, m.red);
-    vs = block_sum(vs, m.red);
-    ph = block_sum(ph, m.red);
-    hl[t] = hs;
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    if (t < nt) {
+    double hs = sums[4 * t], g2 = sums[4 * t + 1];
+    if (tid == 0) hl[t] = hs;
     kin_t[t] = S.hbs2m[t] * (hs - g2);
     kin0 += kin_t[t];
     kin_t[t] /= S.np[t];
     un_t[t] = 1.0 / sqrt(g2);
-    pot_t[t] = vs;
-    efp += S.hbs2m[t] * ph;
+    pot_t[t] = sums[4 * t + 2];
+    efp += S.hbs2m[t] * sums[4 * t + 3];
+    }
   }
   kin0 /= S.npnorm;
   // v2 tails (potential, reptation.f:4001-4022)
-  for (int it = 0; it < nt; it++) {
+#pragma unroll
+  for (int it = 0; it < 2; it++) {
+    if (it >= nt) continue;
     int i = S.iv2[it][it];
     if (i >= 0) pot_t[it] += S.np[it] * (S.np[it] - 1) * 0.5 * S.tab_tail[i];
-    for (int jt = it + 1; jt < nt; jt++) {
-      i = S.iv2[it][jt];
-      if (i < 0) continue;
-      double aux = S.np[it] * S.np[jt] * S.tab_tail[i];
-      pot_t[it] += 0.5 * aux;
-      pot_t[jt] += 0.5 * aux;
+    if (it == 0 && nt > 1) {
+      i = S.iv2[0][1];
+      if (i >= 0) {
+        double aux = S.np[0] * S.np[1] * S.tab_tail[i];
+        pot_t[0] += 0.5 * aux;
+        pot_t[1] += 0.5 * aux;
+      }
     }
   }
-  pot0 = 0.0;
-  for (int t = 0; t < nt; t++) pot0 += pot_t[t];
+  pot0 = pot_t[0] + pot_t[1];
   // k space (reptation.f:4034-4052): rho_k read by type index
-  for (int it = 0; it < nt; it++)
-    for (int jt = 0; jt < nt; jt++) {
-      int iv = S.iv2[it][jt];
-      if (iv < 0 || S.tab_nkew[iv] == 0) continue;
-      const double *vk = S.coef + S.tab_vkoff[iv];
-      double aux = 0.0;
-      for (int k = tid; k < S.tab_nkew[iv]; k += kThreads)
-        aux += __ldg(vk + k) * (m.rhok[2 * (it * S.nk + k)] * m.rhok[2 * (jt * S.nk + k)] +
-                                m.rhok[2 * (it * S.nk + k) + 1] * m.rhok[2 * (jt * S.nk + k) + 1]);
-      aux = block_sum(aux, m.red);
-      double c = aux + __ldg(vk + S.tab_nkew[iv]) * S.npnorm;
-      pot_t[it] += c;
-      pot0 += c;
-    }
+  {
+    double ks[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int it = 0; it < 2; it++)
+#pragma unroll
+      for (int jt = 0; jt < 2; jt++) {
+        if (it >= nt || jt >= nt) continue;
+        int iv = S.iv2[it][jt];
+        if (iv < 0 || S.tab_nkew[iv] == 0) continue;
+        const double *vk = S.coef + S.tab_vkoff[iv];
+        for (int k = tid; k < S.tab_nkew[iv]; k += kThreads)
+          ks[2 * it + jt] +=
+              __ldg(vk + k) * (m.rhok[2 * (it * S.nk + k)] * m.rhok[2 * (jt * S.nk + k)] +
+                               m.rhok[2 * (it * S.nk + k) + 1] * m.rhok[2 * (jt * S.nk + k) + 1]);
+      }
+    block_sum_n<4>(ks, m.red);
+#pragma unroll
+    for (int it = 0; it < 2; it++)
+#pragma unroll
+      for (int jt = 0; jt < 2; jt++) {
+        if (it >= nt || jt >= nt) continue;
+        int iv = S.iv2[it][jt];
+        if (iv < 0 || S.tab_nkew[iv] == 0) continue;
+        double c = ks[2 * it + jt] + __ldg(S.coef + S.tab_vkoff[iv] + S.tab_nkew[iv]) * S.npnorm;
+        pot_t[it] += c;
+        pot0 += c;
+      }
+  }
   pot0 = (pot0 + S.v0) / S.npnorm;
   efp = S.ntheta != 0 ? efp / S.npnorm : 0.0;
   if (tid == 0) {
@@ -673,8 +893,10 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
     props[QMC2D_JACC] = 0.0;
     props[QMC2D_JPOT0] = pot0;
     props[QMC2D_JKIN0] = kin0;
-    props[QMC2D_JGG] = S.adrift != 0.0 ? ggsum / ngg : 1.0;
-    for (int t = 0; t < nt; t++) {
+    props[QMC2D_JGG] = S.adrift != 0.0 ? sums[8] / N : 1.0;
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      if (t >= nt) continue;
       props[J7 + t] = pot_t[t] / S.np[t];
       props[J7 + nt + t] = kin_t[t];
       props[J7 + 2 * nt + t] = un_t[t];
@@ -699,6 +921,7 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
   double et = props[QMC2D_JETOT];
   if (!isfinite(et) || !isfinite(ltf)) status |= ST_NONFINITE;
   __syncthreads();
+  phase_mark(S, PH_ASSEMBLE, tph);
   return status;
 }
 

@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Walker-moves/s of the walker-propagation path on B200.
+
+Workload (default): DMC with backflow, N = 58 (29 up + 29 down) at r_s = 5,
+4096 walkers, time step tau = 0.05 r_s^2, one move per generation followed
+by branch2's fixed-population comb, Jastrow u2 + backflow
+eta(r) = 0.2 exp(-((r - r_s)/0.6 r_s)^2) + 2D Ewald (alpha = 5/L, 60
+half-space k vectors), FP64. Synthetic: tables written by
+2degas_b200/tables.py and walkers drawn uniformly in the cell from a seeded
+Philox stream, then equilibrated by VMC.
+
+One step = one DMC generation over the whole population (4096
+walker-moves). `value` times the device work with CUDA events on the
+library's stream (inputs resident in HBM, L2 flushed between steps);
+`e2e` times the same steps through the public C-ABI with the walker records
+copied from and to pinned host memory every step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "tests")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import importlib  # noqa: E402
+
+import numpy as np  # noqa: E402
+
+CONFIG = "dmc_bf_n58_rs5"
+METRIC = "walker-moves/sec (DMC with backflow, N=58 r_s=5, 4096 walkers)"
+UNIT = "walker-moves/s"
+
+
+def flops_per_move(N, ns, K, u3, backflow):
+    """Algorithmic flops of one all-electron walker-move (proposal + evaluation
+    + accept/reject) of the reference's algorithm, counted from its loop
+    structure: pairs P = N(N-1)/2 cost 16 (distance) + 32 (u2) + 12
+    (potential) + 110 (u3) + 80 (backflow) flops, rho_k costs 7 per
+    (particle, k), and per spin determinant of n electrons
+    backflow: 53 n^2 + 24 n^3 + 40 N n^2 + 44 N n (orbitals, complex LU and
+    inverse, A^-1 dA, drift, Laplacian with the O(N n^2) cross term);
+    no backflow: 45 n^2 + 8 n^3."""
+    P = N * (N - 1) // 2
+    f = P * (16 + 32 + 12 + 110 * u3 + 80 * backflow) + 7 * N * K
+    for n in ns:
+        if backflow:
+            f += 53 * n * n + 24 * n ** 3 + 40 * N * n * n + 44 * N * n
+        else:
+            f += 45 * n * n + 8 * n ** 3
+    return float(f)
+
+
+def make_config(tmp, nconf, seed):
+    tables = importlib.import_module("2degas_b200.tables")
+    cfg = tables.CONFIGS[CONFIG]
+    d = tables.make_run(os.path.join(tmp, CONFIG), "c", nconf=nconf, seed=seed, **cfg)
+    return d, cfg
+
+
+# ------------------------------------------------------------ CPU baseline
+def _cpu_worker(args):
+    """One host process: the oracle's DMC on its own sub-population for
+    `seconds` of wall time; returns walker-moves done and seconds."""
+    d, nw, seed, seconds, delta, etrial = args
+    q = importlib.import_module("2degas_b200")
+    from oracle_lib import Oracle
+
+    s = q.System.read(d, "c")
+    x = s.read_configs(d, ".0", 0, nw)
+    o = Oracle(s.ptr)
+    pop = o.population_init(x)
+    o.vmc_philox(pop, 2, delta, 10 ** 9, seed, 0)
+    t0 = time.perf_counter()
+    moves, gen = 0, 0
+    while time.perf_counter() - t0 < seconds:
+        o.dmc_philox(pop, 1, 1, delta, etrial, 2.0, 50, seed, gen, 1000 + gen)
+        moves += nw
+        gen += 1
+    return moves, time.perf_counter() - t0
+
+
+def cpu_rate(d, seconds, walkers_per_proc=8):
+    """Oracle DMC on every host core (one process per core, spawn)."""
+    import multiprocessing as mp
+
+    try:
+        ncores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        ncores = os.cpu_count() or 1
+    cfg = importlib.import_module("2degas_b200.tables").CONFIGS[CONFIG]
+    delta = 0.05 * cfg["rs"] ** 2
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(ncores) as pool:
+        res = pool.map(_cpu_worker, [(d, walkers_per_proc, 100 + i, seconds, delta, -0.3)
+                                     for i in range(ncores)])
+    moves = sum(r[0] for r in res)
+    wall = max(r[1] for r in res)
+    sample = (f"{ncores} processes x {walkers_per_proc} walkers, oracle DMC generations "
+              f"for {seconds:.0f} s each ({moves} walker-moves)")
+    return moves / wall, ncores, sample
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp64_peak_tflops(torch):
+    """Measured FP64 throughput of a cuBLAS DGEMM on this GPU (TFLOP/s)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+# ------------------------------------------------------------------- arms
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    with tempfile.TemporaryDirectory() as tmp:
+        d, _ = make_config(tmp, 64, 1)
+        secs = max(4.0, min(20.0, 0.4 * (args.steps + args.warmup)))
+        rate, cores, sample = cpu_rate(d, secs)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": CONFIG, "walkers": 4096, "N": 58, "rs": 5.0},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def b200_arm(args, rank, world, local_rank):
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    q = importlib.import_module("2degas_b200")
+    capi = q._capi
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    nw = args.walkers
+    tmp = tempfile.mkdtemp(prefix="qmc2d_bench_")
+    d, cfg = make_config(tmp, nw, 1 + rank)
+    sysobj = q.System.read(d, "c")
+    N = sysobj.N
+    ns = [sysobj.s.np[t] for t in range(sysobj.ntypes)]
+    rs = cfg["rs"]
+    delta = 0.05 * rs * rs
+    x0 = sysobj.read_configs(d, ".0", 0, nw)
+    h = q.Handle(sysobj, capacity=nw, seed=0x9E3779B97F4A7C15 + rank, device=local_rank)
+    h.population_set(x0)
+    h.vmc(args.equil, delta, 10 ** 9)  # seeded VMC equilibration
+    h.block_reset()
+    h.vmc(10, delta, 10 ** 9)
+    blk, norm = h.block_get()
+    etrial = blk[0] / norm
+    mmult, mage = 2.0, 50
+    stream = torch.cuda.ExternalStream(h.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        h.dmc(1, 1, delta, etrial, mmult, mage)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    h.profile(True)
+    h.block_reset()
+    dev_ms = 0.0
+    with Clocks(local_rank) as clk:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (outside the events)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            dev_ms += e0.elapsed_time(e1)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    move_ms, move_n = h.profile_get(capi.KERNEL_MOVE)
+    br_ms, br_n = h.profile_get(capi.KERNEL_BRANCH)
+    ga_ms, ga_n = h.profile_get(capi.KERNEL_GATHER)
+    h.profile(False)
+    blk, norm = h.block_get()
+    e_mean = blk[0] / norm
+    t_max = dev_ms
+    if dist:
+        t = torch.tensor([dev_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = world * nw * args.steps / (t_max * 1e-3)
+
+    # e2e: walker records from/to pinned host memory every step, public API
+    nt, npr = sysobj.ntypes, sysobj.nprops
+    pin = {k: torch.empty(n, dtype=torch.float64, pin_memory=True)
+           for k, n in (("x", nw * 2 * N), ("g", nw * 2 * N), ("h", nw * nt), ("p", nw * npr),
+                        ("s", nw), ("a", nw))}
+    ptr = {k: v.data_ptr() for k, v in pin.items()}
+    h.population_get_ptr(ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"], ptr["a"])
+    h2d = sum(v.numel() * 8 for v in pin.values())
+    d2h = h2d + npr * 8 + 8  # records back + block sums
+    k2 = max(3, args.steps // 2)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(k2):
+        h.population_load_ptr(nw, ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"], ptr["a"])
+        step()
+        h.population_get_ptr(ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"], ptr["a"])
+        h.block_get()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * nw * k2 / e2e_s
+
+    line = None
+    if rank == 0:
+        K = sysobj.s.nk
+        fpm = flops_per_move(N, ns, K, 0, 1)
+        achieved = fpm * nw / (move_ms / max(move_n, 1) * 1e-3) / 1e12
+        peak = fp64_peak_tflops(torch)
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            rate, cores, sample = cpu_rate(d, args.cpu_seconds)
+            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        launches = move_n + br_n + ga_n
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": CONFIG, "walkers_per_gpu": nw, "N": N, "rs": rs,
+                       "tau": delta, "mmstep": 1, "moves_per_step": nw * world,
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "parallelism": f"independent populations x{world}"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "kernel": "move_kernel",
+                         "flops_per_move": fpm,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64)"},
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "kernel_ms": {"move": move_ms, "branch": br_ms, "gather": ga_ms},
+            "wall_s": wall,
+            "e_mixed": e_mean,
+            "clocks": clk.summary(),
+        }
+    if dist:
+        dist.barrier()
+    h.close()
+    if dist:
+        dist.destroy_process_group()
+    if line:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--walkers", type=int, default=4096)
+    ap.add_argument("--equil", type=int, default=20)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+    return b200_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -191,9 +191,17 @@ int qmc2d_compute_properties_dev(qmc2d_handle *h, int nw, const double *x_dev,
  * population (x_old = x, g_old = g, p_old = props, age = 0, p_old(jacc)=1). */
 int qmc2d_population_set(qmc2d_handle *h, int nw, const double *x);
 int qmc2d_population_size(qmc2d_handle *h, int *nw);
-/* Copy the population out (any pointer may be NULL). */
-int qmc2d_population_get(qmc2d_handle *h, double *x, double *g, double *props,
-                         double *age);
+/* Copy the population out (any pointer may be NULL): the walker records of
+ * getconf (reptation.f:2369) - x, g (2N each), hl (ntypes), props
+ * (n_props), sign and age per walker. */
+int qmc2d_population_get(qmc2d_handle *h, double *x, double *g, double *hl, double *props,
+                         double *s, double *age);
+/* putconf (reptation.f:2409) for a whole population: load walker records
+ * that the caller already holds (as returned by qmc2d_population_get),
+ * without re-evaluating them. Pinned host buffers make the copies faster. */
+int qmc2d_population_load(qmc2d_handle *h, int nw, const double *x, const double *g,
+                          const double *hl, const double *props, const double *s,
+                          const double *age);
 
 /* Block accumulators (averages(1/2), reptation.f:4283-4304): weighted sums
  * of p_old over all walkers and steps since the last reset. */
@@ -236,6 +244,31 @@ int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params *prm,
 int qmc2d_rmc(qmc2d_handle *h, int nstp);
 /* Copy reptile r's path (ntau beads, x then props) out. */
 int qmc2d_rmc_get_path(qmc2d_handle *h, int r, double *x, double *props);
+
+/* ----------------------------------------------------- streams and timing
+ * The reference has no timers; these expose device time per kernel. */
+enum qmc2d_kernel {
+  QMC2D_KERNEL_MOVE = 0,    /* fused move + evaluation + accept (VMC/DMC) */
+  QMC2D_KERNEL_BRANCH = 1,  /* branch2 comb */
+  QMC2D_KERNEL_GATHER = 2,  /* walker slot copies after branching */
+  QMC2D_KERNEL_EVAL = 3,    /* batched compute_properties */
+  QMC2D_KERNEL_RMC = 4,     /* reptation moves */
+  QMC2D_NKERNELS = 5
+};
+/* The handle's CUDA stream (a cudaStream_t) so callers can order work and
+ * events after the library's launches. */
+int qmc2d_stream(qmc2d_handle *h, void **stream);
+/* enable = 1 starts recording a CUDA event pair around every launch on the
+ * handle's stream (and clears the totals); 0 stops. */
+int qmc2d_profile(qmc2d_handle *h, int enable);
+/* Total device milliseconds and launch count of one kernel since enable. */
+int qmc2d_profile_get(qmc2d_handle *h, int kernel, double *ms, long *launches);
+/* Phase timers inside the walker kernels: with enable = 1 every CTA adds
+ * the SM clock cycles its thread 0 spends in each phase of a move
+ * (proposal, pair sums, rho_k, u3, orbitals, inversion, F matrices, drift,
+ * cross-term matrix, cross term, assembly, accept) to 16 counters; with
+ * enable = 0 the counters are copied to cycles[16] and the timers stop. */
+int qmc2d_phase_timers(qmc2d_handle *h, int enable, unsigned long long *cycles);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -62,6 +62,10 @@ class Oracle:
         lib.oracle_reptile_run.argtypes = [c_void_p, c_void_p, c_int, c_uint64, c_long, c_int, PD,
                                            POINTER(c_long)]
         lib.oracle_reptile_path.argtypes = [c_void_p, PD, PD]
+        lib.oracle_setrn.argtypes = [c_void_p, PI]
+        lib.oracle_savern.argtypes = [c_void_p, PI]
+        lib.oracle_rannyu.restype = c_double
+        lib.oracle_rannyu.argtypes = [c_void_p]
         self.sysp = sysp
         s = sysp.contents
         self.N = s.nptot
@@ -155,6 +159,17 @@ class Oracle:
         used = self.lib.oracle_branch2(nw, _ptr(wate), _ptr(r), mult.ctypes.data_as(PI),
                                        src.ctypes.data_as(PI), ctypes.byref(ncap))
         return mult, src, used, ncap.value
+
+    def rannyu_stream(self, seed, count):
+        """count draws of the reference's rannyu after setrn(seed); returns
+        (draws, savern state)."""
+        st = (c_int * 8)()
+        sd = (c_int * 4)(*seed)
+        self.lib.oracle_setrn(ctypes.byref(st), sd)
+        out = np.array([self.lib.oracle_rannyu(ctypes.byref(st)) for _ in range(count)])
+        so = (c_int * 4)()
+        self.lib.oracle_savern(ctypes.byref(st), so)
+        return out, list(so)
 
     def philox_uniform2(self, seed, c0, c1, c2, c3):
         u = np.zeros(2)
