@@ -7,12 +7,16 @@
  * and bench.py's CPU-baseline leg may load it; the product library never
  * links or calls it.
  *
- * Parity pin: the reference cannot be compiled here (no Fortran compiler),
- * and it ships no per-configuration golden values. The oracle is pinned by
- * re-running the reference's own recorded VMC block (n26 fixture: seed file,
- * first stored configuration, twist (1,1)) with the reference's RNG and
- * comparing the final RNG state, final configuration and block sums that the
- * reference wrote to n26.res / n26.{up,down}.x.res.0 (tests/test_oracle_pin.py).
+ * Parity unpinned at the per-configuration level: the reference cannot be
+ * compiled here (no Fortran compiler) and ships no per-configuration golden
+ * values. What holds it: the loop-for-loop restatement; the reference's own
+ * self-check (testd, finite differences of -ln psi against the drift and
+ * Laplacian); the reference RNG against the LCG it implements; branch2
+ * against a line-by-line transcription; and a coarse statistical match to
+ * the one recorded VMC block (n26.res: E_L within 3 %, E_pot within 0.5 %).
+ * That block is not reproducible to its error bar (its per-spin kinetic
+ * energies are strongly asymmetric although the deck's wave function is
+ * spin-symmetric), so it came from a different build than the sources.
  */
 #ifndef QMC2D_ORACLE_H
 #define QMC2D_ORACLE_H
