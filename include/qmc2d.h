@@ -183,6 +183,25 @@ int qmc2d_compute_properties_dev(qmc2d_handle *h, int nw, const double *x_dev,
                                  double *g_dev, double *hlap_dev, double *props_dev,
                                  double *s_dev, void *stream);
 
+/* No counterpart in the reference. The same evaluation as
+ * qmc2d_compute_properties_dev for callers that cannot allocate device
+ * memory - a host code that hands out every device buffer from a pool of its
+ * own, or a serving loop that must not trigger a cudaMalloc (which can
+ * synchronise the device) between requests - and so cannot create a handle.
+ * It needs no handle and allocates nothing: the device copy of `sys` and the
+ * status words live in a fixed 2 MiB array that every GPU loading the
+ * library holds until exit. The caller passes device buffers for the inputs
+ * and outputs; the call is asynchronous on `stream` (NULL: the legacy default
+ * stream). Limits: at most 65536 walkers per call and tables, k vectors and
+ * orbital wave vectors of at most 229376 doubles together; larger requests
+ * return QMC2D_ERR_LIMIT. The first call on a device looks up the array's
+ * device address, so make that first call before any stream capture. All
+ * calls share the array: calls that overlap on the GPU (other streams, other
+ * threads) race on it and must be serialised by the caller. */
+int qmc2d_compute_properties_noalloc(const qmc2d_system *sys, int nw, const double *x_dev,
+                                     double *g_dev, double *hlap_dev, double *props_dev,
+                                     double *s_dev, void *stream);
+
 /* ---------------------------------------------------------- populations
  * A population is the reference's walker stack (x_stack, g_stack, h_stack,
  * s_stack, age_stack, p_stack; ewald.h:166-173) held in HBM. */
