@@ -39,12 +39,28 @@ struct EvalSmem {
   double *D2, *U, *part, *red, *gsh, *dk[2];
   int *perm[2], *used[2], *iscal, *gidx;
   double *gval;
+  // register-resident inversion: per spin, double-buffered pivot-row slots
+  // of every warp and the warps' pivot keys (inside the F0 region)
+  double2 *gslot[2];
+  unsigned long long *gkey[2];
 };
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 // Row stride of the inversion workspace: odd, so the rows that the lanes of
 // a warp own fall on distinct 16-byte bank groups.
 __host__ __device__ inline int ws_ld(int n) { return n | 1; }
+
+// Register-resident Gauss-Jordan: complex columns per thread, and the
+// lanes per row L (a power of two) with kGjCols*L >= n and one row per
+// thread of an nthr-thread group; 0 when n does not fit that layout.
+constexpr int kGjCols = 8;
+__host__ __device__ inline int gj_reg_lanes(int n, int nthr) {
+  for (int L = 1; L <= 32; L *= 2)
+    if (kGjCols * L >= n && nthr / L >= n) return L;
+  return 0;
+}
+// Warps per spin for the register-resident inversion (all warps of the CTA).
+__host__ __device__ inline int gj_reg_warps(int nt) { return (kThreads / 32) / (nt > 1 ? 2 : 1); }
 
 // Carve the dynamic shared memory; returns bytes used.
 __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSmem *m) {
@@ -74,6 +90,8 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
   t.rhok = (double *)take(sizeof(double) * 2 * (s.nk > 0 ? s.nk : 1) * 2);
   t.A[0] = t.A[1] = t.W[0] = t.W[1] = nullptr;
   t.F0 = t.F1 = nullptr;
+  t.gslot[0] = t.gslot[1] = nullptr;
+  t.gkey[0] = t.gkey[1] = nullptr;
   t.D2 = t.U = t.part = t.gsh = nullptr;
   t.dk[0] = t.dk[1] = nullptr;
   t.perm[0] = t.perm[1] = t.used[0] = t.used[1] = nullptr;
@@ -91,12 +109,23 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
     }
     // F0/F1 are dead once the cross-term matrix is built, so the cross
     // term's Jacobian columns U and partial sums share their space.
+    // The inversion's pivot-row slots and keys are dead before F0/F1 are
+    // formed, so they share the same space too.
     size_t fbytes = sizeof(double2) * 2 * n * n;
     size_t ubytes = sizeof(double) * (2 * n * kChunk + (n + 1) * kChunk);
-    t.F0 = (double2 *)take(fbytes > ubytes ? fbytes : ubytes);
+    const int gw = gj_reg_warps(nsp), gl = gj_reg_lanes(n, 32 * gw);
+    const size_t slot_per_spin = (size_t)2 * gw * kGjCols * gl;  // double2
+    size_t sbytes = (sizeof(double2) * slot_per_spin + sizeof(unsigned long long) * 2 * gw) * 2;
+    size_t rbytes = fbytes > ubytes ? fbytes : ubytes;
+    if (sbytes > rbytes) rbytes = sbytes;
+    t.F0 = (double2 *)take(rbytes);
     t.F1 = t.F0 ? t.F0 + n * n : nullptr;
     t.U = reinterpret_cast<double *>(t.F0);
     t.part = t.U ? t.U + 2 * n * kChunk : nullptr;
+    t.gslot[0] = t.F0;
+    t.gslot[1] = t.F0 ? t.F0 + slot_per_spin : nullptr;
+    t.gkey[0] = t.F0 ? reinterpret_cast<unsigned long long *>(t.F0 + 2 * slot_per_spin) : nullptr;
+    t.gkey[1] = t.gkey[0] ? t.gkey[0] + 2 * gw : nullptr;
     t.D2 = (double *)take(sizeof(double) * 3 * n);
     t.gsh = (double *)take(sizeof(double) * 2 * n);
   }
@@ -346,24 +375,145 @@ __device__ inline void gj_invert(double2 *W, int ld, int n, int *perm, double *d
   }
 }
 
+// The same inversion (same pivot rule, same outputs perm, dk, W and the
+// singular flag) with every row held in registers: thread gt of the
+// 32G-thread group owns row r = gt / L and the columns s + L j (s = gt % L,
+// j < kGjCols) with L = gj_reg_lanes(n, 32G). Per step k:
+//   * the owner of column k passes each row's entry to the row's lanes
+//     (width-L shuffle) and the row's lane 0 forms its pivot key: the bits
+//     of |re|+|im| (non-negative doubles order as integers) with the low
+//     byte replaced by 255 - r, so ties go to the lowest row;
+//   * a warp-wide max of the keys (two 32-bit redux steps); the warp's best
+//     row publishes its slice to the warp's slot, lane 0 its key;
+//   * one group barrier; every thread takes the best warp and updates its
+//     registers v -= (f / pivot) * pivot_row, column k becoming -f / pivot.
+// The pivot row is left unscaled (its column k set to 1) and every row is
+// divided by its own pivot at the end, which gives the normalised
+// Gauss-Jordan result. Slots and keys are double-buffered by the parity
+// of k, so one barrier per step separates the writes of step k+2 from the
+// reads of step k. Only the low 8 bits of |re|+|im| are dropped from the
+// comparison (ties within 2^-44 relative go to the lowest row).
+// slots: 2 * G * kGjCols * L double2; keys: 2 * G.
+__device__ inline void gj_invert_reg(double2 *W, int ld, int n, int *perm, double *dk,
+                                     int *singular, int gt, int G, int bar_id, double2 *slots,
+                                     unsigned long long *keys) {
+  const int nthr = 32 * G, lane = gt & 31, wg = gt >> 5;
+  const int L = gj_reg_lanes(n, nthr);
+  const int r = gt / L, s = gt - (gt / L) * L;
+  const int sw = kGjCols * L;
+  auto gsync = [&]() {
+    if (G == 1) __syncwarp();
+    else asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthr) : "memory");
+  };
+  double2 v[kGjCols];
+#pragma unroll
+  for (int j = 0; j < kGjCols; j++) {
+    const int c = s + L * j;
+    v[j] = (r < n && c < n) ? W[r * ld + c] : make_double2(0.0, 0.0);
+  }
+  bool used = r >= n;
+  double2 my_inv = make_double2(1.0, 0.0);
+#pragma unroll
+  for (int j = 0; j < kGjCols; j++) {
+#pragma unroll 1
+    for (int ss = 0; ss < L; ss++) {
+      const int k = j * L + ss;
+      if (k >= n) break;
+      const int buf = k & 1;
+      const double fx = __shfl_sync(0xffffffffu, v[j].x, ss, L);
+      const double fy = __shfl_sync(0xffffffffu, v[j].y, ss, L);
+      unsigned long long key = 0ull;
+      if (!used && s == 0) {
+        const double a = fabs(fx) + fabs(fy);
+        key = ((unsigned long long)__double_as_longlong(a) & ~0xFFull) | (unsigned)(255 - r);
+      }
+      {
+        const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+        const unsigned hm = __reduce_max_sync(0xffffffffu, hi);
+        const unsigned lm = __reduce_max_sync(0xffffffffu, hi == hm ? lo : 0u);
+        key = ((unsigned long long)hm << 32) | lm;
+      }
+      const int pw = 255 - (int)(key & 0xFFull);
+      double2 *mys = slots + (buf * G + wg) * sw;
+      if (key != 0ull && r == pw) {
+#pragma unroll
+        for (int jj = 0; jj < kGjCols; jj++) mys[s + L * jj] = v[jj];
+      }
+      if (lane == 0) keys[buf * G + wg] = key;
+      gsync();
+      unsigned long long best = keys[buf * G];
+      int bw = 0;
+      for (int w = 1; w < G; w++) {
+        const unsigned long long kw = keys[buf * G + w];
+        if (kw > best) {
+          best = kw;
+          bw = w;
+        }
+      }
+      const int p = 255 - (int)(best & 0xFFull);
+      const double2 *ps = slots + (buf * G + bw) * sw;
+      const double2 piv = ps[k];
+      const double d = piv.x * piv.x + piv.y * piv.y;
+      const double rd = 1.0 / d;
+      const double2 inv = make_double2(piv.x * rd, -piv.y * rd);
+      if (gt == 0) {
+        perm[k] = p;
+        dk[k] = d;
+        if ((best >> 8) == 0ull) *singular = 1;  // every candidate exactly zero
+      }
+      if (r == p) {
+        used = true;
+        my_inv = inv;
+        if (s == ss) v[j] = make_double2(1.0, 0.0);
+      } else if (r < n) {
+        const double2 fac = cmul(make_double2(fx, fy), inv);
+#pragma unroll
+        for (int jj = 0; jj < kGjCols; jj++) {
+          const double2 a = ps[s + L * jj];
+          v[jj].x = fma(-fac.x, a.x, fma(fac.y, a.y, v[jj].x));
+          v[jj].y = fma(-fac.x, a.y, fma(-fac.y, a.x, v[jj].y));
+        }
+        if (s == ss) v[j] = make_double2(-fac.x, -fac.y);
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kGjCols; j++) {
+    const int c = s + L * j;
+    if (r < n && c < n) W[r * ld + c] = cmul(v[j], my_inv);
+  }
+  gsync();
+}
+
 // rho_k per rhok slot (distances, reptation.f:4225-4243) by threads
 // t0 .. t0+nthr-1.
+// nthr is a multiple of 32 (whole warps): each (type, k) item is summed by
+// a group of 8 lanes, lane l taking particles l, l+8, ..., then a fixed
+// shuffle tree.
 __device__ inline void compute_rhok(const DevSys &S, const EvalSmem &m, int t, int nthr) {
-  for (int e = t; e < S.nt * S.nk; e += nthr) {
-    int ty = e / S.nk, k = e - ty * S.nk;
-    if (S.irhok[ty] == 0) continue;
-    double kx = __ldg(S.kvec + 2 * k), ky = __ldg(S.kvec + 2 * k + 1);
+  const int total = S.nt * S.nk, per_round = nthr / kGroup, l8 = t & (kGroup - 1);
+  for (int e0 = 0; e0 < total; e0 += per_round) {
+    const int e = e0 + t / kGroup;
+    const int ty = e < total ? e / S.nk : 0, k = e - ty * S.nk;
+    const bool on = e < total && S.irhok[ty] != 0;
     double c = 0.0, sn = 0.0;
-    for (int i = S.ipfrst[ty]; i < S.ipfrst[ty] + S.np[ty]; i++) {
-      double kr = kx * m.x[2 * i] + ky * m.x[2 * i + 1];
-      double sv, cv;
-      sincos(kr, &sv, &cv);
-      c += cv;
-      sn += sv;
+    if (on) {
+      const double kx = __ldg(S.kvec + 2 * k), ky = __ldg(S.kvec + 2 * k + 1);
+      for (int i = S.ipfrst[ty] + l8; i < S.ipfrst[ty] + S.np[ty]; i += kGroup) {
+        double kr = kx * m.x[2 * i] + ky * m.x[2 * i + 1];
+        double sv, cv;
+        sincos(kr, &sv, &cv);
+        c += cv;
+        sn += sv;
+      }
     }
-    int slot = S.irhok[ty] - 1;
-    m.rhok[2 * (slot * S.nk + k)] = c;
-    m.rhok[2 * (slot * S.nk + k) + 1] = sn;
+    c = group8_sum(c);
+    sn = group8_sum(sn);
+    if (on && l8 == 0) {
+      const int slot = S.irhok[ty] - 1;
+      m.rhok[2 * (slot * S.nk + k)] = c;
+      m.rhok[2 * (slot * S.nk + k) + 1] = sn;
+    }
   }
 }
 
@@ -553,8 +703,21 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
     if (tid < 2) m.iscal[tid] = 0;  // singular flags
     __syncthreads();
     phase_mark(S, PH_ORBITALS, tph);
-    // inversion by one group of warps per spin; rho_k on the other warps
-    {
+    // inversion: every warp in registers when each spin's matrix fits that
+    // layout (then rho_k), else half the CTA per shared-memory inversion
+    // with rho_k on the other warps
+    const int Gr = gj_reg_warps(nt);
+    bool reg_path = true;
+    for (int sp = 0; sp < nt; sp++) reg_path = reg_path && gj_reg_lanes(S.np[sp], 32 * Gr) > 0;
+    if (reg_path) {
+      const int sp = nt > 1 ? (tid >> 5) / Gr : 0, gt = tid - sp * 32 * Gr;
+      gj_invert_reg(sp ? m.W[1] : m.W[0], ws_ld(S.np[sp]), S.np[sp], sp ? m.perm[1] : m.perm[0],
+                    sp ? m.dk[1] : m.dk[0], &m.iscal[sp], gt, Gr, 1 + sp,
+                    sp ? m.gslot[1] : m.gslot[0], sp ? m.gkey[1] : m.gkey[0]);
+      __syncthreads();
+      compute_rhok(S, m, tid, kThreads);
+      __syncthreads();
+    } else {
       // warps per spin: half the CTA for the inversions, the rest for rho_k
       const int G = (kThreads / 32) / (2 * nt) > 0 ? (kThreads / 32) / (2 * nt) : 1;
       const int w = tid >> 5;
