@@ -62,6 +62,18 @@ __host__ __device__ inline int gj_reg_lanes(int n, int nthr) {
 // Warps per spin for the register-resident inversion (all warps of the CTA).
 __host__ __device__ inline int gj_reg_warps(int nt) { return (kThreads / 32) / (nt > 1 ? 2 : 1); }
 
+// Cross-term GEMM Y = M U on the FP64 tensor cores (mma.m8n8k4): M is
+// n2 x n2 row-major with row stride xt_ldm, the Jacobian block is stored
+// transposed (UT, one row of xt_ldu per column of U). Both strides are
+// 4 or 12 (mod 16) doubles, so the eight-byte fragment loads of a
+// half-warp (4 rows x 4 consecutive columns) fall on 16 distinct banks.
+__host__ __device__ inline int xt_row_tiles(int n2) { return (n2 + 7) / 8; }
+__host__ __device__ inline int xt_ldm(int n2) {
+  int l = (n2 + 3) & ~3;
+  return (l % 8 == 0) ? l + 4 : l;
+}
+__host__ __device__ inline int xt_ldu(int n2) { return 8 * xt_row_tiles(n2) + 4; }
+
 // Carve the dynamic shared memory; returns bytes used.
 __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSmem *m) {
   size_t off = 0;
@@ -97,11 +109,13 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
   t.perm[0] = t.perm[1] = t.used[0] = t.used[1] = nullptr;
   if (s.has_bf) {
     // A[s] and W[s] are adjacent: the 2n x 2n real cross-term matrix of spin
-    // s overlays them once F0/F1 are formed.
+    // s (row stride xt_ldm) overlays them once F0/F1 are formed.
+    const size_t awbytes = sizeof(double2) * (n * n + n * ld);
+    const size_t mbytes = sizeof(double) * 2 * n * xt_ldm(2 * n);
 #pragma unroll
     for (int sp = 0; sp < 2; sp++) {
       if (sp >= nsp) continue;
-      t.A[sp] = (double2 *)take(sizeof(double2) * (n * n + n * ld));
+      t.A[sp] = (double2 *)take(awbytes > mbytes ? awbytes : mbytes);
       t.W[sp] = t.A[sp] ? t.A[sp] + n * n : nullptr;
       t.dk[sp] = (double *)take(sizeof(double) * n);
       t.perm[sp] = (int *)take(sizeof(int) * n);
@@ -112,7 +126,8 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
     // The inversion's pivot-row slots and keys are dead before F0/F1 are
     // formed, so they share the same space too.
     size_t fbytes = sizeof(double2) * 2 * n * n;
-    size_t ubytes = sizeof(double) * (2 * n * kChunk + (n + 1) * kChunk);
+    const int ldu = xt_ldu(2 * n);
+    size_t ubytes = sizeof(double) * ((size_t)kChunk * ldu + (size_t)xt_row_tiles(2 * n) * kChunk);
     const int gw = gj_reg_warps(nsp), gl = gj_reg_lanes(n, 32 * gw);
     const size_t slot_per_spin = (size_t)2 * gw * kGjCols * gl;  // double2
     size_t sbytes = (sizeof(double2) * slot_per_spin + sizeof(unsigned long long) * 2 * gw) * 2;
@@ -121,7 +136,7 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
     t.F0 = (double2 *)take(rbytes);
     t.F1 = t.F0 ? t.F0 + n * n : nullptr;
     t.U = reinterpret_cast<double *>(t.F0);
-    t.part = t.U ? t.U + 2 * n * kChunk : nullptr;
+    t.part = t.U ? t.U + (size_t)kChunk * ldu : nullptr;
     t.gslot[0] = t.F0;
     t.gslot[1] = t.F0 ? t.F0 + slot_per_spin : nullptr;
     t.gkey[0] = t.F0 ? reinterpret_cast<unsigned long long *>(t.F0 + 2 * slot_per_spin) : nullptr;
@@ -201,6 +216,13 @@ __device__ __forceinline__ void bf_offdiag(const DevSys &S, const double *x, int
 }
 
 // Sum within aligned groups of 8 lanes; every lane of the warp must call it.
+// d += a b for one 8x8x4 FP64 tensor-core tile (warp-wide).
+__device__ __forceinline__ void dmma_m8n8k4(double (&d)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
+
 __device__ __forceinline__ double group8_sum(double v) {
   v += __shfl_xor_sync(0xffffffffu, v, 4);
   v += __shfl_xor_sync(0xffffffffu, v, 2);
@@ -859,21 +881,38 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
       }
       __syncthreads();
       phase_mark(S, PH_DRIFT, tph);
-      // cross term: M (2n x 2n over A[sp], W[sp]) then quadratic forms
-      const int n2 = 2 * ns;
+      // cross term: M (2n x 2n, row stride ldM, over A[sp], W[sp]; the
+      // padding columns zero), then per chunk of 16 electrons Y = M U on
+      // the FP64 tensor cores and the quadratic forms sum_p U(p,c) Y(p,c)
+      const int n2 = 2 * ns, ldM = xt_ldm(2 * ns), ldU = xt_ldu(2 * ns);
+      const int RT = xt_row_tiles(n2), KT = (n2 + 3) / 4;
       double *M = reinterpret_cast<double *>(sp ? m.A[1] : m.A[0]);
-      for (int e = tid; e < n2 * n2; e += kThreads) {
-        int p = e % n2, qq = e / n2;
-        int a = p / ns, j = p - a * ns, c = qq / ns, k = qq - c * ns;
-        double2 fa = (a == 0 ? m.F0 : m.F1)[k + j * ns];
-        double2 fc = (c == 0 ? m.F0 : m.F1)[j + k * ns];
-        M[e] = fa.x * fc.x - fa.y * fc.y;
+      for (int e = tid; e < n2 * ldM; e += kThreads) {
+        const int p = e / ldM, qq = e - p * ldM;
+        double v = 0.0;
+        if (qq < n2) {
+          const int a = p / ns, j = p - a * ns, c = qq / ns, k = qq - c * ns;
+          const double2 fa = (a == 0 ? m.F0 : m.F1)[k + j * ns];
+          const double2 fc = (c == 0 ? m.F0 : m.F1)[j + k * ns];
+          v = fa.x * fc.x - fa.y * fc.y;
+        }
+        M[e] = v;
       }
       __syncthreads();
+      // UT (over F0/F1, dead now): rows n2 .. ldU-1 of every column stay
+      // zero, covering the k padding of the last k-step and the rows of the
+      // last row tile beyond n2.
+      double *UT = m.U;
+      for (int e = tid; e < kChunk * (ldU - n2); e += kThreads) {
+        const int col = e / (ldU - n2), r = n2 + (e - col * (ldU - n2));
+        UT[col * ldU + r] = 0.0;
+      }
       phase_mark(S, PH_MBUILD, tph);
-      const int nrt = ns;  // row tiles of 2 rows over n2 = 2 ns rows
+      // work units: (row tile, group of CT column tiles), RT*NTG of them
+      const int NTG = RT >= 5 ? 1 : (RT >= 3 ? 2 : 4), CT = 4 / NTG;
+      const int warp = tid >> 5, lg = (tid & 31) >> 2, lt = tid & 3;
       for (int i0 = 0; i0 < N; i0 += kChunk / 2) {
-        // U[(a,j)][(i,b)] = J_{j,i}[a][b] for electrons i0 .. i0+15
+        // UT[(i,b)][(a,j)] = J_{j,i}[a][b] for electrons i0 .. i0+15
         for (int e = tid; e < ns * (kChunk / 2); e += kThreads) {
           int jl = e % ns, il = e / ns;
           int i = i0 + il, j = f0 + jl;
@@ -887,41 +926,53 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
               bf_offdiag(S, m.x, i, j, S.iub[type_of(S, i)][sp], jxx, jxy, jyy, qbx, qby);
             }
           }
-          m.U[(0 * ns + jl) * kChunk + 2 * il + 0] = jxx;  // a=x, b=x
-          m.U[(0 * ns + jl) * kChunk + 2 * il + 1] = jxy;  // a=x, b=y
-          m.U[(1 * ns + jl) * kChunk + 2 * il + 0] = jxy;  // a=y, b=x
-          m.U[(1 * ns + jl) * kChunk + 2 * il + 1] = jyy;  // a=y, b=y
+          UT[(2 * il + 0) * ldU + 0 * ns + jl] = jxx;  // a=x, b=x
+          UT[(2 * il + 1) * ldU + 0 * ns + jl] = jxy;  // a=x, b=y
+          UT[(2 * il + 0) * ldU + 1 * ns + jl] = jxy;  // a=y, b=x
+          UT[(2 * il + 1) * ldU + 1 * ns + jl] = jyy;  // a=y, b=y
         }
         __syncthreads();
-        // Y = M U in 2-row x 4-column register tiles; each tile's rows dot
-        // their own U rows into part[row tile][column].
-        for (int tile = tid; tile < nrt * (kChunk / 4); tile += kThreads) {
-          const int p0 = 2 * (tile / (kChunk / 4)), c0 = 4 * (tile % (kChunk / 4));
-          double y0[4] = {0, 0, 0, 0}, y1[4] = {0, 0, 0, 0};
-          const double *Mp = M + p0;
-          for (int qq = 0; qq < n2; qq++) {
-            const double2 mm = *reinterpret_cast<const double2 *>(Mp + qq * n2);
-            const double2 ua = *reinterpret_cast<const double2 *>(m.U + qq * kChunk + c0);
-            const double2 ub = *reinterpret_cast<const double2 *>(m.U + qq * kChunk + c0 + 2);
-            y0[0] += mm.x * ua.x;
-            y0[1] += mm.x * ua.y;
-            y0[2] += mm.x * ub.x;
-            y0[3] += mm.x * ub.y;
-            y1[0] += mm.y * ua.x;
-            y1[1] += mm.y * ua.y;
-            y1[2] += mm.y * ub.x;
-            y1[3] += mm.y * ub.y;
-          }
-          const double *u0 = m.U + p0 * kChunk + c0, *u1 = u0 + kChunk;
+        // Y = M U by warps, 8x8 output tiles (mma.m8n8k4 f64 fragments:
+        // A(row lg, col lt), B(row lt, col lg), D(row lg, cols 2lt, 2lt+1)).
+        // Rows of the last row tile beyond n2 reuse row n2-1 (their outputs
+        // meet zero rows of UT). Each unit's rows dot their UT rows into
+        // part[row tile][column].
+        for (int u = warp; u < RT * NTG; u += kThreads / 32) {
+          const int mt = u / NTG, nt0 = (u - mt * NTG) * CT;
+          const double *Ma = M + min(8 * mt + lg, n2 - 1) * ldM + lt;
+          double acc[4][2];
 #pragma unroll
-          for (int v = 0; v < 4; v++) m.part[(p0 / 2) * kChunk + c0 + v] = u0[v] * y0[v] + u1[v] * y1[v];
+          for (int c = 0; c < 4; c++) acc[c][0] = acc[c][1] = 0.0;
+          for (int kt = 0; kt < KT; kt++) {
+            const double a = Ma[4 * kt];
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+              if (c < CT) dmma_m8n8k4(acc[c], a, UT[(8 * (nt0 + c) + lg) * ldU + 4 * kt + lt]);
+          }
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            if (c < CT) {
+              const int col = 8 * (nt0 + c) + 2 * lt;
+              double s0 = acc[c][0] * UT[col * ldU + 8 * mt + lg];
+              double s1 = acc[c][1] * UT[(col + 1) * ldU + 8 * mt + lg];
+#pragma unroll
+              for (int o = 4; o < 32; o <<= 1) {
+                s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+                s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+              }
+              if (lg == 0) {
+                m.part[mt * kChunk + col] = s0;
+                m.part[mt * kChunk + col + 1] = s1;
+              }
+            }
+          }
         }
         __syncthreads();
         if (tid < kChunk / 2) {
           int i = i0 + tid;
           if (i < N) {
             double t3 = 0.0;
-            for (int rt = 0; rt < nrt; rt++)
+            for (int rt = 0; rt < RT; rt++)
               t3 += m.part[rt * kChunk + 2 * tid] + m.part[rt * kChunk + 2 * tid + 1];
             m.lapd[i] += t3;
           }
