@@ -37,6 +37,7 @@ struct EvalSmem {
   double2 *A[2], *W[2];      // per spin: orbitals (column-major) and the inversion workspace
   double2 *F0, *F1;          // F_a of the spin being processed, column-major
   double *D2, *U, *part, *red, *gsh, *dk[2];
+  double *fdg;  // F0(j,j), F1(j,j) of the spin being processed (4 doubles per j)
   int *perm[2], *used[2], *iscal, *gidx;
   double *gval;
   // register-resident inversion: per spin, double-buffered pivot-row slots
@@ -104,7 +105,7 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
   t.F0 = t.F1 = nullptr;
   t.gslot[0] = t.gslot[1] = nullptr;
   t.gkey[0] = t.gkey[1] = nullptr;
-  t.D2 = t.U = t.part = t.gsh = nullptr;
+  t.D2 = t.U = t.part = t.gsh = t.fdg = nullptr;
   t.dk[0] = t.dk[1] = nullptr;
   t.perm[0] = t.perm[1] = t.used[0] = t.used[1] = nullptr;
   if (s.has_bf) {
@@ -142,6 +143,7 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
     t.gkey[0] = t.F0 ? reinterpret_cast<unsigned long long *>(t.F0 + 2 * slot_per_spin) : nullptr;
     t.gkey[1] = t.gkey[0] ? t.gkey[0] + 2 * gw : nullptr;
     t.D2 = (double *)take(sizeof(double) * 3 * n);
+    t.fdg = (double *)take(sizeof(double) * 4 * n);
     t.gsh = (double *)take(sizeof(double) * 2 * n);
   }
   t.red = (double *)take(sizeof(double) * kThreads);
@@ -834,102 +836,101 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
       }
       __syncthreads();
       phase_mark(S, PH_FMAT, tph);
-      // drift, phase gradient and the first two Laplacian terms for every
-      // electron i against this determinant (reptation.f:10201-10237).
-      for (int base = 0; base < N; base += per_round) {
-        int i = base + tid / kGroup;
-        bool valid = i < N;
-        int ti = valid ? type_of(S, i) : 0;
-        double zxr = 0, zxi = 0, zyr = 0, zyi = 0, t12 = 0;
-        if (valid) {
-          for (int jl = lane8; jl < ns; jl += kGroup) {
-            int j = f0 + jl;
-            double jxx, jxy, jyy, qbx, qby;  // J[a][b] = dq_j[a]/dx_i[b]
-            if (j == i) {
-              jxx = 1.0 + m.Sb[3 * i];
-              jxy = m.Sb[3 * i + 1];
-              jyy = 1.0 + m.Sb[3 * i + 2];
-              qbx = m.qbd[2 * i];
-              qby = m.qbd[2 * i + 1];
-            } else {
-              bf_offdiag(S, m.x, i, j, S.iub[ti][sp], jxx, jxy, jyy, qbx, qby);
-            }
-            double2 fx = m.F0[jl + jl * ns], fy = m.F1[jl + jl * ns];
-            zxr += fx.x * jxx + fy.x * jxy;
-            zxi += fx.y * jxx + fy.y * jxy;
-            zyr += fx.x * jxy + fy.x * jyy;
-            zyi += fx.y * jxy + fy.y * jyy;
-            t12 -= fx.x * qbx + fy.x * qby;
-            double jtj_xx = jxx * jxx + jxy * jxy;
-            double jtj_xy = jxx * jxy + jxy * jyy;
-            double jtj_yy = jxy * jxy + jyy * jyy;
-            t12 -= m.D2[3 * jl] * jtj_xx + 2.0 * m.D2[3 * jl + 1] * jtj_xy +
-                   m.D2[3 * jl + 2] * jtj_yy;
-          }
-        }
-        zxr = group8_sum(zxr);
-        zxi = group8_sum(zxi);
-        zyr = group8_sum(zyr);
-        zyi = group8_sum(zyi);
-        t12 = group8_sum(t12);
-        if (valid && lane8 == 0) {
-          m.gd[2 * i] -= zxr;
-          m.gd[2 * i + 1] -= zyr;
-          m.ph2d[i] += zxi * zxi + zyi * zyi;
-          m.lapd[i] += t12;
-        }
-      }
-      __syncthreads();
-      phase_mark(S, PH_DRIFT, tph);
       // cross term: M (2n x 2n, row stride ldM, over A[sp], W[sp]; the
       // padding columns zero), then per chunk of 16 electrons Y = M U on
       // the FP64 tensor cores and the quadratic forms sum_p U(p,c) Y(p,c)
       const int n2 = 2 * ns, ldM = xt_ldm(2 * ns), ldU = xt_ldu(2 * ns);
       const int RT = xt_row_tiles(n2), KT = (n2 + 3) / 4;
+      const int warp = tid >> 5, lane = tid & 31, lg = lane >> 2, lt = tid & 3;
       double *M = reinterpret_cast<double *>(sp ? m.A[1] : m.A[0]);
-      for (int e = tid; e < n2 * ldM; e += kThreads) {
-        const int p = e / ldM, qq = e - p * ldM;
-        double v = 0.0;
-        if (qq < n2) {
-          const int a = p / ns, j = p - a * ns, c = qq / ns, k = qq - c * ns;
-          const double2 fa = (a == 0 ? m.F0 : m.F1)[k + j * ns];
-          const double2 fc = (c == 0 ? m.F0 : m.F1)[j + k * ns];
-          v = fa.x * fc.x - fa.y * fc.y;
+      for (int p = warp; p < n2; p += kThreads / 32) {
+        const int a = p >= ns ? 1 : 0, j = p - a * ns;
+        const double2 *Fa = a ? m.F1 : m.F0;
+        for (int qq = lane; qq < ldM; qq += 32) {
+          double v = 0.0;
+          if (qq < n2) {
+            const int c = qq >= ns ? 1 : 0, k = qq - c * ns;
+            const double2 fa = Fa[k + j * ns];
+            const double2 fc = (c ? m.F1 : m.F0)[j + k * ns];
+            v = fa.x * fc.x - fa.y * fc.y;
+          }
+          M[p * ldM + qq] = v;
         }
-        M[e] = v;
+      }
+      for (int j = tid; j < ns; j += kThreads) {
+        const double2 fx = m.F0[j + j * ns], fy = m.F1[j + j * ns];
+        m.fdg[4 * j] = fx.x;
+        m.fdg[4 * j + 1] = fx.y;
+        m.fdg[4 * j + 2] = fy.x;
+        m.fdg[4 * j + 3] = fy.y;
       }
       __syncthreads();
       // UT (over F0/F1, dead now): rows n2 .. ldU-1 of every column stay
       // zero, covering the k padding of the last k-step and the rows of the
       // last row tile beyond n2.
       double *UT = m.U;
-      for (int e = tid; e < kChunk * (ldU - n2); e += kThreads) {
-        const int col = e / (ldU - n2), r = n2 + (e - col * (ldU - n2));
-        UT[col * ldU + r] = 0.0;
-      }
+      for (int col = warp; col < kChunk; col += kThreads / 32)
+        for (int r = n2 + lane; r < ldU; r += 32) UT[col * ldU + r] = 0.0;
       phase_mark(S, PH_MBUILD, tph);
       // work units: (row tile, group of CT column tiles), RT*NTG of them
       const int NTG = RT >= 5 ? 1 : (RT >= 3 ? 2 : 4), CT = 4 / NTG;
-      const int warp = tid >> 5, lg = (tid & 31) >> 2, lt = tid & 3;
+      static_assert(kThreads == 16 * (kChunk / 2), "16 lanes per electron of a chunk");
       for (int i0 = 0; i0 < N; i0 += kChunk / 2) {
-        // UT[(i,b)][(a,j)] = J_{j,i}[a][b] for electrons i0 .. i0+15
-        for (int e = tid; e < ns * (kChunk / 2); e += kThreads) {
-          int jl = e % ns, il = e / ns;
-          int i = i0 + il, j = f0 + jl;
-          double jxx = 0, jxy = 0, jyy = 0, qbx, qby;
-          if (i < N) {
-            if (j == i) {
-              jxx = 1.0 + m.Sb[3 * i];
-              jxy = m.Sb[3 * i + 1];
-              jyy = 1.0 + m.Sb[3 * i + 2];
-            } else {
-              bf_offdiag(S, m.x, i, j, S.iub[type_of(S, i)][sp], jxx, jxy, jyy, qbx, qby);
+        // UT[(i,b)][(a,j)] = J_{j,i}[a][b] for electrons i = i0 .. i0+15,
+        // 16 lanes per electron; on the way, this determinant's drift,
+        // phase gradient and first two Laplacian terms of electron i
+        // (reptation.f:10201-10237), summed over the lanes in a fixed order.
+        {
+          const int il = tid >> 4, l16 = tid & 15, i = i0 + il;
+          const bool valid = i < N;
+          const int iub = S.iub[valid ? type_of(S, i) : 0][sp];
+          double zxr = 0, zxi = 0, zyr = 0, zyi = 0, t12 = 0;
+          for (int jl = l16; jl < ns; jl += 16) {
+            const int j = f0 + jl;
+            double jxx = 0, jxy = 0, jyy = 0;
+            if (valid) {
+              double qbx, qby;  // J[a][b] = dq_j[a]/dx_i[b]
+              if (j == i) {
+                jxx = 1.0 + m.Sb[3 * i];
+                jxy = m.Sb[3 * i + 1];
+                jyy = 1.0 + m.Sb[3 * i + 2];
+                qbx = m.qbd[2 * i];
+                qby = m.qbd[2 * i + 1];
+              } else {
+                bf_offdiag(S, m.x, i, j, iub, jxx, jxy, jyy, qbx, qby);
+              }
+              const double fxr = m.fdg[4 * jl], fxi = m.fdg[4 * jl + 1];
+              const double fyr = m.fdg[4 * jl + 2], fyi = m.fdg[4 * jl + 3];
+              zxr += fxr * jxx + fyr * jxy;
+              zxi += fxi * jxx + fyi * jxy;
+              zyr += fxr * jxy + fyr * jyy;
+              zyi += fxi * jxy + fyi * jyy;
+              t12 -= fxr * qbx + fyr * qby;
+              const double jtj_xx = jxx * jxx + jxy * jxy;
+              const double jtj_xy = jxx * jxy + jxy * jyy;
+              const double jtj_yy = jxy * jxy + jyy * jyy;
+              t12 -= m.D2[3 * jl] * jtj_xx + 2.0 * m.D2[3 * jl + 1] * jtj_xy +
+                     m.D2[3 * jl + 2] * jtj_yy;
             }
+            UT[(2 * il + 0) * ldU + 0 * ns + jl] = jxx;  // a=x, b=x
+            UT[(2 * il + 1) * ldU + 0 * ns + jl] = jxy;  // a=x, b=y
+            UT[(2 * il + 0) * ldU + 1 * ns + jl] = jxy;  // a=y, b=x
+            UT[(2 * il + 1) * ldU + 1 * ns + jl] = jyy;  // a=y, b=y
           }
-          UT[(2 * il + 0) * ldU + 0 * ns + jl] = jxx;  // a=x, b=x
-          UT[(2 * il + 1) * ldU + 0 * ns + jl] = jxy;  // a=x, b=y
-          UT[(2 * il + 0) * ldU + 1 * ns + jl] = jxy;  // a=y, b=x
-          UT[(2 * il + 1) * ldU + 1 * ns + jl] = jyy;  // a=y, b=y
+#pragma unroll
+          for (int o = 8; o > 0; o >>= 1) {
+            zxr += __shfl_xor_sync(0xffffffffu, zxr, o);
+            zxi += __shfl_xor_sync(0xffffffffu, zxi, o);
+            zyr += __shfl_xor_sync(0xffffffffu, zyr, o);
+            zyi += __shfl_xor_sync(0xffffffffu, zyi, o);
+            t12 += __shfl_xor_sync(0xffffffffu, t12, o);
+          }
+          if (valid && l16 == 0) {
+            m.gd[2 * i] -= zxr;
+            m.gd[2 * i + 1] -= zyr;
+            m.ph2d[i] += zxi * zxi + zyi * zyi;
+            m.lapd[i] += t12;
+          }
         }
         __syncthreads();
         // Y = M U by warps, 8x8 output tiles (mma.m8n8k4 f64 fragments:
