@@ -87,7 +87,7 @@ int build_devsys(const qmc2d_system *sys, q2d::DevSys *hs, std::vector<double> *
   coef->clear();
   for (int t = 0; t < sys->ntables; t++) {
     const qmc2d_table &tb = sys->tables[t];
-    while (coef->size() % 2) coef->push_back(0.0);  // 16-byte rows
+    while (coef->size() % 4) coef->push_back(0.0);  // 32-byte rows (one 256-bit load each)
     s.tab_off[t] = (int)coef->size();
     s.tab_ngrid[t] = tb.ngrid;
     s.tab_iexp[t] = tb.iexp;

@@ -141,7 +141,7 @@ extern "C" int qmc2d_compute_properties_noalloc(const qmc2d_system *sys, int nw,
   const size_t limit = kScratchDoubles - kStatusDoubles;
   for (int t = 0; t < sys->ntables && t < QMC2D_MAX_TABLES; t++) {
     const qmc2d_table &tb = sys->tables[t];
-    off = (off + 1) & ~size_t(1);
+    off = (off + 3) & ~size_t(3);  // 32-byte rows (one 256-bit load each)
     s.tab_off[t] = (int)off;
     s.tab_ngrid[t] = tb.ngrid;
     s.tab_iexp[t] = tb.iexp;

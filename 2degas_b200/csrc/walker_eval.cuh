@@ -160,26 +160,35 @@ __device__ __forceinline__ int type_of(const DevSys &S, int i) {
   return (S.nt > 1 && i >= S.ipfrst[1]) ? 1 : 0;
 }
 
+// One knot row (four doubles) of the packed tables in a single 256-bit
+// read-only load; every table starts on a 32-byte boundary of the packed
+// buffer (the packers pad to four doubles), so every row is 32-byte aligned.
+__device__ __forceinline__ double4 knot_row(const double *p) {
+  double4 r;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w)
+      : "l"(p));
+  return r;
+}
+
 // getf (reptation.f:4114): cubic at knot min(ngrid, ind), f, f', f''.
 __device__ __forceinline__ void spline3(const DevSys &S, int t, int ind, double rem, double &f,
                                         double &df, double &ddf) {
   int i = max(0, min(S.tab_ngrid[t], ind));  // NaN/negative -> knot 0
-  const double2 *u = reinterpret_cast<const double2 *>(S.coef + S.tab_off[t] + 4 * i);
-  double2 a = __ldg(u), b = __ldg(u + 1);
+  const double4 u = knot_row(S.coef + S.tab_off[t] + 4 * i);
   double rm = rem * S.drti;
-  f = a.x + rm * (a.y + rm * (b.x + rm * b.y));
-  df = (a.y + rm * (2.0 * b.x + rm * (3.0 * b.y))) * S.drti;
-  ddf = (b.x + rm * (3.0 * b.y)) * S.drti2;
+  f = u.x + rm * (u.y + rm * (u.z + rm * u.w));
+  df = (u.y + rm * (2.0 * u.z + rm * (3.0 * u.w))) * S.drti;
+  ddf = (u.z + rm * (3.0 * u.w)) * S.drti2;
 }
 
 // getf_0 (reptation.f:4103): f * (1/r)**iexp.
 __device__ __forceinline__ double spline0(const DevSys &S, int t, int ind, double rem,
                                           double byr) {
   int i = max(0, min(S.tab_ngrid[t], ind));  // NaN/negative -> knot 0
-  const double2 *u = reinterpret_cast<const double2 *>(S.coef + S.tab_off[t] + 4 * i);
-  double2 a = __ldg(u), b = __ldg(u + 1);
+  const double4 u = knot_row(S.coef + S.tab_off[t] + 4 * i);
   double rm = rem * S.drti;
-  double f = a.x + rm * (a.y + rm * (b.x + rm * b.y));
+  double f = u.x + rm * (u.y + rm * (u.z + rm * u.w));
   for (int k = 0; k < S.tab_iexp[t]; k++) f *= byr;
   return f;
 }
@@ -933,6 +942,7 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
           }
         }
         __syncthreads();
+        phase_mark(S, PH_DRIFT, tph);
         // Y = M U by warps, 8x8 output tiles (mma.m8n8k4 f64 fragments:
         // A(row lg, col lt), B(row lt, col lg), D(row lg, cols 2lt, 2lt+1)).
         // Rows of the last row tile beyond n2 reuse row n2-1 (their outputs
@@ -979,8 +989,8 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
           }
         }
         __syncthreads();
+        phase_mark(S, PH_CROSS, tph);
       }
-      phase_mark(S, PH_CROSS, tph);
     }
   } else {
     compute_rhok(S, m, tid, kThreads);
