@@ -39,6 +39,11 @@ import numpy as np  # noqa: E402
 CONFIG = "dmc_bf_n58_rs5"
 METRIC = "walker-moves/sec (DMC with backflow, N=58 r_s=5, 4096 walkers)"
 UNIT = "walker-moves/s"
+# DRAM bytes (read + write) of one move_kernel launch per walker, from the ncu
+# capture summarised in profiles/move_kernel_dmc_bf_n58_296w.md (296 walkers,
+# scaled linearly: the traffic is the walker records read and written).
+MOVE_DRAM_BYTES_PER_WALKER = 2.040064e6 / 296
+TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 296-walker launch, x walkers/296"
 
 
 def flops_per_move(N, ns, K, u3, backflow):
@@ -186,6 +191,30 @@ def fp64_peak_tflops(torch):
     return best
 
 
+# ------------------------------------------------------- multi-rank logic
+def rank_seeds(rank):
+    """(configuration seed, walker-stream seed) of a rank: every rank runs its
+    own independent population (weak scaling, no data-path collective)."""
+    return 1 + rank, 0x9E3779B97F4A7C15 + rank
+
+
+def max_over_ranks(value, dist=None, device="cpu"):
+    """The largest `value` over all ranks (timings are the slowest rank's)."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, walkers_per_rank, steps, seconds):
+    """Walker-moves per second of the whole job: every rank's walker-moves
+    over the slowest rank's time."""
+    return world * walkers_per_rank * steps / seconds
+
+
 # ------------------------------------------------------------------- arms
 def reference_arm(args, rank, world):
     if rank != 0:
@@ -222,14 +251,15 @@ def b200_arm(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     nw = args.walkers
     tmp = tempfile.mkdtemp(prefix="qmc2d_bench_")
-    d, cfg = make_config(tmp, nw, 1 + rank)
+    cfg_seed, walker_seed = rank_seeds(rank)
+    d, cfg = make_config(tmp, nw, cfg_seed)
     sysobj = q.System.read(d, "c")
     N = sysobj.N
     ns = [sysobj.s.np[t] for t in range(sysobj.ntypes)]
     rs = cfg["rs"]
     delta = 0.05 * rs * rs
     x0 = sysobj.read_configs(d, ".0", 0, nw)
-    h = q.Handle(sysobj, capacity=nw, seed=0x9E3779B97F4A7C15 + rank, device=local_rank)
+    h = q.Handle(sysobj, capacity=nw, seed=walker_seed, device=local_rank)
     h.population_set(x0)
     h.vmc(args.equil, delta, 10 ** 9)  # seeded VMC equilibration
     h.block_reset()
@@ -242,6 +272,27 @@ def b200_arm(args, rank, world, local_rank):
 
     def step():
         h.dmc(1, 1, delta, etrial, mmult, mage)
+
+    if args.phases:
+        # SM cycles per walker-move of each phase of the move kernel (clock64
+        # deltas of thread 0 of every CTA, summed over CTAs), no timing
+        for _ in range(args.warmup):
+            step()
+        h.phase_timers(True)
+        for _ in range(args.steps):
+            step()
+        ph = h.phase_timers(False)
+        moves = nw * args.steps
+        tot = sum(ph.values())
+        if rank == 0:
+            print(json.dumps({"phases_cycles_per_move": {k: v / moves for k, v in ph.items() if v},
+                              "share": {k: v / tot for k, v in ph.items() if v},
+                              "workload": CONFIG, "walkers": nw, "steps": args.steps}), flush=True)
+        h.close()
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
 
     for _ in range(args.warmup):
         step()
@@ -272,12 +323,8 @@ def b200_arm(args, rank, world, local_rank):
     h.profile(False)
     blk, norm = h.block_get()
     e_mean = blk[0] / norm
-    t_max = dev_ms
-    if dist:
-        t = torch.tensor([dev_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = world * nw * args.steps / (t_max * 1e-3)
+    t_max = max_over_ranks(dev_ms, dist, "cuda")
+    value = whole_job_rate(world, nw, args.steps, t_max * 1e-3)
 
     # e2e: walker records from/to pinned host memory every step, public API
     nt, npr = sysobj.ntypes, sysobj.nprops
@@ -299,12 +346,8 @@ def b200_arm(args, rank, world, local_rank):
         h.population_get_ptr(ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"], ptr["a"])
         h.block_get()
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * nw * k2 / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+    e2e = whole_job_rate(world, nw, k2, e2e_s)
 
     line = None
     if rank == 0:
@@ -328,7 +371,9 @@ def b200_arm(args, rank, world, local_rank):
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": MOVE_DRAM_BYTES_PER_WALKER * nw,
+                         "traffic_source": TRAFFIC_SOURCE,
                          "kernel": "move_kernel",
                          "flops_per_move": fpm,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64)"},
@@ -352,13 +397,15 @@ def b200_arm(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--walkers", type=int, default=4096)
     ap.add_argument("--equil", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--phases", action="store_true",
+                    help="print SM cycles per walker-move of each move-kernel phase instead")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
