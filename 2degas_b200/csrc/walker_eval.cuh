@@ -14,14 +14,15 @@
 //     sum_j (xi'' + 3 xi'/r) r_kj.(G_k - G_j) - tr(S_k^2) - sum_j tr(M_kj^2),
 //     S_k = sum_j M_kj: the dense dg/ddg of makeg/dotg are never formed.
 //   * determinants: A(k,j) = exp(i g_k.q_j) for both spins at once; each
-//     spin's matrix is inverted by its own group of warps (Gauss-Jordan with
-//     partial pivoting, rows chosen in place instead of swapped, warp-level
-//     synchronisation only), while the remaining warps compute rho_k.
+//     spin's matrix is inverted by half the CTA (Gauss-Jordan with partial
+//     pivoting, rows chosen in place instead of swapped, every row held in
+//     registers, one group barrier per step), then rho_k on all warps.
 //     Then, per spin, F_a = A^-1 diag(i g_a) A (register-tiled complex
-//     GEMM), the drift and the first two Laplacian terms, and the backflow
-//     cross term sum_{j,k} Re[(J_j.F(k,j))(J_k.F(j,k))] as the quadratic
-//     form of the symmetric 2n x 2n matrix M_ac(j,k) = Re[F_a(k,j) F_c(j,k)]
-//     against the Jacobian columns of every electron (register-tiled GEMM).
+//     GEMM) and the backflow cross term sum_{j,k} Re[(J_j.F(k,j))(J_k.F(j,k))]
+//     as the quadratic form of the symmetric 2n x 2n matrix
+//     M_ac(j,k) = Re[F_a(k,j) F_c(j,k)] against the Jacobian columns of every
+//     electron (FP64 tensor-core GEMM, mma.m8n8k4); the drift and the first
+//     two Laplacian terms are summed while the Jacobian columns are built.
 #pragma once
 
 #include <cuda_runtime.h>
