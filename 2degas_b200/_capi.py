@@ -29,7 +29,7 @@ ERR_LIMIT = 10
 ERR_STACK = 11
 
 # kernels for qmc2d_profile_get
-KERNEL_MOVE, KERNEL_BRANCH, KERNEL_GATHER, KERNEL_EVAL, KERNEL_RMC = range(5)
+KERNEL_MOVE, KERNEL_BRANCH, KERNEL_GATHER, KERNEL_EVAL, KERNEL_RMC, KERNEL_PAIRS = range(6)
 
 # property indices (0-based; reptation.f:577-637)
 JETOT, JLTF, JACC, JPOT0, JKIN0, JE2, JGG = range(7)

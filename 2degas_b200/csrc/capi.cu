@@ -17,6 +17,42 @@
 #include "rmc.cuh"
 #include "handle.h"
 
+namespace q2d {
+
+void pack_pair_rows(const qmc2d_system *sys, DevSys *s, std::vector<double> *rows) {
+  int ng = 0;
+  for (int a = 0; a < s->nt; a++)
+    for (int b = 0; b < s->nt; b++)
+      for (int t : {s->iu2[a][b], s->iu3[a][b], s->iub[a][b], s->iv2[a][b]})
+        if (t >= 0 && sys->tables[t].ngrid > ng) ng = sys->tables[t].ngrid;
+  s->cmb_ng = ng;
+  std::vector<std::vector<int>> blocks;  // distinct (u2, u3, bf, v2) table tuples
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 2; b++) {
+      s->cmb_blk[a][b] = 0;
+      if (a >= s->nt || b >= s->nt) continue;
+      std::vector<int> key = {s->iu2[a][b], s->iu3[a][b], s->iub[a][b], s->iv2[a][b]};
+      size_t k = 0;
+      while (k < blocks.size() && blocks[k] != key) k++;
+      if (k == blocks.size()) blocks.push_back(key);
+      s->cmb_blk[a][b] = (int)k;
+    }
+  s->cmb_nblk = (int)blocks.size();
+  for (const std::vector<int> &tab : blocks)
+    for (int k = 0; k <= ng; k++)
+      for (int q = 0; q < 4; q++) {
+        if (tab[q] < 0) {
+          rows->insert(rows->end(), 4, 0.0);
+          continue;
+        }
+        const qmc2d_table &tb = sys->tables[tab[q]];
+        const double *r = tb.ut + 4 * (size_t)std::min(k, tb.ngrid);
+        rows->insert(rows->end(), r, r + 4);
+      }
+}
+
+}  // namespace q2d
+
 namespace {
 
 int cuda_fail(cudaError_t e, const char *what) {
@@ -34,6 +70,7 @@ template <typename T>
 cudaError_t dalloc(T **p, size_t n) {
   return cudaMalloc((void **)p, sizeof(T) * (n > 0 ? n : 1));
 }
+
 
 int build_devsys(const qmc2d_system *sys, q2d::DevSys *hs, std::vector<double> *coef) {
   q2d::DevSys s{};
@@ -97,6 +134,9 @@ int build_devsys(const qmc2d_system *sys, q2d::DevSys *hs, std::vector<double> *
     s.tab_vkoff[t] = (int)coef->size();
     if (tb.nk_ewald > 0) coef->insert(coef->end(), tb.vk, tb.vk + tb.nk_ewald + 1);
   }
+  while (coef->size() % 16) coef->push_back(0.0);  // 128-byte pair rows
+  s.cmb_off = (int)coef->size();
+  q2d::pack_pair_rows(sys, &s, coef);
   *hs = s;
   return QMC2D_OK;
 }
@@ -215,7 +255,8 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
       (e = dalloc(&h->d_g, (size_t)cap * 2 * N)) != cudaSuccess ||
       (e = dalloc(&h->d_h, (size_t)cap * nt)) != cudaSuccess ||
       (e = dalloc(&h->d_p, (size_t)cap * np)) != cudaSuccess ||
-      (e = dalloc(&h->d_s, (size_t)cap)) != cudaSuccess)
+      (e = dalloc(&h->d_s, (size_t)cap)) != cudaSuccess ||
+      (e = dalloc(&h->d_mscr, (size_t)cap * q2d::move_scratch_doubles(h->hs))) != cudaSuccess)
     return fail(cuda_fail(e, "cudaMalloc"));
   cudaMemset(h->d_blk, 0, sizeof(double) * cap * np);
   cudaMemset(h->d_norm, 0, sizeof(double) * cap);
@@ -235,7 +276,7 @@ extern "C" int qmc2d_destroy(qmc2d_handle *h) {
   void *bufs[] = {h->ds, h->d_coef, h->d_kvec, h->d_gvec, h->d_blk, h->d_norm, h->d_cnt,
                   h->d_wate, h->d_status, h->br.delt, h->br.csum, h->br.mult, h->br.src,
                   h->br.ecum, h->br.zrank, h->br.ncapped, h->d_x, h->d_g, h->d_h, h->d_p,
-                  h->d_s, h->hs.phase};
+                  h->d_s, h->d_mscr, h->hs.phase};
   for (void *b : bufs) cudaFree(b);
   for (int k = 0; k < QMC2D_NKERNELS; k++)
     for (cudaEvent_t e : h->ev[k]) cudaEventDestroy(e);
@@ -461,8 +502,8 @@ static int run_moves(qmc2d_handle *h, int nstp, int dmc, double delta, double et
                      double mmult, int mage) {
   q2d::MoveArgs a{};
   a.nw = h->nw;
-  a.nstp = nstp;
   a.dmc = dmc;
+  a.scr = h->d_mscr;
   a.delta = delta;
   a.mage = mage;
   a.etrial = etrial;
@@ -478,9 +519,17 @@ static int run_moves(qmc2d_handle *h, int nstp, int dmc, double delta, double et
     h->hs.delta = delta;
     CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
   }
-  {
-    ProfScope ps(h, QMC2D_KERNEL_MOVE, h->stream);
-    CK(q2d::launch_moves(h->hs, h->ds, h->pop[h->cur], a, h->stream));
+  for (int istp = 0; istp < nstp; istp++) {
+    a.step0 = h->move_counter + (uint32_t)istp;
+    a.first = istp == 0;
+    {
+      ProfScope ps(h, QMC2D_KERNEL_PAIRS, h->stream);
+      CK(q2d::launch_pairs(h->hs, h->ds, h->pop[h->cur], a, h->stream));
+    }
+    {
+      ProfScope ps(h, QMC2D_KERNEL_MOVE, h->stream);
+      CK(q2d::launch_move(h->hs, h->ds, h->pop[h->cur], a, h->stream));
+    }
   }
   h->move_counter += (uint32_t)nstp;
   return QMC2D_OK;

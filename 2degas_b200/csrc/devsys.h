@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 
 #include "../../include/qmc2d.h"
 
@@ -34,6 +35,13 @@ struct DevSys {
   int tab_nkew[QMC2D_MAX_TABLES];
   int tab_vkoff[QMC2D_MAX_TABLES];  // offset of v_k in the packed buffer
   double tab_tail[QMC2D_MAX_TABLES];
+  // Pair rows: for type pair (a, b) (block cmb_blk[a][b] of cmb_ng + 1 rows;
+  // type pairs with the same four tables share a block) and knot k, 16
+  // doubles = the four-coefficient rows of the u2, u3, backflow and v2
+  // tables of that pair side by side (zeros for an absent kind), each
+  // table's row min(k, its ngrid). One 128-byte line per pair lookup.
+  int cmb_off, cmb_ng;  // offset (doubles, 128-byte aligned) in coef; last knot
+  int cmb_blk[2][2], cmb_nblk;
   const double *coef;  // packed tables: ut rows (4 doubles each) and v_k lists
   const double *kvec;  // 2*nk
   const double *gvec;  // 2*ngvec
@@ -52,6 +60,9 @@ enum : int {
 struct DevPop {
   double *x, *g, *h, *p, *s, *age;  // 2N, 2N, nt, nprops, 1, 1 per walker
 };
+
+// Pair rows of s appended to rows; sets s->cmb_ng and s->cmb_blk (host side).
+void pack_pair_rows(const qmc2d_system *sys, DevSys *s, std::vector<double> *rows);
 
 // Shared-memory footprint (bytes) of the walker evaluation for this system.
 size_t eval_smem_bytes(const DevSys &s);

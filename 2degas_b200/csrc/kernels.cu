@@ -1,10 +1,12 @@
 // kernels.cu - walker kernels for sm_100a: batched evaluation
-// (compute_properties), the fused VMC/DMC move (move + compute_properties +
+// (compute_properties), the VMC/DMC move in two launches (move + the pair
+// passes of compute_properties; the rest of compute_properties +
 // metropolis_test + averages(2), reptation.f:4617, 2661, 2622, 4275), the
 // fixed-population comb of branch2 (reptation.f:2162) and the slot gather
 // that replaces its send/receive/prov_dest copies.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "kernels.cuh"
@@ -111,6 +113,81 @@ size_t move_smem_bytes(const DevSys &s) {
   return eval_carve(s, nullptr, nullptr) + move_carve(s, nullptr, nullptr);
 }
 
+// One move of one walker is two launches. pairs_kernel: the proposal
+// (move, reptation.f:4631-4646) and the pair passes, written to the
+// walker's MoveScratch block. move_kernel: the rest of the evaluation, the
+// reverse move, metropolis_test and the averages, with the walker's state
+// in shared memory.
+//
+// pairs_kernel is persistent: one CTA of kPairThreads per SM walks over the
+// population. Its random spline-row lookups (three per pair) go to a
+// shared-memory copy of the pair rows when they fit (stage_rows), made once
+// per launch; random rows in global memory cost an L1 tag lookup per lane,
+// shared memory a few bank wavefronts per warp.
+constexpr int kPairThreads = 512;
+
+__global__ void __launch_bounds__(kPairThreads, 1) pairs_kernel(const DevSys *sp, DevPop pop,
+                                                                MoveArgs a, int stage_rows) {
+  __shared__ DevSys S;
+  extern __shared__ __align__(16) char smem[];
+  load_sys(S, sp);
+  EvalSmem m;
+  const size_t off = (pair_carve(S, smem, &m, kPairThreads) + 127) & ~size_t(127);
+  const int tid = threadIdx.x;
+  const double *rows_g = S.coef + S.cmb_off;
+  double *rows_s = reinterpret_cast<double *>(smem + off);
+  if (stage_rows) {  // 16-double rows to kPairRowSh-double rows
+    const int nrow = S.cmb_nblk * (S.cmb_ng + 1);
+    const double2 *src = reinterpret_cast<const double2 *>(rows_g);
+    for (int e = tid; e < nrow * 8; e += kPairThreads) {
+      const int r = e >> 3, q = e & 7;
+      reinterpret_cast<double2 *>(rows_s + (size_t)r * kPairRowSh)[q] = __ldg(src + e);
+    }
+    __syncthreads();
+  }
+  const int N = S.N, N2 = 2 * N;
+  const uint32_t step = a.step0;
+  const double pi = 3.141592653589793;
+  const MoveScratch L = move_scratch(S);
+  for (int w = blockIdx.x; w < a.nw; w += gridDim.x) {
+    long long tph = clock64();
+    double wo = 0.0;
+    for (int j = tid; j < N2; j += kPairThreads) {
+      int ti = type_of(S, j >> 1);
+      double var = 2.0 * S.hbs2m[ti] * a.delta, vari = 1.0 / var;
+      double2 u = uniform2(a.seed, (uint32_t)j, (uint32_t)w, step, 0u);
+      double chi = cos(pi * u.x) * sqrt(-2.0 * var * log(u.y));
+      wo -= chi * chi * vari;
+      m.x[j] = chi + (-var * pop.g[(size_t)w * N2 + j]) + pop.x[(size_t)w * N2 + j];
+    }
+    const double wold = block_sum_t<kPairThreads>(wo, m.red);
+    phase_mark(S, PH_PROPOSE, tph);
+    double *o = a.scr + (size_t)w * L.stride;
+    double *pout = S.has_bf ? o + L.pair : nullptr;
+    if (stage_rows)
+      eval_pairs<kPairThreads, true>(S, m, tph, pout, rows_s);
+    else
+      eval_pairs<kPairThreads, false>(S, m, tph, pout, rows_g);
+    __syncthreads();
+    for (int j = tid; j < N2; j += kPairThreads) {
+      o[L.x + j] = m.x[j];
+      o[L.g + j] = m.g[j];
+      o[L.q + j] = m.q[j];
+      o[L.qbd + j] = m.qbd[j];
+    }
+    for (int j = tid; j < 3 * N; j += kPairThreads) o[L.sb + j] = m.Sb[j];
+    for (int j = tid; j < N; j += kPairThreads) {
+      o[L.lap + j] = m.lap[j];
+      o[L.ltf + j] = m.ltf[j];
+      o[L.vp + j] = m.vp[j];
+    }
+    if (tid == 0) o[L.wold] = wold;
+    __syncthreads();  // m is reused by the next walker
+  }
+}
+
+size_t move_scratch_doubles(const DevSys &hs) { return move_scratch(hs).stride; }
+
 __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, DevPop pop,
                                                            MoveArgs a) {
   __shared__ DevSys S;
@@ -122,95 +199,96 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
   move_carve(S, smem + off, &v);
   const int w = blockIdx.x, tid = threadIdx.x;
   if (w >= a.nw) return;
-  const int N2 = 2 * S.N, np = S.nprops, nt = S.nt;
+  const int N = S.N, N2 = 2 * N, np = S.nprops, nt = S.nt;
+  const MoveScratch L = move_scratch(S);
+  const double *o = a.scr + (size_t)w * L.stride;
   for (int j = tid; j < N2; j += kThreads) {
     v.xo[j] = pop.x[(size_t)w * N2 + j];
     v.go[j] = pop.g[(size_t)w * N2 + j];
+    m.x[j] = o[L.x + j];
+    m.g[j] = o[L.g + j];
+    m.q[j] = o[L.q + j];
+    m.qbd[j] = o[L.qbd + j];
+    m.gd[j] = 0.0;
+  }
+  for (int j = tid; j < 3 * N; j += kThreads) m.Sb[j] = o[L.sb + j];
+  for (int j = tid; j < N; j += kThreads) {
+    m.lap[j] = o[L.lap + j];
+    m.ltf[j] = o[L.ltf + j];
+    m.vp[j] = o[L.vp + j];
+    m.lapd[j] = 0.0;
+    m.ph2[j] = 0.0;
+    m.ph2d[j] = 0.0;
   }
   for (int j = tid; j < np; j += kThreads) {
     v.po[j] = pop.p[(size_t)w * np + j];
     v.blk[j] = a.blk[(size_t)w * np + j];
   }
   if (tid < nt) v.ho[tid] = pop.h[(size_t)w * nt + tid];
+  const double wold = o[L.wold];
   __syncthreads();
   double so = pop.s[w];
   double age = pop.age[w];
   double norm = a.blk_norm[w];
-  double wate = 1.0;
+  double wate = (a.dmc && !a.first) ? a.wate[w] : 1.0;
   double nacc = 0.0, nforced = 0.0;
   int status = 0;
-  const uint64_t seed = a.seed;
-  const double pi = 3.141592653589793;
+  const uint32_t step = a.step0;
   long long tph = clock64();
-  for (int istp = 0; istp < a.nstp; istp++) {
-    const uint32_t step = a.step0 + (uint32_t)istp;
-    // proposal (move, reptation.f:4631-4646)
-    double wo = 0.0;
-    for (int j = tid; j < N2; j += kThreads) {
-      int ti = type_of(S, j >> 1);
-      double var = 2.0 * S.hbs2m[ti] * a.delta, vari = 1.0 / var;
-      double2 u = uniform2(seed, (uint32_t)j, (uint32_t)w, step, 0u);
-      double chi = cos(pi * u.x) * sqrt(-2.0 * var * log(u.y));
-      wo -= chi * chi * vari;
-      m.x[j] = chi + (-var * v.go[j]) + v.xo[j];
-    }
-    double wold = block_sum(wo, m.red);
-    phase_mark(S, PH_PROPOSE, tph);
-    double sn = 1.0;
-    status |= eval_walker(S, m, v.hn, v.pn, &v.sc[0], tph);
-    sn = v.sc[0];
-    // reverse move (reptation.f:4660-4674)
-    double wn = 0.0;
-    for (int j = tid; j < N2; j += kThreads) {
-      int ti = type_of(S, j >> 1);
-      double var = 2.0 * S.hbs2m[ti] * a.delta, vari = 1.0 / var;
-      double chi = v.xo[j] - m.x[j] - (-var * m.g[j]);
-      wn -= chi * chi * vari;
-    }
-    double wnew = block_sum(wn, m.red);
-    double p;
-    if (age == a.mage) {
-      p = 1.0;
-      nforced += 1.0;
-    } else {
-      p = (v.po[QMC2D_JLTF] - v.pn[QMC2D_JLTF]) * 2.0 + 0.5 * (wnew - wold);
-      p = fmin(0.0, fmax(-50.0, p));
-      p = exp(p);
-    }
-    // metropolis_test (reptation.f:2622-2659)
-    double xr = 1.0;
-    if (p < 1.0) xr = uniform2(seed, 0xFFFFFFFEu, (uint32_t)w, step, 0u).x;
-    bool acc = p >= xr;
-    double elocal = acc ? 0.5 * (v.pn[QMC2D_JETOT] + v.po[QMC2D_JETOT]) : v.po[QMC2D_JETOT];
-    __syncthreads();
-    if (acc) {
-      for (int j = tid; j < N2; j += kThreads) {
-        v.xo[j] = m.x[j];
-        v.go[j] = m.g[j];
-      }
-      for (int j = tid; j < np; j += kThreads) v.po[j] = v.pn[j];
-      if (tid < nt) v.ho[tid] = v.hn[tid];
-      so = sn;
-      age = 0.0;
-      nacc += 1.0;
-    } else {
-      age += 1.0;
-    }
-    __syncthreads();
-    if (tid == 0) v.po[QMC2D_JACC] = p;
-    double wgt = 1.0;
-    if (a.dmc) {
-      // dmc weight (reptation.f:898-903)
-      double peso = exp(-S.npnorm * (elocal - a.etrial) * a.delta);
-      if (peso > a.mmult) peso = a.mmult;
-      wate *= peso;
-      wgt = wate;
-    }
-    __syncthreads();
-    for (int j = tid; j < np; j += kThreads) v.blk[j] += v.po[j] * wgt;
-    norm += wgt;
-    phase_mark(S, PH_ACCEPT, tph);
+  double sn = 1.0;
+  status |= eval_det(S, m, v.hn, v.pn, &v.sc[0], tph, S.has_bf ? o + L.pair : nullptr);
+  sn = v.sc[0];
+  // reverse move (reptation.f:4660-4674)
+  double wn = 0.0;
+  for (int j = tid; j < N2; j += kThreads) {
+    int ti = type_of(S, j >> 1);
+    double var = 2.0 * S.hbs2m[ti] * a.delta, vari = 1.0 / var;
+    double chi = v.xo[j] - m.x[j] - (-var * m.g[j]);
+    wn -= chi * chi * vari;
   }
+  double wnew = block_sum(wn, m.red);
+  double p;
+  if (age == a.mage) {
+    p = 1.0;
+    nforced += 1.0;
+  } else {
+    p = (v.po[QMC2D_JLTF] - v.pn[QMC2D_JLTF]) * 2.0 + 0.5 * (wnew - wold);
+    p = fmin(0.0, fmax(-50.0, p));
+    p = exp(p);
+  }
+  // metropolis_test (reptation.f:2622-2659)
+  double xr = 1.0;
+  if (p < 1.0) xr = uniform2(a.seed, 0xFFFFFFFEu, (uint32_t)w, step, 0u).x;
+  bool acc = p >= xr;
+  double elocal = acc ? 0.5 * (v.pn[QMC2D_JETOT] + v.po[QMC2D_JETOT]) : v.po[QMC2D_JETOT];
+  __syncthreads();
+  if (acc) {
+    for (int j = tid; j < N2; j += kThreads) {
+      v.xo[j] = m.x[j];
+      v.go[j] = m.g[j];
+    }
+    for (int j = tid; j < np; j += kThreads) v.po[j] = v.pn[j];
+    if (tid < nt) v.ho[tid] = v.hn[tid];
+    so = sn;
+    age = 0.0;
+    nacc += 1.0;
+  } else {
+    age += 1.0;
+  }
+  __syncthreads();
+  if (tid == 0) v.po[QMC2D_JACC] = p;
+  double wgt = 1.0;
+  if (a.dmc) {
+    // dmc weight (reptation.f:898-903), multiplied over the generation's moves
+    double peso = exp(-S.npnorm * (elocal - a.etrial) * a.delta);
+    if (peso > a.mmult) peso = a.mmult;
+    wate *= peso;
+    wgt = wate;
+  }
+  __syncthreads();
+  for (int j = tid; j < np; j += kThreads) v.blk[j] += v.po[j] * wgt;
+  norm += wgt;
+  phase_mark(S, PH_ACCEPT, tph);
   __syncthreads();
   for (int j = tid; j < N2; j += kThreads) {
     pop.x[(size_t)w * N2 + j] = v.xo[j];
@@ -226,7 +304,7 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
     pop.age[w] = age;
     a.blk_norm[w] = norm;
     a.cnt[4 * w + 0] += nacc;
-    a.cnt[4 * w + 1] += a.nstp;
+    a.cnt[4 * w + 1] += 1.0;
     a.cnt[4 * w + 2] += nforced;
     if (status) a.cnt[4 * w + 3] += 1.0;
     if (a.wate) a.wate[w] = wate;
@@ -416,9 +494,30 @@ cudaError_t launch_eval(const DevSys &hs, const DevSys *ds, int nw, const double
   return cudaGetLastError();
 }
 
-cudaError_t launch_moves(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
+cudaError_t launch_pairs(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
                          cudaStream_t st) {
-  if (a.nw <= 0 || a.nstp <= 0) return cudaSuccess;
+  if (a.nw <= 0) return cudaSuccess;
+  int dev = 0, nsm = 0, optin = 0;
+  cudaError_t e;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+    return e;
+  if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) !=
+      cudaSuccess)
+    return e;
+  const size_t carve = (pair_carve(hs, nullptr, nullptr, kPairThreads) + 127) & ~size_t(127);
+  const size_t rows = sizeof(double) * kPairRowSh * (size_t)hs.cmb_nblk * (hs.cmb_ng + 1);
+  const int stage = carve + rows + sizeof(DevSys) <= (size_t)optin ? 1 : 0;
+  const size_t sm = carve + (stage ? rows : 0);
+  if ((e = set_smem((const void *)pairs_kernel, sm)) != cudaSuccess) return e;
+  const int grid = a.nw < nsm ? a.nw : nsm;
+  pairs_kernel<<<grid, kPairThreads, sm, st>>>(ds, pop, a, stage);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_move(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
+                        cudaStream_t st) {
+  if (a.nw <= 0) return cudaSuccess;
   size_t sm = move_smem_bytes(hs);
   cudaError_t e = set_smem((const void *)move_kernel, sm);
   if (e != cudaSuccess) return e;

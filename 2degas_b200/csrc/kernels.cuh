@@ -9,19 +9,21 @@
 
 namespace q2d {
 
+// One walker-move of a population: pairs kernel then move kernel.
 struct MoveArgs {
   int nw;
-  int nstp;           // VMC steps, or DMC moves per generation (mmstep)
+  int first;          // first move of a DMC generation (weights restart at 1)
   int dmc;            // 0: VMC averages (weight 1), 1: DMC weights
   double delta;
   double mage;        // forced-move age (compared with ==, as the reference)
   double etrial, mmult;
   uint64_t seed;
-  uint32_t step0;     // Philox c2 of the first move
+  uint32_t step0;     // Philox c2 of this move
+  double *scr;        // nw * move_scratch(s).stride doubles (MoveScratch blocks)
   double *blk;        // nw * nprops block sums of p_old (* weight)
   double *blk_norm;   // nw
   double *cnt;        // nw * 4: accepted, proposed, forced, nonzero status
-  double *wate;       // nw DMC weights (out)
+  double *wate;       // nw DMC weights (product over the generation's moves)
   int *status;        // nw status words (OR-ed)
 };
 
@@ -29,9 +31,15 @@ struct MoveArgs {
 cudaError_t launch_eval(const DevSys &hs, const DevSys *ds, int nw, const double *x, double *g,
                         double *hl, double *props, double *s, int *status, cudaStream_t st);
 
-// VMC steps or one DMC generation's moves on a resident population.
-cudaError_t launch_moves(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
+// One move of a resident population: the proposal and pair passes into the
+// move scratch (launch_pairs), then the rest of the evaluation, the
+// acceptance and the averages (launch_move).
+cudaError_t launch_pairs(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
                          cudaStream_t st);
+cudaError_t launch_move(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
+                        cudaStream_t st);
+// Doubles of move scratch per walker.
+size_t move_scratch_doubles(const DevSys &hs);
 
 // branch2's comb: wate -> src (new slot j copies old slot src[j]).
 struct BranchScratch {

@@ -151,6 +151,11 @@ extern "C" int qmc2d_compute_properties_noalloc(const qmc2d_system *sys, int nw,
     s.tab_vkoff[t] = (int)off;
     if (tb.nk_ewald > 0) off += tb.nk_ewald + 1;
   }
+  off = (off + 15) & ~size_t(15);  // 128-byte pair rows
+  s.cmb_off = (int)off;
+  std::vector<double> rows;
+  q2d::pack_pair_rows(sys, &s, &rows);
+  off += rows.size();
   const size_t kvec_off = off;
   off += 2 * (size_t)(sys->nk > 0 ? sys->nk : 0);
   const size_t gvec_off = off;
@@ -189,6 +194,11 @@ extern "C" int qmc2d_compute_properties_noalloc(const qmc2d_system *sys, int nw,
                              cudaMemcpyHostToDevice, cs)) != cudaSuccess)
       return fail(e, "cudaMemcpyAsync(v_k)");
   }
+  // rows is pageable: the copy is staged before cudaMemcpyAsync returns
+  if (!rows.empty() &&
+      (e = cudaMemcpyAsync(base + s.cmb_off, rows.data(), sizeof(double) * rows.size(),
+                           cudaMemcpyHostToDevice, cs)) != cudaSuccess)
+    return fail(e, "cudaMemcpyAsync(pair rows)");
   if (sys->nk > 0 && (e = cudaMemcpyAsync(base + kvec_off, sys->kvec, sizeof(double) * 2 * sys->nk,
                                           cudaMemcpyHostToDevice, cs)) != cudaSuccess)
     return fail(e, "cudaMemcpyAsync(kvec)");

@@ -155,15 +155,72 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
   return off;
 }
 
+// The pair passes alone (pairs_kernel): only the per-particle arrays they
+// write and the reduction buffer; every other pointer is null.
+__host__ __device__ inline size_t pair_carve(const DevSys &s, char *base, EvalSmem *m,
+                                             int nthreads) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) -> char * {
+    char *p = base ? base + off : nullptr;
+    off += align16(bytes);
+    return p;
+  };
+  const int N = s.N;
+  EvalSmem t{};
+  t.x = (double *)take(sizeof(double) * 2 * N);
+  t.g = (double *)take(sizeof(double) * 2 * N);
+  t.q = (double *)take(sizeof(double) * 2 * N);
+  t.G3 = (double *)take(sizeof(double) * 2 * N);
+  t.S3 = (double *)take(sizeof(double) * 3 * N);
+  t.Sb = (double *)take(sizeof(double) * 3 * N);
+  t.qbd = (double *)take(sizeof(double) * 2 * N);
+  t.lap = (double *)take(sizeof(double) * N);
+  t.ltf = (double *)take(sizeof(double) * N);
+  t.vp = (double *)take(sizeof(double) * N);
+  t.ph2 = (double *)take(sizeof(double) * N);
+  t.gd = (double *)take(sizeof(double) * 2 * N);
+  t.lapd = (double *)take(sizeof(double) * N);
+  t.ph2d = (double *)take(sizeof(double) * N);
+  t.red = (double *)take(sizeof(double) * nthreads);
+  if (m) *m = t;
+  return off;
+}
+
+// Per-walker move scratch in global memory (doubles), written by the pair
+// kernel and read by the move kernel of the same step: the proposed
+// configuration, the pair passes' per-particle sums, the proposal's log
+// density, and (backflow) the spline values of every ordered pair (i, j):
+// eta(r_ij), eta'(r_ij)/r_ij and 3 eta'/r + eta'' at [k N^2 + i N + j].
+struct MoveScratch {
+  int x, g, q, sb, qbd, lap, ltf, vp, wold, pair;
+  size_t stride;
+};
+__host__ __device__ inline MoveScratch move_scratch(const DevSys &s) {
+  const int N = s.N;
+  MoveScratch l;
+  l.x = 0;
+  l.g = 2 * N;
+  l.q = 4 * N;
+  l.sb = 6 * N;
+  l.qbd = 9 * N;
+  l.lap = 11 * N;
+  l.ltf = 12 * N;
+  l.vp = 13 * N;
+  l.wold = 14 * N;
+  l.pair = (14 * N + 1 + 3) & ~3;
+  size_t end = (size_t)l.pair + (s.has_bf ? 3 * (size_t)N * N : 0);
+  l.stride = (end + 31) & ~size_t(31);  // 256-byte aligned walker blocks
+  return l;
+}
+
 // ----------------------------------------------------------------- helpers
 
 __device__ __forceinline__ int type_of(const DevSys &S, int i) {
   return (S.nt > 1 && i >= S.ipfrst[1]) ? 1 : 0;
 }
 
-// One knot row (four doubles) of the packed tables in a single 256-bit
-// read-only load; every table starts on a 32-byte boundary of the packed
-// buffer (the packers pad to four doubles), so every row is 32-byte aligned.
+// Four doubles of the packed tables in a single 256-bit read-only load; p is
+// 32-byte aligned (pair rows are 128-byte aligned, their parts 32 bytes).
 __device__ __forceinline__ double4 knot_row(const double *p) {
   double4 r;
   asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
@@ -172,11 +229,43 @@ __device__ __forceinline__ double4 knot_row(const double *p) {
   return r;
 }
 
-// getf (reptation.f:4114): cubic at knot min(ngrid, ind), f, f', f''.
-__device__ __forceinline__ void spline3(const DevSys &S, int t, int ind, double rem, double &f,
-                                        double &df, double &ddf) {
-  int i = max(0, min(S.tab_ngrid[t], ind));  // NaN/negative -> knot 0
-  const double4 u = knot_row(S.coef + S.tab_off[t] + 4 * i);
+// Pair-row parts: the four coefficients of each kind's table.
+enum : int { PR_U2 = 0, PR_U3 = 4, PR_BF = 8, PR_V2 = 12 };
+
+// The pair row of type pair (a, b) at knot min(cmb_ng, ind) in the rows at
+// `rows` (the packed buffer's S.coef + S.cmb_off, or a shared-memory copy):
+// part q holds the row min(ngrid, ind) of that pair's table of kind q, which
+// is the knot getf/getf_0 clamp to (NaN/negative ind -> knot 0).
+// Rows are 16 doubles apart in global memory and kPairRowSh apart in a
+// shared-memory copy: 144 bytes, so consecutive knots start on different
+// 16-byte bank groups and a warp's random rows spread over eight of them.
+constexpr int kPairRowSh = 18;
+template <int RS = 16>
+__device__ __forceinline__ const double *pair_row(const DevSys &S, const double *rows, int a,
+                                                  int b, int ind) {
+  const int k = max(0, min(S.cmb_ng, ind));
+  return rows + ((size_t)S.cmb_blk[a][b] * (S.cmb_ng + 1) + k) * RS;
+}
+__device__ __forceinline__ const double *pair_row(const DevSys &S, int a, int b, int ind) {
+  return pair_row(S, S.coef + S.cmb_off, a, b, ind);
+}
+
+// Four doubles of a pair row in shared (kSh) or global memory.
+template <bool kSh>
+__device__ __forceinline__ double4 row_part(const double *p) {
+  if (kSh) {
+    const double2 a = reinterpret_cast<const double2 *>(p)[0];
+    const double2 b = reinterpret_cast<const double2 *>(p)[1];
+    return make_double4(a.x, a.y, b.x, b.y);
+  }
+  return knot_row(p);
+}
+
+// getf (reptation.f:4114): the cubic of one knot row, f, f', f''.
+template <bool kSh = false>
+__device__ __forceinline__ void spline3(const DevSys &S, const double *part, double rem,
+                                        double &f, double &df, double &ddf) {
+  const double4 u = row_part<kSh>(part);
   double rm = rem * S.drti;
   f = u.x + rm * (u.y + rm * (u.z + rm * u.w));
   df = (u.y + rm * (2.0 * u.z + rm * (3.0 * u.w))) * S.drti;
@@ -184,13 +273,13 @@ __device__ __forceinline__ void spline3(const DevSys &S, int t, int ind, double 
 }
 
 // getf_0 (reptation.f:4103): f * (1/r)**iexp.
-__device__ __forceinline__ double spline0(const DevSys &S, int t, int ind, double rem,
-                                          double byr) {
-  int i = max(0, min(S.tab_ngrid[t], ind));  // NaN/negative -> knot 0
-  const double4 u = knot_row(S.coef + S.tab_off[t] + 4 * i);
+template <bool kSh = false>
+__device__ __forceinline__ double spline0(const DevSys &S, const double *part, int iexp,
+                                          double rem, double byr) {
+  const double4 u = row_part<kSh>(part);
   double rm = rem * S.drti;
   double f = u.x + rm * (u.y + rm * (u.z + rm * u.w));
-  for (int k = 0; k < S.tab_iexp[t]; k++) f *= byr;
+  for (int k = 0; k < iexp; k++) f *= byr;
   return f;
 }
 
@@ -210,14 +299,15 @@ __device__ __forceinline__ void pair_geom(const DevSys &S, const double *x, int 
 
 // Backflow Jacobian dq_j/dx_i (2x2, symmetric) for j != i (qa of
 // slater_excitations, reptation.f:10093-10168): -(eta I + eta'/r r r^T).
+// ti, tj: the types of i and j.
 __device__ __forceinline__ void bf_offdiag(const DevSys &S, const double *x, int i, int j,
-                                           int tab, double &jxx, double &jxy, double &jyy,
-                                           double &qbx, double &qby) {
+                                           int ti, int tj, double &jxx, double &jxy,
+                                           double &jyy, double &qbx, double &qby) {
   double rx, ry, r, byr, rem;
   int ind;
   pair_geom(S, x, i, j, rx, ry, r, byr, ind, rem);
   double t, dt, ddt;
-  spline3(S, tab, ind, rem, t, dt, ddt);
+  spline3(S, pair_row(S, ti, tj, ind) + PR_BF, rem, t, dt, ddt);
   double c = dt * byr;
   jxx = -(t + c * rx * rx);
   jxy = -(c * rx * ry);
@@ -262,6 +352,20 @@ __device__ __forceinline__ void block_sum_n(double (&v)[K], double *red) {
     v[k] = t;
   }
   __syncthreads();
+}
+
+// Deterministic sum over a block of NT threads (NT/32 warps); red[0 .. NT/32).
+template <int NT>
+__device__ __forceinline__ double block_sum_t(double v, double *red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int ww = 0; ww < NT / 32; ww++) t += red[ww];
+  __syncthreads();
+  return t;
 }
 
 __device__ __forceinline__ double block_sum(double v, double *red) {
@@ -555,13 +659,22 @@ __device__ inline void compute_rhok(const DevSys &S, const EvalSmem &m, int t, i
 //
 // Input: m.x holds the configuration. Output (in shared memory): m.g (drift
 // -grad ln psi), hl[nt] (-lap ln psi per type), props[nprops], *sign.
-// Returns a status word (ST_*), identical in all threads.
-__device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl, double *props,
-                                  double *sign, long long &tph) {
+// eval_walker (= eval_pairs then eval_det) returns a status word (ST_*),
+// identical in all threads.
+//
+// Pair passes A and B: writes m.{ltf, g, lap, vp, G3, S3, q, Sb, qbd} and
+// zeroes m.{gd, lapd, ph2, ph2d}. With pout (backflow), also the backflow
+// spline values of every ordered pair, laid out as in MoveScratch.
+// NT threads (a multiple of 32) run the passes; the pair rows are read at
+// `rows`, from shared memory when kSh.
+template <int NT, bool kSh>
+__device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long &tph,
+                                  double *pout, const double *rows) {
   const int tid = threadIdx.x;
-  const int N = S.N, nt = S.nt;
+  const int N = S.N;
   const int lane8 = tid & (kGroup - 1);
-  const int per_round = kThreads / kGroup;
+  const int per_round = NT / kGroup;
+  const size_t NN = (size_t)N * N;
 
   // ---- pass A: pair sums of u2, the pair part of u3, u3 G vectors and S,
   // backflow displacement, Jacobian diagonal and Laplacian, pair potential.
@@ -579,9 +692,10 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
         double rx, ry, r, byr, rem;
         int ind;
         pair_geom(S, m.x, i, j, rx, ry, r, byr, ind, rem);
+        const double *row = pair_row<kSh ? kPairRowSh : 16>(S, rows, ti, tj, ind);
         double t, dt, ddt;
         if (S.has_u2) {
-          spline3(S, S.iu2[ti][tj], ind, rem, t, dt, ddt);
+          spline3<kSh>(S, row + PR_U2, rem, t, dt, ddt);
           ltf += 0.5 * t;
           double dtr = dt * byr;
           gx += dtr * rx;
@@ -589,7 +703,7 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
           lap += ddt + dtr;
         }
         if (S.has_u3) {
-          spline3(S, S.iu3[ti][tj], ind, rem, t, dt, ddt);
+          spline3<kSh>(S, row + PR_U3, rem, t, dt, ddt);
           Gx -= t * rx;
           Gy -= t * ry;
           double c = dt * byr;
@@ -606,7 +720,7 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
           lap += d3 + c3;
         }
         if (S.has_bf) {
-          spline3(S, S.iub[ti][tj], ind, rem, t, dt, ddt);
+          spline3<kSh>(S, row + PR_BF, rem, t, dt, ddt);
           qx += t * rx;
           qy += t * ry;
           double c = dt * byr;
@@ -616,8 +730,14 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
           double w2 = dt * byr * 3.0 + ddt;
           qbx += w2 * rx;
           qby += w2 * ry;
+          if (pout) {
+            const size_t e = (size_t)i * N + j;
+            pout[e] = t;
+            pout[NN + e] = c;
+            pout[2 * NN + e] = w2;
+          }
         }
-        if (S.has_v2) vp += 0.5 * spline0(S, S.iv2[ti][tj], ind, rem, byr);
+        if (S.has_v2) vp += 0.5 * spline0<kSh>(S, row + PR_V2, S.tab_iexp[S.iv2[ti][tj]], rem, byr);
       }
     }
     ltf = group8_sum(ltf);
@@ -685,7 +805,7 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
           int ind;
           pair_geom(S, m.x, k, j, rx, ry, r, byr, ind, rem);
           double t, dt, ddt;
-          spline3(S, S.iu3[tk][tj], ind, rem, t, dt, ddt);
+          spline3<kSh>(S, pair_row<kSh ? kPairRowSh : 16>(S, rows, tk, tj, ind) + PR_U3, rem, t, dt, ddt);
           double c = dt * byr;
           double mxx = t + c * rx * rx, mxy = c * rx * ry, myy = t + c * ry * ry;
           double dGx = Gkx - m.G3[2 * j], dGy = Gky - m.G3[2 * j + 1];
@@ -709,6 +829,17 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
     __syncthreads();
     phase_mark(S, PH_U3, tph);
   }
+}
+
+// Everything after the pair passes: determinants (orbitals, inversion,
+// F, drift, Laplacian with the cross term), rho_k, assembly. With pin, the
+// backflow Jacobian blocks take the pair spline values written by
+// eval_pairs(pout) instead of evaluating them again.
+__device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, double *props,
+                               double *sign, long long &tph, const double *pin) {
+  const int tid = threadIdx.x;
+  const int N = S.N, nt = S.nt;
+  const size_t NN = (size_t)N * N;
 
   // ---- backflow Slater determinants (slater_excitations, reptation.f:9967)
   int status = ST_OK;
@@ -893,39 +1024,68 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
         {
           const int il = tid >> 4, l16 = tid & 15, i = i0 + il;
           const bool valid = i < N;
-          const int iub = S.iub[valid ? type_of(S, i) : 0][sp];
+          const int ti = valid ? type_of(S, i) : 0;
           double zxr = 0, zxi = 0, zyr = 0, zyi = 0, t12 = 0;
-          for (int jl = l16; jl < ns; jl += 16) {
-            const int j = f0 + jl;
-            double jxx = 0, jxy = 0, jyy = 0;
-            if (valid) {
-              double qbx, qby;  // J[a][b] = dq_j[a]/dx_i[b]
-              if (j == i) {
-                jxx = 1.0 + m.Sb[3 * i];
-                jxy = m.Sb[3 * i + 1];
-                jyy = 1.0 + m.Sb[3 * i + 2];
-                qbx = m.qbd[2 * i];
-                qby = m.qbd[2 * i + 1];
-              } else {
-                bf_offdiag(S, m.x, i, j, iub, jxx, jxy, jyy, qbx, qby);
+          // columns in blocks of 32 (two per lane): the stored pair values of
+          // both are requested before either is used
+          for (int jb = 0; jb < ns; jb += 32) {
+            double pv[2][3];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+              const int jl = jb + l16 + 16 * u, j = f0 + jl;
+              pv[u][0] = pv[u][1] = pv[u][2] = 0.0;
+              if (pin && valid && jl < ns && j != i) {
+                const size_t e = (size_t)i * N + j;
+                pv[u][0] = __ldg(pin + e);
+                pv[u][1] = __ldg(pin + NN + e);
+                pv[u][2] = __ldg(pin + 2 * NN + e);
               }
-              const double fxr = m.fdg[4 * jl], fxi = m.fdg[4 * jl + 1];
-              const double fyr = m.fdg[4 * jl + 2], fyi = m.fdg[4 * jl + 3];
-              zxr += fxr * jxx + fyr * jxy;
-              zxi += fxi * jxx + fyi * jxy;
-              zyr += fxr * jxy + fyr * jyy;
-              zyi += fxi * jxy + fyi * jyy;
-              t12 -= fxr * qbx + fyr * qby;
-              const double jtj_xx = jxx * jxx + jxy * jxy;
-              const double jtj_xy = jxx * jxy + jxy * jyy;
-              const double jtj_yy = jxy * jxy + jyy * jyy;
-              t12 -= m.D2[3 * jl] * jtj_xx + 2.0 * m.D2[3 * jl + 1] * jtj_xy +
-                     m.D2[3 * jl + 2] * jtj_yy;
             }
-            UT[(2 * il + 0) * ldU + 0 * ns + jl] = jxx;  // a=x, b=x
-            UT[(2 * il + 1) * ldU + 0 * ns + jl] = jxy;  // a=x, b=y
-            UT[(2 * il + 0) * ldU + 1 * ns + jl] = jxy;  // a=y, b=x
-            UT[(2 * il + 1) * ldU + 1 * ns + jl] = jyy;  // a=y, b=y
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+              const int jl = jb + l16 + 16 * u;
+              if (jl >= ns) continue;
+              const int j = f0 + jl;
+              double jxx = 0, jxy = 0, jyy = 0;
+              if (valid) {
+                double qbx, qby;  // J[a][b] = dq_j[a]/dx_i[b]
+                if (j == i) {
+                  jxx = 1.0 + m.Sb[3 * i];
+                  jxy = m.Sb[3 * i + 1];
+                  jyy = 1.0 + m.Sb[3 * i + 2];
+                  qbx = m.qbd[2 * i];
+                  qby = m.qbd[2 * i + 1];
+                } else if (pin) {
+                  double rx = m.x[2 * i] - m.x[2 * j], ry = m.x[2 * i + 1] - m.x[2 * j + 1];
+                  rx = rx - S.el[0] * round(S.eli[0] * rx);
+                  ry = ry - S.el[1] * round(S.eli[1] * ry);
+                  const double t = pv[u][0], c = pv[u][1], w2 = pv[u][2];
+                  jxx = -(t + c * rx * rx);
+                  jxy = -(c * rx * ry);
+                  jyy = -(t + c * ry * ry);
+                  qbx = -w2 * rx;
+                  qby = -w2 * ry;
+                } else {
+                  bf_offdiag(S, m.x, i, j, ti, sp, jxx, jxy, jyy, qbx, qby);
+                }
+                const double fxr = m.fdg[4 * jl], fxi = m.fdg[4 * jl + 1];
+                const double fyr = m.fdg[4 * jl + 2], fyi = m.fdg[4 * jl + 3];
+                zxr += fxr * jxx + fyr * jxy;
+                zxi += fxi * jxx + fyi * jxy;
+                zyr += fxr * jxy + fyr * jyy;
+                zyi += fxi * jxy + fyi * jyy;
+                t12 -= fxr * qbx + fyr * qby;
+                const double jtj_xx = jxx * jxx + jxy * jxy;
+                const double jtj_xy = jxx * jxy + jxy * jyy;
+                const double jtj_yy = jxy * jxy + jyy * jyy;
+                t12 -= m.D2[3 * jl] * jtj_xx + 2.0 * m.D2[3 * jl + 1] * jtj_xy +
+                       m.D2[3 * jl + 2] * jtj_yy;
+              }
+              UT[(2 * il + 0) * ldU + 0 * ns + jl] = jxx;  // a=x, b=x
+              UT[(2 * il + 1) * ldU + 0 * ns + jl] = jxy;  // a=x, b=y
+              UT[(2 * il + 0) * ldU + 1 * ns + jl] = jxy;  // a=y, b=x
+              UT[(2 * il + 1) * ldU + 1 * ns + jl] = jyy;  // a=y, b=y
+            }
           }
 #pragma unroll
           for (int o = 8; o > 0; o >>= 1) {
@@ -1149,6 +1309,14 @@ __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl
   __syncthreads();
   phase_mark(S, PH_ASSEMBLE, tph);
   return status;
+}
+
+// The whole evaluation of the configuration in m.x (compute_properties,
+// reptation.f:2661).
+__device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl, double *props,
+                                  double *sign, long long &tph) {
+  eval_pairs<kThreads, false>(S, m, tph, nullptr, S.coef + S.cmb_off);
+  return eval_det(S, m, hl, props, sign, tph, nullptr);
 }
 
 }  // namespace q2d

@@ -267,12 +267,13 @@ int qmc2d_rmc_get_path(qmc2d_handle *h, int r, double *x, double *props);
 /* ----------------------------------------------------- streams and timing
  * The reference has no timers; these expose device time per kernel. */
 enum qmc2d_kernel {
-  QMC2D_KERNEL_MOVE = 0,    /* fused move + evaluation + accept (VMC/DMC) */
+  QMC2D_KERNEL_MOVE = 0,    /* evaluation after the pair passes + accept (VMC/DMC) */
   QMC2D_KERNEL_BRANCH = 1,  /* branch2 comb */
   QMC2D_KERNEL_GATHER = 2,  /* walker slot copies after branching */
   QMC2D_KERNEL_EVAL = 3,    /* batched compute_properties */
   QMC2D_KERNEL_RMC = 4,     /* reptation moves */
-  QMC2D_NKERNELS = 5
+  QMC2D_KERNEL_PAIRS = 5,   /* proposal + pair passes of a VMC/DMC move */
+  QMC2D_NKERNELS = 6
 };
 /* The handle's CUDA stream (a cudaStream_t) so callers can order work and
  * events after the library's launches. */
