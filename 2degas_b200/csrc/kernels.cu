@@ -202,6 +202,20 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
   const int N = S.N, N2 = 2 * N, np = S.nprops, nt = S.nt;
   const MoveScratch L = move_scratch(S);
   const double *o = a.scr + (size_t)w * L.stride;
+  if (S.has_bf) {
+    // the pair values are read by the Jacobian build long after this point;
+    // by now the pair kernel's writes for this walker have left L2, so bring
+    // them back (bulk L2 prefetch, 32 KB per request; the block is 256-byte
+    // aligned and 3 N^2 doubles long, a multiple of 8 bytes: round down to
+    // 16 bytes and let the tail come with the loads)
+    const size_t bytes = (sizeof(double) * 3 * (size_t)N * N) & ~size_t(15);
+    const char *base = reinterpret_cast<const char *>(o + L.pair);
+    for (size_t b0 = (size_t)tid * 32768; b0 < bytes; b0 += (size_t)kThreads * 32768) {
+      const unsigned sz = (unsigned)(bytes - b0 < 32768 ? bytes - b0 : 32768);
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + b0), "r"(sz)
+                   : "memory");
+    }
+  }
   for (int j = tid; j < N2; j += kThreads) {
     v.xo[j] = pop.x[(size_t)w * N2 + j];
     v.go[j] = pop.g[(size_t)w * N2 + j];

@@ -880,6 +880,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
                     sp ? m.dk[1] : m.dk[0], &m.iscal[sp], gt, Gr, 1 + sp,
                     sp ? m.gslot[1] : m.gslot[0], sp ? m.gkey[1] : m.gkey[0]);
       __syncthreads();
+      phase_mark(S, PH_INVERT, tph);
       compute_rhok(S, m, tid, kThreads);
       __syncthreads();
     } else {
@@ -909,7 +910,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
       logdet_sum = block_sum(ld_acc, m.red);
       if (m.iscal[0] || m.iscal[1]) status |= ST_SINGULAR;
     }
-    phase_mark(S, PH_INVERT, tph);
+    phase_mark(S, reg_path ? PH_RHOK : PH_INVERT, tph);
 
     for (int sp = 0; sp < nt; sp++) {
       const int ns = S.np[sp], ld = ws_ld(ns), f0 = S.ipfrst[sp];
