@@ -39,11 +39,21 @@ import numpy as np  # noqa: E402
 CONFIG = "dmc_bf_n58_rs5"
 METRIC = "walker-moves/sec (DMC with backflow, N=58 r_s=5, 4096 walkers)"
 UNIT = "walker-moves/s"
-# DRAM bytes (read + write) of one move_kernel launch per walker, from the ncu
-# capture summarised in profiles/move_kernel_dmc_bf_n58_296w.md (296 walkers,
-# scaled linearly: the traffic is the walker records read and written).
-MOVE_DRAM_BYTES_PER_WALKER = 2.040064e6 / 296
-TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 296-walker launch, x walkers/296"
+# DRAM bytes read per walker by one pairs_kernel + move_kernel pair of
+# launches, from the ncu capture summarised in
+# profiles/move_kernels_dmc_bf_n58_296w.md (296 walkers, scaled linearly: the
+# walker records and the move scratch), plus the move scratch block the pair
+# kernel writes, which reaches DRAM at 4096 walkers (356 MB > L2) though not
+# in the 296-walker capture.
+MOVE_DRAM_READ_PER_WALKER = (0.956160e6 + 27.777792e6) / 296
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum of pairs_kernel + move_kernel (296 walkers) "
+                  "x walkers/296, + the move scratch written per walker")
+
+
+def move_scratch_bytes(N):
+    """Bytes of one walker's move scratch block (MoveScratch, backflow)."""
+    pair = (14 * N + 1 + 3) & ~3
+    return 8 * ((pair + 3 * N * N + 31) & ~31)
 
 
 def flops_per_move(N, ns, K, u3, backflow):
@@ -375,7 +385,7 @@ def b200_arm(args, rank, world, local_rank):
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": MOVE_DRAM_BYTES_PER_WALKER * nw,
+                         "traffic": (MOVE_DRAM_READ_PER_WALKER + move_scratch_bytes(N)) * nw,
                          "traffic_source": TRAFFIC_SOURCE,
                          "kernel": "pairs_kernel + move_kernel",
                          "flops_per_move": fpm,
