@@ -839,6 +839,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
                                double *sign, long long &tph, const double *pin) {
   const int tid = threadIdx.x;
   const int N = S.N, nt = S.nt;
+  const int lane8 = tid & (kGroup - 1);
   const size_t NN = (size_t)N * N;
 
   // ---- backflow Slater determinants (slater_excitations, reptation.f:9967)
@@ -960,21 +961,30 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
             }
         }
       }
-      // D2(j)[ab] = Re sum_k Ainv(j,k) (-g_ka g_kb) A(k,j)  (ddzorb term)
-      for (int j = tid; j < ns; j += kThreads) {
+      // D2(j)[ab] = Re sum_k Ainv(j,k) (-g_ka g_kb) A(k,j)  (ddzorb term),
+      // 8 lanes per electron, fixed shuffle order
+      for (int base = 0; base < ns; base += kThreads / kGroup) {
+        const int j = base + tid / kGroup;
         double dxx = 0, dxy = 0, dyy = 0;
-        const double2 *wj = W + pm[j] * ld;
-        for (int c = 0; c < ns; c++) {
-          const int pc = pm[c];
-          double pr = wj[c].x * A[pc + j * ns].x - wj[c].y * A[pc + j * ns].y;
-          double gx = m.gsh[2 * pc], gy = m.gsh[2 * pc + 1];
-          dxx -= gx * gx * pr;
-          dxy -= gx * gy * pr;
-          dyy -= gy * gy * pr;
+        if (j < ns) {
+          const double2 *wj = W + pm[j] * ld;
+          for (int c = lane8; c < ns; c += kGroup) {
+            const int pc = pm[c];
+            double pr = wj[c].x * A[pc + j * ns].x - wj[c].y * A[pc + j * ns].y;
+            double gx = m.gsh[2 * pc], gy = m.gsh[2 * pc + 1];
+            dxx -= gx * gx * pr;
+            dxy -= gx * gy * pr;
+            dyy -= gy * gy * pr;
+          }
         }
-        m.D2[3 * j] = dxx;
-        m.D2[3 * j + 1] = dxy;
-        m.D2[3 * j + 2] = dyy;
+        dxx = group8_sum(dxx);
+        dxy = group8_sum(dxy);
+        dyy = group8_sum(dyy);
+        if (j < ns && lane8 == 0) {
+          m.D2[3 * j] = dxx;
+          m.D2[3 * j + 1] = dxy;
+          m.D2[3 * j + 2] = dyy;
+        }
       }
       __syncthreads();
       phase_mark(S, PH_FMAT, tph);
