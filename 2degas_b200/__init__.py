@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _capi
 
-__all__ = ["System", "Handle", "QMCError", "load_library", "_capi"]
+__all__ = ["System", "Handle", "Stats", "QMCError", "load_library", "_capi"]
 
 QMCError = _capi.QMCError
 
@@ -225,3 +225,73 @@ class Handle:
         p = np.zeros((ntau, np_))
         self._chk(self.lib.qmc2d_rmc_get_path(self.h, rep, _pd(x), _pd(p)))
         return x, p
+
+    def write_conf(self, directory, rank=0):
+        """write_conf: the population's coordinates to <dir>/<x_file>.<rank>."""
+        self._chk(self.lib.qmc2d_write_conf(self.h, self.system.ptr, str(directory).encode(),
+                                            rank))
+
+    def restart_write(self, stats, iblk, who, directory, runid, rank=0):
+        """restart(1): <dir>/<runid>.res and <dir>/<x_file>.res.<rank>."""
+        self._chk(self.lib.qmc2d_restart_write(self.h, self.system.ptr, stats.p, iblk,
+                                               who.encode(), str(directory).encode(),
+                                               runid.encode(), rank))
+
+    def restart_read(self, stats, who, directory, runid, rank=0):
+        """restart(0): returns (stored block, etrial); the configurations
+        become the population."""
+        ib = ctypes.c_int()
+        et = ctypes.c_double()
+        self._chk(self.lib.qmc2d_restart_read(self.h, self.system.ptr, stats.p, who.encode(),
+                                              str(directory).encode(), runid.encode(), rank,
+                                              ctypes.byref(ib), ctypes.byref(et)))
+        return ib.value, et.value
+
+
+class Stats:
+    """Cumulative block statistics of averages(3) (qmc2d_stats_*)."""
+
+    def __init__(self, system):
+        self.system = system
+        self.lib = system.lib
+        self.p = ctypes.c_void_p()
+        _capi.check(self.lib, self.lib.qmc2d_stats_create(system.nprops, ctypes.byref(self.p)))
+
+    def __del__(self):
+        try:
+            if self.p:
+                self.lib.qmc2d_stats_destroy(self.p)
+                self.p = None
+        except Exception:
+            pass
+
+    def add_block(self, blk, norm):
+        blk = np.ascontiguousarray(blk, dtype=np.float64)
+        _capi.check(self.lib, self.lib.qmc2d_stats_add_block(self.p, _pd(blk), norm))
+
+    def get(self):
+        """(cumulative means, errors, cml_norm, blocks)."""
+        n = self.system.nprops
+        mean, err = np.zeros(n), np.zeros(n)
+        norm, ib = ctypes.c_double(), ctypes.c_int()
+        _capi.check(self.lib, self.lib.qmc2d_stats_get(self.p, _pd(mean), _pd(err),
+                                                       ctypes.byref(norm), ctypes.byref(ib)))
+        return mean, err, norm.value, ib.value
+
+    def report(self, blk, norm, who):
+        """The averages(3) block report text."""
+        blk = np.ascontiguousarray(blk, dtype=np.float64)
+        need = ctypes.c_size_t()
+        _capi.check(self.lib, self.lib.qmc2d_stats_report(self.p, self.system.ptr, _pd(blk), norm,
+                                                          who.encode(), None, 0,
+                                                          ctypes.byref(need)))
+        buf = ctypes.create_string_buffer(need.value)
+        _capi.check(self.lib, self.lib.qmc2d_stats_report(self.p, self.system.ptr, _pd(blk), norm,
+                                                          who.encode(), buf, need.value, None))
+        return buf.value.decode()
+
+    def write_rhok(self, blk, norm, directory, runid):
+        blk = np.ascontiguousarray(blk, dtype=np.float64)
+        _capi.check(self.lib, self.lib.qmc2d_stats_write_rhok(self.p, self.system.ptr, _pd(blk),
+                                                              norm, str(directory).encode(),
+                                                              runid.encode()))

@@ -172,6 +172,20 @@ SIGNATURES = {
     "qmc2d_block_reset": (c_int, [c_void_p]),
     "qmc2d_block_get": (c_int, [c_void_p, PD, PD]),
     "qmc2d_counters_get": (c_int, [c_void_p, POINTER(Counters)]),
+    "qmc2d_stats_create": (c_int, [c_int, POINTER(c_void_p)]),
+    "qmc2d_stats_destroy": (c_int, [c_void_p]),
+    "qmc2d_stats_add_block": (c_int, [c_void_p, PD, c_double]),
+    "qmc2d_stats_get": (c_int, [c_void_p, PD, PD, PD, POINTER(c_int)]),
+    "qmc2d_stats_report": (c_int, [c_void_p, SYSP, PD, c_double, ctypes.c_char_p,
+                                   ctypes.c_char_p, ctypes.c_size_t,
+                                   POINTER(ctypes.c_size_t)]),
+    "qmc2d_stats_write_rhok": (c_int, [c_void_p, SYSP, PD, c_double, ctypes.c_char_p,
+                                       ctypes.c_char_p]),
+    "qmc2d_write_conf": (c_int, [c_void_p, SYSP, ctypes.c_char_p, c_int]),
+    "qmc2d_restart_write": (c_int, [c_void_p, SYSP, c_void_p, c_int, ctypes.c_char_p,
+                                    ctypes.c_char_p, ctypes.c_char_p, c_int]),
+    "qmc2d_restart_read": (c_int, [c_void_p, SYSP, c_void_p, ctypes.c_char_p, ctypes.c_char_p,
+                                   ctypes.c_char_p, c_int, POINTER(c_int), PD]),
     "qmc2d_vmc": (c_int, [c_void_p, c_int, c_double, c_int]),
     "qmc2d_dmc": (c_int, [c_void_p, c_int, c_int, c_double, c_double, c_double, c_int]),
     "qmc2d_rmc_init": (c_int, [c_void_p, c_int, POINTER(RmcParams), PD]),

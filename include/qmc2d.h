@@ -234,6 +234,59 @@ typedef struct qmc2d_counters {
 } qmc2d_counters;
 int qmc2d_counters_get(qmc2d_handle *h, qmc2d_counters *c);
 
+/* ------------------------------------------------------ block statistics
+ * averages(3) (reptation.f:4305-4352) on the host: cumulative sums over
+ * blocks, the error bars, the block report and the rho_k files. */
+typedef struct qmc2d_stats qmc2d_stats;
+int qmc2d_stats_create(int n_props, qmc2d_stats **out);
+int qmc2d_stats_destroy(qmc2d_stats *st);
+/* Fold one block (sums and norm as from qmc2d_block_get, over all walkers):
+ * cml_av += blk, cml2 += blk^2 / blk_norm, cml_norm += blk_norm, iblk += 1
+ * (reptation.f:4318-4322). */
+int qmc2d_stats_add_block(qmc2d_stats *st, const double *blk, double blk_norm);
+/* Cumulative means cml_av/cml_norm, errors
+ * sqrt(|cml2/cml_norm - mean^2| / (iblk-1)) (0 for one block,
+ * reptation.f:4336-4341), cml_norm and the block count; pointers may be NULL.
+ * The DMC trial energy of dmc blocks is mean[QMC2D_JETOT] (:4328). */
+int qmc2d_stats_get(const qmc2d_stats *st, double *mean, double *err, double *cml_norm,
+                    int *iblk);
+/* The block report of averages(3): " ===>> <who> block <iblk>", then per
+ * scalar property block mean, cumulative mean, error, block norm and name in
+ * the reference's format (2e19.11,e9.2,e10.3,2x,a20; :4343-4345), into buf
+ * (NUL-terminated; QMC2D_ERR_LIMIT if len is short). *needed gets the size. */
+int qmc2d_stats_report(const qmc2d_stats *st, const qmc2d_system *sys, const double *blk,
+                       double blk_norm, const char *who, char *buf, size_t len, size_t *needed);
+/* write_nonscalar_props for the rho_k slots (reptation.f:4349-4357, 4582):
+ * <dir>/<runid>.rhok_<type>, one line per component
+ * (2e19.11,e9.2,e10.3,1x,a7,i5). */
+int qmc2d_stats_write_rhok(const qmc2d_stats *st, const qmc2d_system *sys, const double *blk,
+                           double blk_norm, const char *dir, const char *runid);
+
+/* ---------------------------------------------------------- checkpoints */
+/* write_conf (reptation.f:2504): the population's coordinates to the
+ * per-type files <dir>/<x_file(type)>.<rank>, one "x y" line per particle,
+ * walker after walker; qmc2d_read_configs reads them with suffix ".<rank>". */
+int qmc2d_write_conf(qmc2d_handle *h, const qmc2d_system *sys, const char *dir, int rank);
+/* restart(1) (reptation.f:4448-4507): <dir>/<runid>.res holds "iblk who",
+ * cml_norm, one "cml_av cml2" line per property, the random-stream state
+ * line and, when ntheta != 0, "ith jth"; the coordinates go to
+ * <dir>/<x_file(type)>.res.<rank>: every walker for who "vmc" or "dmc",
+ * every reptile's ntau-bead path for "rmc". The state line holds this
+ * library's counter-based streams (seed low and high words, move,
+ * generation and reptation counters, three zeros) in the place of the
+ * rannyu/rannyu2 seed words. */
+int qmc2d_restart_write(qmc2d_handle *h, const qmc2d_system *sys, const qmc2d_stats *st,
+                        int iblk, const char *who, const char *dir, const char *runid,
+                        int rank);
+/* restart(0) (reptation.f:4508-4540) for who "vmc" or "dmc": the .res file
+ * back into st and the handle's streams, *iblk = the stored block (the
+ * caller continues at mod(iblk, nblk)+1), *etrial = cml_av(jetot)/cml_norm,
+ * and the stored configurations become the population (as
+ * qmc2d_population_set). */
+int qmc2d_restart_read(qmc2d_handle *h, const qmc2d_system *sys, qmc2d_stats *st,
+                       const char *who, const char *dir, const char *runid, int rank,
+                       int *iblk, double *etrial);
+
 /* VMC: nstp steps of move + metropolis_test + averages(2) on every walker
  * (vmc loop body, reptation.f:995-1003; move :4617; metropolis_test :2622).
  * mage forces a move after that many consecutive rejections (<=0: never). */
