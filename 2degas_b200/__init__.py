@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _capi
 
-__all__ = ["System", "Handle", "Stats", "QMCError", "load_library", "_capi"]
+__all__ = ["System", "Handle", "Stats", "tabc", "QMCError", "load_library", "_capi"]
 
 QMCError = _capi.QMCError
 
@@ -226,6 +226,10 @@ class Handle:
         self._chk(self.lib.qmc2d_rmc_get_path(self.h, rep, _pd(x), _pd(p)))
         return x, p
 
+    def update_twist(self):
+        """After system.set_twist(ith, jth): the orbitals use the new wave vectors."""
+        self._chk(self.lib.qmc2d_update_twist(self.h, self.system.ptr))
+
     def write_conf(self, directory, rank=0):
         """write_conf: the population's coordinates to <dir>/<x_file>.<rank>."""
         self._chk(self.lib.qmc2d_write_conf(self.h, self.system.ptr, str(directory).encode(),
@@ -295,3 +299,39 @@ class Stats:
         _capi.check(self.lib, self.lib.qmc2d_stats_write_rhok(self.p, self.system.ptr, _pd(blk),
                                                               norm, str(directory).encode(),
                                                               runid.encode()))
+
+
+def tabc(handle, run, ntheta=None, resume=None, dmc_preequilibrate=None):
+    """The twist loop of tabc (reptation.f:9559-9636): for ith, jth =
+    1..ntheta (jth fastest) set the twist's wave vectors, then call
+    run(handle, ith, jth); the walkers carry over from one twist to the next.
+
+    resume = (ith, jth, iblk0) continues a restarted run the reference's way
+    (:9567-9576): at the stored twist if iblk0 != 1, else at the next one.
+    dmc_preequilibrate(handle), when given, runs before run() at every twist
+    that is not resumed mid-way, like the reference's short DMC (one block of
+    min(100, nstp) steps at delta/4, :9621-9632).
+    Returns the list of twists visited."""
+    system = handle.system
+    nth = ntheta if ntheta is not None else system.s.ntheta
+    if nth <= 0:
+        raise ValueError("tabc: ntheta must be positive")
+    i0, j0, mid = 1, 1, False
+    if resume is not None:
+        ith, jth, iblk0 = resume
+        if iblk0 != 1:
+            i0, j0, mid = ith, jth, True
+        else:
+            i0, j0 = ith + jth // nth, jth % nth + 1
+    done = []
+    for ith in range(i0, nth + 1):
+        for jth in range(j0, nth + 1):
+            system.set_twist(ith, jth)
+            handle.update_twist()
+            if dmc_preequilibrate is not None and not mid:
+                dmc_preequilibrate(handle)
+            mid = False
+            run(handle, ith, jth)
+            done.append((ith, jth))
+        j0 = 1
+    return done

@@ -172,6 +172,7 @@ SIGNATURES = {
     "qmc2d_block_reset": (c_int, [c_void_p]),
     "qmc2d_block_get": (c_int, [c_void_p, PD, PD]),
     "qmc2d_counters_get": (c_int, [c_void_p, POINTER(Counters)]),
+    "qmc2d_update_twist": (c_int, [c_void_p, SYSP]),
     "qmc2d_stats_create": (c_int, [c_int, POINTER(c_void_p)]),
     "qmc2d_stats_destroy": (c_int, [c_void_p]),
     "qmc2d_stats_add_block": (c_int, [c_void_p, PD, c_double]),

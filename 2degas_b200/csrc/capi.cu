@@ -234,6 +234,7 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
   h->hs.coef = h->d_coef;
   h->hs.kvec = h->d_kvec;
   h->hs.gvec = h->d_gvec;
+  h->gvec_cap = std::max(1, sys->ngvec);
   if ((e = dalloc(&h->ds, 1)) != cudaSuccess) return fail(cuda_fail(e, "alloc"));
   cudaMemcpy(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice);
   int cap = h->cap, N = h->N, nt = h->nt, np = h->nprops;
@@ -265,6 +266,25 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
   cudaMemset(h->br.ncapped, 0, sizeof(int));
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(cuda_fail(e, "create"));
   *out = h;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_update_twist(qmc2d_handle *h, const qmc2d_system *sys) {
+  if (!h || !sys || !sys->gvec || sys->ngvec <= 0 || sys->nptot != h->N) {
+    q2d::set_error("qmc2d_update_twist: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  if (sys->ngvec > h->gvec_cap) {
+    q2d::set_error("qmc2d_update_twist: more wave vectors than the handle was created with");
+    return QMC2D_ERR_LIMIT;
+  }
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(h->d_gvec, sys->gvec, sizeof(double) * 2 * sys->ngvec,
+                     cudaMemcpyHostToDevice, h->stream));
+  h->hs.ngvec = sys->ngvec;
+  CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
+  // sys->gvec is replaced by the next qmc2d_system_set_twist: finish reading it
+  CK(cudaStreamSynchronize(h->stream));
   return QMC2D_OK;
 }
 

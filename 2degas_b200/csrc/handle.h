@@ -15,6 +15,7 @@ struct qmc2d_handle {
   q2d::DevSys hs{};
   q2d::DevSys *ds = nullptr;
   double *d_coef = nullptr, *d_kvec = nullptr, *d_gvec = nullptr;
+  int gvec_cap = 0;  // wave vectors d_gvec holds
   int cap = 0, nw = 0, cur = 0;
   int nt = 0, N = 0, nprops = 0;
   q2d::DevPop pop[2]{};

@@ -170,6 +170,11 @@ typedef struct qmc2d_options {
 /* Copy the system's tables to the device and allocate walker storage. */
 int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt, qmc2d_handle **out);
 int qmc2d_destroy(qmc2d_handle *h);
+/* After qmc2d_system_set_twist on the handle's system, make the handle's
+ * orbitals use the new wave vectors (the gvec/gtens reset at each twist of
+ * tabc, reptation.f:9581-9616); the population is left as it is, as in the
+ * reference, which carries its walkers from one twist to the next. */
+int qmc2d_update_twist(qmc2d_handle *h, const qmc2d_system *sys);
 
 /* compute_properties (reptation.f:2661): for nw configurations x (2*nptot
  * each) compute g = -grad ln psi (2*nptot), hlap = -lap ln psi per type

@@ -52,3 +52,30 @@ def test_restart_continues_the_chain(q, n26, n26_configs, tmp_path):
     assert etrial == pytest.approx(m1[0], rel=1e-15)
     # the re-evaluated walkers continue the same Philox chain
     np.testing.assert_allclose(x_new, x_ref, rtol=0, atol=1e-9)
+
+
+def test_update_twist_matches_a_fresh_handle(q, n26, n26_configs):
+    """A handle moved to twist (2, 3) evaluates like one created there."""
+    x = n26_configs[:8]
+    with q.Handle(n26, capacity=8, seed=1) as h:
+        n26.set_twist(2, 3)
+        h.update_twist()
+        g1, hl1, p1, s1 = h.compute_properties(x)
+    with q.Handle(n26, capacity=8, seed=1) as h2:
+        g2, hl2, p2, s2 = h2.compute_properties(x)
+    n26.set_twist(1, 1)
+    assert np.array_equal(g1, g2) and np.array_equal(p1, p2)
+
+
+def test_tabc_visits_the_grid_in_order(q, n26, n26_configs):
+    x0 = n26_configs[:8]
+    seen = []
+    with q.Handle(n26, capacity=8, seed=2) as h:
+        h.population_set(x0)
+        done = q.tabc(h, lambda hh, i, j: (hh.vmc(1, DELTA, 10 ** 9), seen.append((i, j))),
+                      ntheta=2)
+        # resume after a restart stored at twist (1, 2), block 1: next twist
+        rest = q.tabc(h, lambda hh, i, j: None, ntheta=2, resume=(1, 2, 1))
+    n26.set_twist(1, 1)
+    assert done == seen == [(1, 1), (1, 2), (2, 1), (2, 2)]
+    assert rest == [(2, 1), (2, 2)]
