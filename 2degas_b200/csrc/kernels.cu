@@ -119,40 +119,45 @@ size_t move_smem_bytes(const DevSys &s) {
 // reverse move, metropolis_test and the averages, with the walker's state
 // in shared memory.
 //
-// pairs_kernel is persistent: one CTA of kPairThreads per SM walks over the
-// population. Its random spline-row lookups (three per pair) go to a
-// shared-memory copy of the pair rows when they fit (stage_rows), made once
-// per launch; random rows in global memory cost an L1 tag lookup per lane,
-// shared memory a few bank wavefronts per warp.
-constexpr int kPairThreads = 512;
+// pairs_kernel is persistent: one CTA per SM walks over the population with
+// kPairGroups independent groups of kThreads threads, each on its own walker
+// and its own named barrier, so one group's latency overlaps the other's.
+// Its random spline-row lookups (three per pair) go to a shared-memory copy
+// of the pair rows when they fit (stage_rows), made once per launch and
+// shared by the groups; random rows in global memory cost an L1 tag lookup
+// per lane, shared memory a few bank wavefronts per warp.
+constexpr int kPairGroups = 2;
+constexpr int kPairThreads = kPairGroups * kThreads;
 
 __global__ void __launch_bounds__(kPairThreads, 1) pairs_kernel(const DevSys *sp, DevPop pop,
                                                                 MoveArgs a, int stage_rows) {
   __shared__ DevSys S;
   extern __shared__ __align__(16) char smem[];
   load_sys(S, sp);
+  const size_t carve = (pair_carve(S, nullptr, nullptr, kThreads) + 127) & ~size_t(127);
+  const int grp = threadIdx.x / kThreads, tid = threadIdx.x - grp * kThreads;
   EvalSmem m;
-  const size_t off = (pair_carve(S, smem, &m, kPairThreads) + 127) & ~size_t(127);
-  const int tid = threadIdx.x;
+  pair_carve(S, smem + grp * carve, &m, kThreads);
   const double *rows_g = S.coef + S.cmb_off;
-  double *rows_s = reinterpret_cast<double *>(smem + off);
+  double *rows_s = reinterpret_cast<double *>(smem + kPairGroups * carve);
   if (stage_rows) {  // 16-double rows to kPairRowSh-double rows
     const int nrow = S.cmb_nblk * (S.cmb_ng + 1);
     const double2 *src = reinterpret_cast<const double2 *>(rows_g);
-    for (int e = tid; e < nrow * 8; e += kPairThreads) {
+    for (int e = threadIdx.x; e < nrow * 8; e += kPairThreads) {
       const int r = e >> 3, q = e & 7;
       reinterpret_cast<double2 *>(rows_s + (size_t)r * kPairRowSh)[q] = __ldg(src + e);
     }
-    __syncthreads();
   }
+  __syncthreads();
+  const GroupSync sync{1 + grp, kThreads};
   const int N = S.N, N2 = 2 * N;
   const uint32_t step = a.step0;
   const double pi = 3.141592653589793;
   const MoveScratch L = move_scratch(S);
-  for (int w = blockIdx.x; w < a.nw; w += gridDim.x) {
+  for (int w = blockIdx.x * kPairGroups + grp; w < a.nw; w += gridDim.x * kPairGroups) {
     long long tph = clock64();
     double wo = 0.0;
-    for (int j = tid; j < N2; j += kPairThreads) {
+    for (int j = tid; j < N2; j += kThreads) {
       int ti = type_of(S, j >> 1);
       double var = 2.0 * S.hbs2m[ti] * a.delta, vari = 1.0 / var;
       double2 u = uniform2(a.seed, (uint32_t)j, (uint32_t)w, step, 0u);
@@ -160,29 +165,31 @@ __global__ void __launch_bounds__(kPairThreads, 1) pairs_kernel(const DevSys *sp
       wo -= chi * chi * vari;
       m.x[j] = chi + (-var * pop.g[(size_t)w * N2 + j]) + pop.x[(size_t)w * N2 + j];
     }
-    const double wold = block_sum_t<kPairThreads>(wo, m.red);
-    phase_mark(S, PH_PROPOSE, tph);
+    const double wold = block_sum_t<kThreads>(wo, m.red, sync, tid);
+    phase_mark(S, PH_PROPOSE, tph, tid == 0);
     double *o = a.scr + (size_t)w * L.stride;
     double *pout = S.has_bf ? o + L.pair : nullptr;
     if (stage_rows)
-      eval_pairs<kPairThreads, true>(S, m, tph, pout, rows_s);
+      eval_pairs<kThreads, true>(S, m, tph, pout, rows_s, sync, tid);
     else
-      eval_pairs<kPairThreads, false>(S, m, tph, pout, rows_g);
-    __syncthreads();
-    for (int j = tid; j < N2; j += kPairThreads) {
+      eval_pairs<kThreads, false>(S, m, tph, pout, rows_g, sync, tid);
+    compute_rhok(S, m, tid, kThreads);
+    sync();
+    for (int j = tid; j < 4 * S.nk; j += kThreads) o[L.rhok + j] = m.rhok[j];
+    for (int j = tid; j < N2; j += kThreads) {
       o[L.x + j] = m.x[j];
       o[L.g + j] = m.g[j];
       o[L.q + j] = m.q[j];
       o[L.qbd + j] = m.qbd[j];
     }
-    for (int j = tid; j < 3 * N; j += kPairThreads) o[L.sb + j] = m.Sb[j];
-    for (int j = tid; j < N; j += kPairThreads) {
+    for (int j = tid; j < 3 * N; j += kThreads) o[L.sb + j] = m.Sb[j];
+    for (int j = tid; j < N; j += kThreads) {
       o[L.lap + j] = m.lap[j];
       o[L.ltf + j] = m.ltf[j];
       o[L.vp + j] = m.vp[j];
     }
     if (tid == 0) o[L.wold] = wold;
-    __syncthreads();  // m is reused by the next walker
+    sync();  // m is reused by the group's next walker
   }
 }
 
@@ -250,7 +257,8 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
   const uint32_t step = a.step0;
   long long tph = clock64();
   double sn = 1.0;
-  status |= eval_det(S, m, v.hn, v.pn, &v.sc[0], tph, S.has_bf ? o + L.pair : nullptr);
+  status |= eval_det(S, m, v.hn, v.pn, &v.sc[0], tph, S.has_bf ? o + L.pair : nullptr,
+                     o + L.rhok);
   sn = v.sc[0];
   // reverse move (reptation.f:4660-4674)
   double wn = 0.0;
@@ -519,12 +527,14 @@ cudaError_t launch_pairs(const DevSys &hs, const DevSys *ds, DevPop pop, const M
   if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) !=
       cudaSuccess)
     return e;
-  const size_t carve = (pair_carve(hs, nullptr, nullptr, kPairThreads) + 127) & ~size_t(127);
+  const size_t carve =
+      kPairGroups * ((pair_carve(hs, nullptr, nullptr, kThreads) + 127) & ~size_t(127));
   const size_t rows = sizeof(double) * kPairRowSh * (size_t)hs.cmb_nblk * (hs.cmb_ng + 1);
   const int stage = carve + rows + sizeof(DevSys) <= (size_t)optin ? 1 : 0;
   const size_t sm = carve + (stage ? rows : 0);
   if ((e = set_smem((const void *)pairs_kernel, sm)) != cudaSuccess) return e;
-  const int grid = a.nw < nsm ? a.nw : nsm;
+  const int need = (a.nw + kPairGroups - 1) / kPairGroups;
+  const int grid = need < nsm ? need : nsm;
   pairs_kernel<<<grid, kPairThreads, sm, st>>>(ds, pop, a, stage);
   return cudaGetLastError();
 }

@@ -181,6 +181,7 @@ __host__ __device__ inline size_t pair_carve(const DevSys &s, char *base, EvalSm
   t.gd = (double *)take(sizeof(double) * 2 * N);
   t.lapd = (double *)take(sizeof(double) * N);
   t.ph2d = (double *)take(sizeof(double) * N);
+  t.rhok = (double *)take(sizeof(double) * 2 * (s.nk > 0 ? s.nk : 1) * 2);
   t.red = (double *)take(sizeof(double) * nthreads);
   if (m) *m = t;
   return off;
@@ -189,10 +190,11 @@ __host__ __device__ inline size_t pair_carve(const DevSys &s, char *base, EvalSm
 // Per-walker move scratch in global memory (doubles), written by the pair
 // kernel and read by the move kernel of the same step: the proposed
 // configuration, the pair passes' per-particle sums, the proposal's log
-// density, and (backflow) the spline values of every ordered pair (i, j):
+// density, rho_k (both slots), and (backflow) the spline values of every
+// ordered pair (i, j):
 // eta(r_ij), eta'(r_ij)/r_ij and 3 eta'/r + eta'' at [k N^2 + i N + j].
 struct MoveScratch {
-  int x, g, q, sb, qbd, lap, ltf, vp, wold, pair;
+  int x, g, q, sb, qbd, lap, ltf, vp, wold, rhok, pair;
   size_t stride;
 };
 __host__ __device__ inline MoveScratch move_scratch(const DevSys &s) {
@@ -207,7 +209,8 @@ __host__ __device__ inline MoveScratch move_scratch(const DevSys &s) {
   l.ltf = 12 * N;
   l.vp = 13 * N;
   l.wold = 14 * N;
-  l.pair = (14 * N + 1 + 3) & ~3;
+  l.rhok = 14 * N + 1;
+  l.pair = (14 * N + 1 + 4 * (s.nk > 0 ? s.nk : 1) + 3) & ~3;
   size_t end = (size_t)l.pair + (s.has_bf ? 3 * (size_t)N * N : 0);
   l.stride = (end + 31) & ~size_t(31);  // 256-byte aligned walker blocks
   return l;
@@ -354,17 +357,31 @@ __device__ __forceinline__ void block_sum_n(double (&v)[K], double *red) {
   __syncthreads();
 }
 
-// Deterministic sum over a block of NT threads (NT/32 warps); red[0 .. NT/32).
-template <int NT>
-__device__ __forceinline__ double block_sum_t(double v, double *red) {
+// Barriers of a group of threads: the whole CTA, or the `n` threads that use
+// named barrier `id` (whole warps; a CTA running several walkers).
+struct CtaSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct GroupSync {
+  int id, n;
+  __device__ __forceinline__ void operator()() const {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+  }
+};
+
+// Deterministic sum over a group of NT threads (NT/32 warps) with index tid
+// in the group and barrier sync; red[0 .. NT/32).
+template <int NT, class Sync = CtaSync>
+__device__ __forceinline__ double block_sum_t(double v, double *red, Sync sync = Sync(),
+                                              int tid = threadIdx.x) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
+  const int w = tid >> 5, l = tid & 31;
+  sync();
   if (l == 0) red[w] = v;
-  __syncthreads();
+  sync();
   double t = 0.0;
   for (int ww = 0; ww < NT / 32; ww++) t += red[ww];
-  __syncthreads();
+  sync();
   return t;
 }
 
@@ -375,12 +392,16 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 }
 
 // Adds the SM cycles since t to phase k (thread 0 only, when timers are on).
-__device__ __forceinline__ void phase_mark(const DevSys &S, int k, long long &t) {
-  if (S.phase != nullptr && threadIdx.x == 0) {
+// (lead: the thread that records, thread 0 of its group.)
+__device__ __forceinline__ void phase_mark(const DevSys &S, int k, long long &t, bool lead) {
+  if (S.phase != nullptr && lead) {
     long long now = clock64();
     atomicAdd(&S.phase[k], (unsigned long long)(now - t));
     t = now;
   }
+}
+__device__ __forceinline__ void phase_mark(const DevSys &S, int k, long long &t) {
+  phase_mark(S, k, t, threadIdx.x == 0);
 }
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -667,10 +688,12 @@ __device__ inline void compute_rhok(const DevSys &S, const EvalSmem &m, int t, i
 // spline values of every ordered pair, laid out as in MoveScratch.
 // NT threads (a multiple of 32) run the passes; the pair rows are read at
 // `rows`, from shared memory when kSh.
-template <int NT, bool kSh>
+// Sync is the barrier of the NT threads (the CTA, or a named-barrier group
+// of a CTA that runs several walkers); tid is the thread's index among them.
+template <int NT, bool kSh, class Sync = CtaSync>
 __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long &tph,
-                                  double *pout, const double *rows) {
-  const int tid = threadIdx.x;
+                                  double *pout, const double *rows, Sync sync = Sync(),
+                                  int tid = threadIdx.x) {
   const int N = S.N;
   const int lane8 = tid & (kGroup - 1);
   const int per_round = NT / kGroup;
@@ -786,8 +809,8 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
       m.ph2d[i] = 0.0;
     }
   }
-  __syncthreads();
-  phase_mark(S, PH_PAIRS, tph);
+  sync();
+  phase_mark(S, PH_PAIRS, tph, tid == 0);
 
   // ---- pass B: u3 gradient and Laplacian from the G vectors.
   if (S.has_u3) {
@@ -826,8 +849,8 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
         m.ltf[k] -= 0.5 * (Gkx * Gkx + Gky * Gky);
       }
     }
-    __syncthreads();
-    phase_mark(S, PH_U3, tph);
+    sync();
+    phase_mark(S, PH_U3, tph, tid == 0);
   }
 }
 
@@ -836,8 +859,16 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
 // backflow Jacobian blocks take the pair spline values written by
 // eval_pairs(pout) instead of evaluating them again.
 __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, double *props,
-                               double *sign, long long &tph, const double *pin) {
+                               double *sign, long long &tph, const double *pin,
+                               const double *rhok_in = nullptr) {
   const int tid = threadIdx.x;
+  // rho_k of both slots: copied when given (MoveScratch), else summed
+  auto rhok = [&](int t0, int nthr) {
+    if (rhok_in)
+      for (int e = t0; e < 4 * S.nk; e += nthr) m.rhok[e] = rhok_in[e];
+    else
+      compute_rhok(S, m, t0, nthr);
+  };
   const int N = S.N, nt = S.nt;
   const int lane8 = tid & (kGroup - 1);
   const size_t NN = (size_t)N * N;
@@ -882,7 +913,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
                     sp ? m.gslot[1] : m.gslot[0], sp ? m.gkey[1] : m.gkey[0]);
       __syncthreads();
       phase_mark(S, PH_INVERT, tph);
-      compute_rhok(S, m, tid, kThreads);
+      rhok(tid, kThreads);
       __syncthreads();
     } else {
       // warps per spin: half the CTA for the inversions, the rest for rho_k
@@ -895,11 +926,11 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
                   sp ? m.dk[1] : m.dk[0], sp ? m.used[1] : m.used[0], &m.iscal[sp], gt,
                   G, 1 + sp, m.gval + 8 * sp, m.gidx + 8 * sp);
       } else {
-        compute_rhok(S, m, tid - G * nt * 32, kThreads - G * nt * 32);
+        rhok(tid - G * nt * 32, kThreads - G * nt * 32);
       }
       __syncthreads();
       if (G * nt == kThreads / 32) {
-        compute_rhok(S, m, tid, kThreads);
+        rhok(tid, kThreads);
         __syncthreads();
       }
     }
@@ -1165,7 +1196,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
       }
     }
   } else {
-    compute_rhok(S, m, tid, kThreads);
+    rhok(tid, kThreads);
     __syncthreads();
     phase_mark(S, PH_RHOK, tph);
   }

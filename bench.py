@@ -50,9 +50,9 @@ TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum of pairs_kernel + move_kernel (296 w
                   "x walkers/296, + the move scratch written per walker")
 
 
-def move_scratch_bytes(N):
+def move_scratch_bytes(N, nk):
     """Bytes of one walker's move scratch block (MoveScratch, backflow)."""
-    pair = (14 * N + 1 + 3) & ~3
+    pair = (14 * N + 1 + 4 * max(nk, 1) + 3) & ~3
     return 8 * ((pair + 3 * N * N + 31) & ~31)
 
 
@@ -385,7 +385,7 @@ def b200_arm(args, rank, world, local_rank):
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": (MOVE_DRAM_READ_PER_WALKER + move_scratch_bytes(N)) * nw,
+                         "traffic": (MOVE_DRAM_READ_PER_WALKER + move_scratch_bytes(N, K)) * nw,
                          "traffic_source": TRAFFIC_SOURCE,
                          "kernel": "pairs_kernel + move_kernel",
                          "flops_per_move": fpm,
