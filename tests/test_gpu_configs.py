@@ -1,0 +1,91 @@
+"""GPU parity against the oracle on generated decks that take the device
+paths the n26 deck does not reach:
+
+- n58_bf: the benchmark state point (29 + 29, backflow, 1001-knot tables):
+  register Gauss-Jordan with 4 lanes per row, pair rows staged in shared
+  memory by the pair kernel;
+- n74_bf: 37 + 37, above 32 electrons per spin: the shared-memory
+  Gauss-Jordan with rho_k on the other warps;
+- pol25_bf: one type of 25 electrons: the register Gauss-Jordan with all
+  eight warps on one spin;
+- n26_u3_fine: u2 + u3 + backflow on 6001-knot tables, whose pair rows
+  (864 KB) do not fit in shared memory: the pair kernel reads them from
+  global memory.
+
+Each case checks compute_properties on fresh configurations (1e-10, as the
+n26 tests) and three VMC steps against the oracle's replay of the same
+Philox streams."""
+import importlib
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SEED = 0xC0FFEE1234
+RTOL = 1e-10
+
+CASES = {
+    "n58_bf": dict(n_up=29, n_down=29, rs=5.0, backflow=(0.2, 5.0, 3.0)),
+    "n74_bf": dict(n_up=37, n_down=37, rs=5.0, backflow=(0.2, 5.0, 3.0)),
+    "pol25_bf": dict(n_up=25, n_down=0, rs=3.0, backflow=(0.2, 3.0, 2.0)),
+    "n26_u3_fine": dict(n_up=13, n_down=13, rs=10.0, backflow=(0.2, 10.0, 6.0), u3=True,
+                        nknots=6000),
+}
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def close(a, b):
+    """|a-b| / max(|b|, 1e-3 max|b|), elementwise maximum (as the n26 tests)."""
+    a, b = np.asarray(a), np.asarray(b)
+    scale = max(np.abs(b).max(), 1e-300)
+    return (np.abs(a - b) / np.maximum(np.abs(b), scale * 1e-3)).max()
+
+
+@pytest.fixture(params=sorted(CASES))
+def deck(request, q, tmp_path):
+    tables = importlib.import_module("2degas_b200.tables")
+    d = tables.make_run(os.path.join(tmp_path, request.param), "c", nconf=8, seed=17,
+                        **CASES[request.param])
+    s = q.System.read(d, "c")
+    return request.param, s, s.read_configs(d, ".0", 0, 8)
+
+
+def test_evaluation_parity(q, oracle_cls, deck):
+    name, s, x = deck
+    o = oracle_cls(s.ptr)
+    with q.Handle(s, capacity=len(x), seed=3) as h:
+        g, hl, p, sg = h.compute_properties(x)
+    for k in range(len(x)):
+        go, ho, po, so, _ = o.compute_properties(x[k])
+        assert close(g[k], go) < RTOL, f"{name}: drift, config {k}"
+        assert close(hl[k], ho) < RTOL, f"{name}: laplacian, config {k}"
+        assert close(p[k], po) < RTOL, f"{name}: properties, config {k}"
+        assert sg[k] == so, f"{name}: sign, config {k}"
+
+
+def test_vmc_parity(q, oracle_cls, deck):
+    name, s, x = deck
+    nw, nstp = len(x), 3
+    delta = 0.02 * CASES[name]["rs"] ** 2
+    o = oracle_cls(s.ptr)
+    pop = o.population_init(x)
+    blk_o, nacc_o = o.vmc_philox(pop, nstp, delta, 1000, SEED, 0)
+    with q.Handle(s, capacity=nw, seed=SEED) as h:
+        h.population_set(x)
+        h.block_reset()
+        h.vmc(nstp, delta, 1000)
+        got = h.population_get()
+        blk, norm = h.block_get()
+        cnt = h.counters()
+    ns = s.s.n_scalar_props
+    assert cnt["accepted"] == nacc_o, name
+    assert rel(got["x"], pop["x"]) < 1e-11, name
+    assert rel(got["g"], pop["g"]) < 1e-9, name
+    assert rel(got["p"][:, :ns], pop["p"][:, :ns]) < 1e-9, name
+    assert rel(blk[:ns], blk_o[:ns]) < 1e-9, name
