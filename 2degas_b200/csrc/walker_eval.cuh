@@ -1191,7 +1191,11 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
             m.lapd[i] += t3;
           }
         }
-        __syncthreads();
+        // The next chunk's Jacobian build touches neither part nor these
+        // electrons' sums, and its own barrier precedes the next GEMM; only
+        // after the last chunk must everyone wait (the next spin's F
+        // overwrites this region, the assembly reads lapd).
+        if (i0 + kChunk / 2 >= N) __syncthreads();
         phase_mark(S, PH_CROSS, tph);
       }
     }
