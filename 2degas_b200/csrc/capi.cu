@@ -257,7 +257,8 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
       (e = dalloc(&h->d_h, (size_t)cap * nt)) != cudaSuccess ||
       (e = dalloc(&h->d_p, (size_t)cap * np)) != cudaSuccess ||
       (e = dalloc(&h->d_s, (size_t)cap)) != cudaSuccess ||
-      (e = dalloc(&h->d_mscr, (size_t)cap * q2d::move_scratch_doubles(h->hs))) != cudaSuccess)
+      (e = dalloc(&h->d_mscr, (size_t)cap * q2d::move_scratch_doubles(h->hs))) != cudaSuccess ||
+      (e = dalloc(&h->d_blksum, (size_t)np + 1)) != cudaSuccess)
     return fail(cuda_fail(e, "cudaMalloc"));
   cudaMemset(h->d_blk, 0, sizeof(double) * cap * np);
   cudaMemset(h->d_norm, 0, sizeof(double) * cap);
@@ -296,7 +297,7 @@ extern "C" int qmc2d_destroy(qmc2d_handle *h) {
   void *bufs[] = {h->ds, h->d_coef, h->d_kvec, h->d_gvec, h->d_blk, h->d_norm, h->d_cnt,
                   h->d_wate, h->d_status, h->br.delt, h->br.csum, h->br.mult, h->br.src,
                   h->br.ecum, h->br.zrank, h->br.ncapped, h->d_x, h->d_g, h->d_h, h->d_p,
-                  h->d_s, h->d_mscr, h->hs.phase};
+                  h->d_s, h->d_mscr, h->d_blksum, h->hs.phase};
   for (void *b : bufs) cudaFree(b);
   for (int k = 0; k < QMC2D_NKERNELS; k++)
     for (cudaEvent_t e : h->ev[k]) cudaEventDestroy(e);
@@ -480,22 +481,17 @@ extern "C" int qmc2d_block_reset(qmc2d_handle *h) {
 extern "C" int qmc2d_block_get(qmc2d_handle *h, double *blk_av, double *blk_norm) {
   if (!h) return QMC2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
-  CK(cudaStreamSynchronize(h->stream));
-  int np = h->nprops, n = std::max(h->nw, h->rmc.nrep);
-  std::vector<double> b((size_t)n * np), nn(n);
-  CK(cudaMemcpy(b.data(), h->d_blk, sizeof(double) * b.size(), cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(nn.data(), h->d_norm, sizeof(double) * n, cudaMemcpyDeviceToHost));
-  if (blk_av)
-    for (int j = 0; j < np; j++) {
-      double t = 0.0;
-      for (int w = 0; w < n; w++) t += b[(size_t)w * np + j];
-      blk_av[j] = t;
-    }
-  if (blk_norm) {
-    double t = 0.0;
-    for (int w = 0; w < n; w++) t += nn[w];
-    *blk_norm = t;
+  const int np = h->nprops, n = std::max(h->nw, h->rmc.nrep);
+  std::vector<double> sums((size_t)np + 1, 0.0);
+  if (n > 0) {
+    CK(q2d::launch_block_reduce(h->d_blk, h->d_norm, n, np, h->d_blksum, h->stream));
+    CK(cudaMemcpyAsync(sums.data(), h->d_blksum, sizeof(double) * (np + 1),
+                       cudaMemcpyDeviceToHost, h->stream));
   }
+  CK(cudaStreamSynchronize(h->stream));
+  if (blk_av)
+    for (int j = 0; j < np; j++) blk_av[j] = sums[j];
+  if (blk_norm) *blk_norm = sums[np];
   return QMC2D_OK;
 }
 

@@ -22,6 +22,7 @@ struct qmc2d_handle {
   double *d_blk = nullptr, *d_norm = nullptr, *d_cnt = nullptr, *d_wate = nullptr;
   int *d_status = nullptr;
   double *d_mscr = nullptr;  // move scratch: cap * move_scratch_doubles(hs)
+  double *d_blksum = nullptr;  // n_props + 1: block sums over the population
   q2d::BranchScratch br{};
   // staging for the batched evaluation entry point
   double *d_x = nullptr, *d_g = nullptr, *d_h = nullptr, *d_p = nullptr, *d_s = nullptr;

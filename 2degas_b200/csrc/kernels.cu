@@ -501,6 +501,27 @@ __global__ void philox_probe_kernel(uint64_t seed, const uint32_t *ctr, uint32_t
   out[4 * i + 3] = o.w;
 }
 
+// ------------------------------------------------- block sums over walkers
+// out[j] = sum_w blk[w*np + j] (j < np), out[np] = sum_w norm[w]: one CTA per
+// output, a fixed strided split and tree, so the result is reproducible.
+__global__ void __launch_bounds__(256) block_reduce_kernel(const double *blk, const double *norm,
+                                                           int n, int np, double *out) {
+  __shared__ double part[256];
+  const int j = blockIdx.x, t = threadIdx.x;
+  double s = 0.0;
+  if (j < np)
+    for (int w = t; w < n; w += 256) s += blk[(size_t)w * np + j];
+  else
+    for (int w = t; w < n; w += 256) s += norm[w];
+  part[t] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (t < o) part[t] += part[t + o];
+    __syncthreads();
+  }
+  if (t == 0) out[j] = part[0];
+}
+
 // ------------------------------------------------------------ launchers
 static cudaError_t set_smem(const void *fn, size_t bytes) {
   return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -546,6 +567,13 @@ cudaError_t launch_move(const DevSys &hs, const DevSys *ds, DevPop pop, const Mo
   cudaError_t e = set_smem((const void *)move_kernel, sm);
   if (e != cudaSuccess) return e;
   move_kernel<<<a.nw, kThreads, sm, st>>>(ds, pop, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_block_reduce(const double *blk, const double *norm, int n, int np,
+                                double *out, cudaStream_t st) {
+  if (n <= 0 || np <= 0) return cudaSuccess;
+  block_reduce_kernel<<<np + 1, 256, 0, st>>>(blk, norm, n, np, out);
   return cudaGetLastError();
 }
 

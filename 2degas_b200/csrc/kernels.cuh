@@ -41,6 +41,11 @@ cudaError_t launch_move(const DevSys &hs, const DevSys *ds, DevPop pop, const Mo
 // Doubles of move scratch per walker.
 size_t move_scratch_doubles(const DevSys &hs);
 
+// out[0..np) = per-property sums of blk (n walkers x np), out[np] = sum of
+// norm: the block accumulators over the population, on the device.
+cudaError_t launch_block_reduce(const double *blk, const double *norm, int n, int np,
+                                double *out, cudaStream_t st);
+
 // branch2's comb: wate -> src (new slot j copies old slot src[j]).
 struct BranchScratch {
   double *delt, *csum;
