@@ -226,6 +226,13 @@ class Handle:
         self._chk(self.lib.qmc2d_rmc_get_path(self.h, rep, _pd(x), _pd(p)))
         return x, p
 
+    def set_precision(self, precision):
+        """Precision of the pair passes: "fp64" (the default) or "mixed" (u2
+        and real-space Ewald pair terms in FP32 with compensated sums, all
+        else FP64)."""
+        code = {"fp64": _capi.PRECISION_FP64, "mixed": _capi.PRECISION_MIXED}[precision]
+        self._chk(self.lib.qmc2d_set_precision(self.h, code))
+
     def update_twist(self):
         """After system.set_twist(ith, jth): the orbitals use the new wave vectors."""
         self._chk(self.lib.qmc2d_update_twist(self.h, self.system.ptr))

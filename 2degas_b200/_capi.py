@@ -30,6 +30,7 @@ ERR_STACK = 11
 
 # kernels for qmc2d_profile_get
 KERNEL_MOVE, KERNEL_BRANCH, KERNEL_GATHER, KERNEL_EVAL, KERNEL_RMC, KERNEL_PAIRS = range(6)
+PRECISION_FP64, PRECISION_MIXED = 0, 1
 
 # property indices (0-based; reptation.f:577-637)
 JETOT, JLTF, JACC, JPOT0, JKIN0, JE2, JGG = range(7)
@@ -173,6 +174,7 @@ SIGNATURES = {
     "qmc2d_block_get": (c_int, [c_void_p, PD, PD]),
     "qmc2d_counters_get": (c_int, [c_void_p, POINTER(Counters)]),
     "qmc2d_update_twist": (c_int, [c_void_p, SYSP]),
+    "qmc2d_set_precision": (c_int, [c_void_p, c_int]),
     "qmc2d_stats_create": (c_int, [c_int, POINTER(c_void_p)]),
     "qmc2d_stats_destroy": (c_int, [c_void_p]),
     "qmc2d_stats_add_block": (c_int, [c_void_p, PD, c_double]),

@@ -38,6 +38,7 @@ void pack_pair_rows(const qmc2d_system *sys, DevSys *s, std::vector<double> *row
       s->cmb_blk[a][b] = (int)k;
     }
   s->cmb_nblk = (int)blocks.size();
+  const size_t start = rows->size();
   for (const std::vector<int> &tab : blocks)
     for (int k = 0; k <= ng; k++)
       for (int q = 0; q < 4; q++) {
@@ -49,6 +50,25 @@ void pack_pair_rows(const qmc2d_system *sys, DevSys *s, std::vector<double> *row
         const double *r = tb.ut + 4 * (size_t)std::min(k, tb.ngrid);
         rows->insert(rows->end(), r, r + 4);
       }
+  // the mixed rows: per knot the backflow and u3 parts (doubles 8..11 and
+  // 4..7 of the FP64 row), then the u2 and v2 parts rounded to float, then 32
+  // bytes of padding (16 doubles)
+  const size_t nrow = (rows->size() - start) / 16;
+  s->cmbm_off = s->cmb_off + (int)(rows->size() - start);
+  const size_t at = rows->size();
+  rows->resize(at + 16 * nrow, 0.0);
+  for (size_t k = 0; k < nrow; k++) {
+    const double *src = rows->data() + start + 16 * k;
+    double *dst = rows->data() + at + 16 * k;
+    std::memcpy(dst, src + 8, sizeof(double) * 4);
+    std::memcpy(dst + 4, src + 4, sizeof(double) * 4);
+    float f[8];
+    for (int q = 0; q < 4; q++) {
+      f[q] = (float)src[q];           // u2
+      f[4 + q] = (float)src[12 + q];  // v2
+    }
+    std::memcpy(dst + 8, f, sizeof f);
+  }
 }
 
 }  // namespace q2d
@@ -267,6 +287,18 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
   cudaMemset(h->br.ncapped, 0, sizeof(int));
   if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(cuda_fail(e, "create"));
   *out = h;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_set_precision(qmc2d_handle *h, int precision) {
+  if (!h || (precision != QMC2D_PRECISION_FP64 && precision != QMC2D_PRECISION_MIXED)) {
+    q2d::set_error("qmc2d_set_precision: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  h->hs.pair_f32 = precision == QMC2D_PRECISION_MIXED ? 1 : 0;
+  CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
   return QMC2D_OK;
 }
 

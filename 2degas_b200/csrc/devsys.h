@@ -42,6 +42,13 @@ struct DevSys {
   // table's row min(k, its ngrid). One 128-byte line per pair lookup.
   int cmb_off, cmb_ng;  // offset (doubles, 128-byte aligned) in coef; last knot
   int cmb_blk[2][2], cmb_nblk;
+  // Mixed rows at coef + cmbm_off (doubles, 128-byte aligned), read by the
+  // pair passes when pair_f32: per knot the backflow and u3 rows in FP64,
+  // then the u2 and v2 rows rounded to float, 128 bytes apart.
+  int cmbm_off;
+  // Precision of the pair passes (qmc2d_set_precision): 0 FP64; 1 the u2
+  // and v2 pair terms in FP32 with compensated sums read out in FP64.
+  int pair_f32;
   const double *coef;  // packed tables: ut rows (4 doubles each) and v_k lists
   const double *kvec;  // 2*nk
   const double *gvec;  // 2*ngvec

@@ -50,6 +50,7 @@ __device__ __forceinline__ void load_sys(DevSys &S, const DevSys *sp) {
 }
 
 // ---------------------------------------------------------------- eval
+template <class R>
 __global__ void __launch_bounds__(kThreads, 2) eval_kernel(const DevSys *sp, int nw,
                                                         const double *__restrict__ x, double *g,
                                                         double *hl, double *props, double *s,
@@ -68,7 +69,7 @@ __global__ void __launch_bounds__(kThreads, 2) eval_kernel(const DevSys *sp, int
   for (int j = threadIdx.x; j < N2; j += blockDim.x) m.x[j] = x[(size_t)w * N2 + j];
   __syncthreads();
   long long tph = clock64();
-  int st = eval_walker(S, m, hn, pn, sn, tph);
+  int st = eval_walker<R>(S, m, hn, pn, sn, tph);
   for (int j = threadIdx.x; j < N2; j += blockDim.x) g[(size_t)w * N2 + j] = m.g[j];
   for (int j = threadIdx.x; j < S.nprops; j += blockDim.x)
     props[(size_t)w * S.nprops + j] = pn[j];
@@ -129,6 +130,9 @@ size_t move_smem_bytes(const DevSys &s) {
 constexpr int kPairGroups = 2;
 constexpr int kPairThreads = kPairGroups * kThreads;
 
+//
+// R is the precision of the u2 and v2 pair terms (qmc2d_set_precision).
+template <class R>
 __global__ void __launch_bounds__(kPairThreads, 1) pairs_kernel(const DevSys *sp, DevPop pop,
                                                                 MoveArgs a, int stage_rows) {
   __shared__ DevSys S;
@@ -138,14 +142,17 @@ __global__ void __launch_bounds__(kPairThreads, 1) pairs_kernel(const DevSys *sp
   const int grp = threadIdx.x / kThreads, tid = threadIdx.x - grp * kThreads;
   EvalSmem m;
   pair_carve(S, smem + grp * carve, &m, kThreads);
-  const double *rows_g = S.coef + S.cmb_off;
-  double *rows_s = reinterpret_cast<double *>(smem + kPairGroups * carve);
-  if (stage_rows) {  // 16-double rows to kPairRowSh-double rows
+  const R *rows_g = pair_rows<R>(S);
+  R *rows_s = reinterpret_cast<R *>(smem + kPairGroups * carve);
+  if (stage_rows) {  // the first copy16 16-byte parts of each global row
+    using Lay = RowLayout<R>;
+    constexpr int V = Lay::copy16, VG = Lay::gstride * (int)sizeof(R) / 16;
     const int nrow = S.cmb_nblk * (S.cmb_ng + 1);
-    const double2 *src = reinterpret_cast<const double2 *>(rows_g);
-    for (int e = threadIdx.x; e < nrow * 8; e += kPairThreads) {
-      const int r = e >> 3, q = e & 7;
-      reinterpret_cast<double2 *>(rows_s + (size_t)r * kPairRowSh)[q] = __ldg(src + e);
+    const float4 *src = reinterpret_cast<const float4 *>(rows_g);
+    for (int e = threadIdx.x; e < nrow * V; e += kPairThreads) {
+      const int r = e / V, q = e - r * V;
+      reinterpret_cast<float4 *>(rows_s + (size_t)r * Lay::sstride)[q] =
+          __ldg(src + (size_t)r * VG + q);
     }
   }
   __syncthreads();
@@ -170,7 +177,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) pairs_kernel(const DevSys *sp
     double *o = a.scr + (size_t)w * L.stride;
     double *pout = S.has_bf ? o + L.pair : nullptr;
     if (stage_rows)
-      eval_pairs<kThreads, true>(S, m, tph, pout, rows_s, sync, tid);
+      eval_pairs<kThreads, true>(S, m, tph, pout, (const R *)rows_s, sync, tid);
     else
       eval_pairs<kThreads, false>(S, m, tph, pout, rows_g, sync, tid);
     compute_rhok(S, m, tid, kThreads);
@@ -531,9 +538,14 @@ cudaError_t launch_eval(const DevSys &hs, const DevSys *ds, int nw, const double
                         double *hl, double *props, double *s, int *status, cudaStream_t st) {
   if (nw <= 0) return cudaSuccess;
   size_t sm = eval_smem_bytes(hs);
-  cudaError_t e = set_smem((const void *)eval_kernel, sm);
+  const void *k =
+      hs.pair_f32 ? (const void *)eval_kernel<float> : (const void *)eval_kernel<double>;
+  cudaError_t e = set_smem(k, sm);
   if (e != cudaSuccess) return e;
-  eval_kernel<<<nw, kThreads, sm, st>>>(ds, nw, x, g, hl, props, s, status);
+  if (hs.pair_f32)
+    eval_kernel<float><<<nw, kThreads, sm, st>>>(ds, nw, x, g, hl, props, s, status);
+  else
+    eval_kernel<double><<<nw, kThreads, sm, st>>>(ds, nw, x, g, hl, props, s, status);
   return cudaGetLastError();
 }
 
@@ -550,13 +562,20 @@ cudaError_t launch_pairs(const DevSys &hs, const DevSys *ds, DevPop pop, const M
     return e;
   const size_t carve =
       kPairGroups * ((pair_carve(hs, nullptr, nullptr, kThreads) + 127) & ~size_t(127));
-  const size_t rows = sizeof(double) * kPairRowSh * (size_t)hs.cmb_nblk * (hs.cmb_ng + 1);
+  const size_t rows = (hs.pair_f32 ? sizeof(float) * RowLayout<float>::sstride
+                                   : sizeof(double) * RowLayout<double>::sstride) *
+                      (size_t)hs.cmb_nblk * (hs.cmb_ng + 1);
   const int stage = carve + rows + sizeof(DevSys) <= (size_t)optin ? 1 : 0;
   const size_t sm = carve + (stage ? rows : 0);
-  if ((e = set_smem((const void *)pairs_kernel, sm)) != cudaSuccess) return e;
+  const void *k =
+      hs.pair_f32 ? (const void *)pairs_kernel<float> : (const void *)pairs_kernel<double>;
+  if ((e = set_smem(k, sm)) != cudaSuccess) return e;
   const int need = (a.nw + kPairGroups - 1) / kPairGroups;
   const int grid = need < nsm ? need : nsm;
-  pairs_kernel<<<grid, kPairThreads, sm, st>>>(ds, pop, a, stage);
+  if (hs.pair_f32)
+    pairs_kernel<float><<<grid, kPairThreads, sm, st>>>(ds, pop, a, stage);
+  else
+    pairs_kernel<double><<<grid, kPairThreads, sm, st>>>(ds, pop, a, stage);
   return cudaGetLastError();
 }
 

@@ -300,6 +300,137 @@ __device__ __forceinline__ void pair_geom(const DevSys &S, const double *x, int 
   byr = 1.0 / r;
 }
 
+// ---- the pair passes in either precision R of the two-body Jastrow and
+// real-space Ewald terms (double, or float in the mixed-precision mode of
+// qmc2d_set_precision); the u3 and backflow terms are FP64 in both.
+//
+// Row layouts per knot (units of R):
+// - FP64 rows: u2 | u3 | backflow | v2, four doubles each (128 bytes), 16
+//   apart in global memory and kPairRowSh (144 bytes) in shared memory;
+// - mixed rows: the backflow and u3 rows in FP64, then the u2 and v2 rows
+//   rounded to float (96 bytes), 32 floats (128 bytes, so the FP64 parts
+//   stay 32-byte aligned for one 256-bit load) apart in global memory and
+//   28 floats (112 bytes) in shared memory, which spreads a warp's random
+//   rows over eight 16-byte bank groups as kPairRowSh does.
+template <class R>
+struct RowLayout;
+template <>
+struct RowLayout<double> {
+  static constexpr int u2 = 0, u3 = 4, bf = 8, v2 = 12;
+  static constexpr int gstride = 16, sstride = kPairRowSh, copy16 = 8;
+};
+template <>
+struct RowLayout<float> {
+  static constexpr int bf = 0, u3 = 8, u2 = 16, v2 = 20;
+  static constexpr int gstride = 32, sstride = 28, copy16 = 6;
+};
+
+template <class R>
+__device__ __forceinline__ const R *pair_rows(const DevSys &S);
+template <>
+__device__ __forceinline__ const double *pair_rows<double>(const DevSys &S) {
+  return S.coef + S.cmb_off;
+}
+template <>
+__device__ __forceinline__ const float *pair_rows<float>(const DevSys &S) {
+  return reinterpret_cast<const float *>(S.coef + S.cmbm_off);
+}
+
+template <int RS>
+__device__ __forceinline__ const float *pair_row(const DevSys &S, const float *rows, int a, int b,
+                                                 int ind) {
+  const int k = max(0, min(S.cmb_ng, ind));
+  return rows + ((size_t)S.cmb_blk[a][b] * (S.cmb_ng + 1) + k) * RS;
+}
+
+// Four floats of a mixed row (one 128-bit load).
+template <bool kSh>
+__device__ __forceinline__ float4 row_part(const float *p) {
+  return kSh ? *reinterpret_cast<const float4 *>(p) : __ldg(reinterpret_cast<const float4 *>(p));
+}
+
+// The knot spacing in precision R.
+template <class R>
+struct Knots {
+  R drt, drti, drti2;
+  __device__ explicit Knots(const DevSys &S) : drt((R)S.drt), drti((R)S.drti), drti2((R)S.drti2) {}
+};
+
+// getf / getf_0 in precision R (for R = double the same operations as
+// spline3 / spline0 above).
+template <bool kSh, class R>
+__device__ __forceinline__ void spline3(const Knots<R> &K, const R *part, R rem, R &f, R &df,
+                                        R &ddf) {
+  const auto u = row_part<kSh>(part);
+  const R rm = rem * K.drti;
+  f = u.x + rm * (u.y + rm * (u.z + rm * u.w));
+  df = (u.y + rm * ((R)2 * u.z + rm * ((R)3 * u.w))) * K.drti;
+  ddf = (u.z + rm * ((R)3 * u.w)) * K.drti2;
+}
+template <bool kSh, class R>
+__device__ __forceinline__ R spline0(const Knots<R> &K, const R *part, int iexp, R rem, R byr) {
+  const auto u = row_part<kSh>(part);
+  const R rm = rem * K.drti;
+  R f = u.x + rm * (u.y + rm * (u.z + rm * u.w));
+  for (int k = 0; k < iexp; k++) f *= byr;
+  return f;
+}
+
+// Pair geometry. FP64: as pair_geom above. FP32: the minimum-image
+// difference is formed in FP64 (walker coordinates are not wrapped into the
+// cell and can lie many cells away) and rounded to float; r, 1/r, the knot
+// and the remainder follow in FP32.
+__device__ __forceinline__ void pair_geom(const DevSys &S, const Knots<double> &K,
+                                          const double *x, int i, int j, double &rx, double &ry,
+                                          double &r, double &byr, int &ind, double &rem) {
+  rx = x[2 * i] - x[2 * j];
+  ry = x[2 * i + 1] - x[2 * j + 1];
+  rx = rx - S.el[0] * round(S.eli[0] * rx);
+  ry = ry - S.el[1] * round(S.eli[1] * ry);
+  r = sqrt(rx * rx + ry * ry);
+  ind = (int)(r * K.drti);
+  rem = r - ind * K.drt;
+  byr = 1.0 / r;
+}
+__device__ __forceinline__ void pair_geom(const DevSys &S, const Knots<float> &K,
+                                          const double *x, int i, int j, float &rx, float &ry,
+                                          float &r, float &byr, int &ind, float &rem) {
+  double dx = x[2 * i] - x[2 * j];
+  double dy = x[2 * i + 1] - x[2 * j + 1];
+  dx = dx - S.el[0] * round(S.eli[0] * dx);
+  dy = dy - S.el[1] * round(S.eli[1] * dy);
+  rx = (float)dx;
+  ry = (float)dy;
+  const float r2 = rx * rx + ry * ry;
+  byr = rsqrtf(r2);
+  r = r2 * byr;
+  ind = (int)(r * K.drti);
+  rem = r - (float)ind * K.drt;
+}
+
+// A lane's running sum of pair terms. FP64: a plain sum. FP32: Kahan's
+// compensated sum (the rounding error of each addition is carried in c and
+// subtracted from the next term), read out in FP64 as s - c.
+template <class R>
+struct PairSum;
+template <>
+struct PairSum<double> {
+  double s = 0.0;
+  __device__ __forceinline__ void add(double v) { s += v; }
+  __device__ __forceinline__ double value() const { return s; }
+};
+template <>
+struct PairSum<float> {
+  float s = 0.f, c = 0.f;
+  __device__ __forceinline__ void add(float v) {
+    const float y = v - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
 // Backflow Jacobian dq_j/dx_i (2x2, symmetric) for j != i (qa of
 // slater_excitations, reptation.f:10093-10168): -(eta I + eta'/r r r^T).
 // ti, tj: the types of i and j.
@@ -686,18 +817,29 @@ __device__ inline void compute_rhok(const DevSys &S, const EvalSmem &m, int t, i
 // Pair passes A and B: writes m.{ltf, g, lap, vp, G3, S3, q, Sb, qbd} and
 // zeroes m.{gd, lapd, ph2, ph2d}. With pout (backflow), also the backflow
 // spline values of every ordered pair, laid out as in MoveScratch.
-// NT threads (a multiple of 32) run the passes; the pair rows are read at
-// `rows`, from shared memory when kSh.
+// NT threads (a multiple of 32) run the passes; the pair rows (layout
+// RowLayout<R>) are read at `rows`, from shared memory when kSh.
+// R is the precision of the u2 and v2 terms: double, or float with the pair
+// vector from the FP64 minimum image and each lane's sums compensated
+// (PairSum); the lanes' sums and all that follows are FP64. The u3 and
+// backflow terms are FP64 in both: FP32 u3 terms put the local energy off
+// by up to 2e-6 Ry per electron, and an FP32 backflow displacement error
+// reaches it through the determinant amplified by the inverse square of the
+// distance to the nearest node.
 // Sync is the barrier of the NT threads (the CTA, or a named-barrier group
 // of a CTA that runs several walkers); tid is the thread's index among them.
-template <int NT, bool kSh, class Sync = CtaSync>
+template <int NT, bool kSh, class R = double, class Sync = CtaSync>
 __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long &tph,
-                                  double *pout, const double *rows, Sync sync = Sync(),
+                                  double *pout, const R *rows, Sync sync = Sync(),
                                   int tid = threadIdx.x) {
+  using Lay = RowLayout<R>;
   const int N = S.N;
   const int lane8 = tid & (kGroup - 1);
   const int per_round = NT / kGroup;
   const size_t NN = (size_t)N * N;
+  constexpr int RS = kSh ? Lay::sstride : Lay::gstride;
+  constexpr bool kF64 = sizeof(R) == 8;
+  const Knots<R> K(S);
 
   // ---- pass A: pair sums of u2, the pair part of u3, u3 G vectors and S,
   // backflow displacement, Jacobian diagonal and Laplacian, pair potential.
@@ -705,54 +847,76 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
     int i = base + tid / kGroup;
     bool valid = i < N;
     int ti = valid ? type_of(S, i) : 0;
-    double ltf = 0, gx = 0, gy = 0, lap = 0, vp = 0;
-    double Gx = 0, Gy = 0, s3xx = 0, s3xy = 0, s3yy = 0;
-    double qx = 0, qy = 0, sbxx = 0, sbxy = 0, sbyy = 0, qbx = 0, qby = 0;
+    PairSum<R> ltf, gx, gy, lap, vp;
+    PairSum<double> ltf3, gx3, gy3, lap3;  // the u3 terms' share when R = float
+    PairSum<double> Gx, Gy, s3xx, s3xy, s3yy;
+    PairSum<double> qx, qy, sbxx, sbxy, sbyy, qbx, qby;
     if (valid) {
       for (int j = lane8; j < N; j += kGroup) {
         if (j == i) continue;
         int tj = type_of(S, j);
-        double rx, ry, r, byr, rem;
+        R rx, ry, r, byr, rem;
+        double rxd = 0, ryd = 0, rd = 0, byrd = 0, remd = 0;
         int ind;
-        pair_geom(S, m.x, i, j, rx, ry, r, byr, ind, rem);
-        const double *row = pair_row<kSh ? kPairRowSh : 16>(S, rows, ti, tj, ind);
-        double t, dt, ddt;
+        if (kF64 || S.has_bf || S.has_u3) {  // FP64 geometry (the u3 and backflow terms)
+          pair_geom(S, Knots<double>(S), m.x, i, j, rxd, ryd, rd, byrd, ind, remd);
+          rx = (R)rxd;
+          ry = (R)ryd;
+          r = (R)rd;
+          byr = (R)byrd;
+          rem = (R)remd;
+        } else {
+          pair_geom(S, K, m.x, i, j, rx, ry, r, byr, ind, rem);
+        }
+        const R *row = pair_row<RS>(S, rows, ti, tj, ind);
         if (S.has_u2) {
-          spline3<kSh>(S, row + PR_U2, rem, t, dt, ddt);
-          ltf += 0.5 * t;
-          double dtr = dt * byr;
-          gx += dtr * rx;
-          gy += dtr * ry;
-          lap += ddt + dtr;
+          R t, dt, ddt;
+          spline3<kSh>(K, row + Lay::u2, rem, t, dt, ddt);
+          ltf.add((R)0.5 * t);
+          R dtr = dt * byr;
+          gx.add(dtr * rx);
+          gy.add(dtr * ry);
+          lap.add(ddt + dtr);
         }
         if (S.has_u3) {
-          spline3<kSh>(S, row + PR_U3, rem, t, dt, ddt);
-          Gx -= t * rx;
-          Gy -= t * ry;
-          double c = dt * byr;
-          s3xx += t + c * rx * rx;
-          s3xy += c * rx * ry;
-          s3yy += t + c * ry * ry;
+          double t, dt, ddt;
+          spline3<kSh>(Knots<double>(S), reinterpret_cast<const double *>(row + Lay::u3), remd, t,
+                       dt, ddt);
+          Gx.add(-t * rxd);
+          Gy.add(-t * ryd);
+          double c = dt * byrd;
+          s3xx.add(t + c * rxd * rxd);
+          s3xy.add(c * rxd * ryd);
+          s3yy.add(t + c * ryd * ryd);
           // the two-body piece (xi r)^2 removed from sum |G|^2 (three_body :2824-2832)
-          double d3 = 2.0 * (t * t + 4.0 * r * t * dt + r * r * (dt * dt + ddt * t));
-          double c3 = 2.0 * t * (t + r * dt);
-          double tr = t * r;
-          ltf += 0.5 * tr * tr;
-          gx += c3 * rx;
-          gy += c3 * ry;
-          lap += d3 + c3;
+          double d3 = 2.0 * (t * t + 4.0 * rd * t * dt + rd * rd * (dt * dt + ddt * t));
+          double c3 = 2.0 * t * (t + rd * dt);
+          double tr = t * rd;
+          if constexpr (kF64) {
+            ltf.add(0.5 * tr * tr);
+            gx.add(c3 * rxd);
+            gy.add(c3 * ryd);
+            lap.add(d3 + c3);
+          } else {
+            ltf3.add(0.5 * tr * tr);
+            gx3.add(c3 * rxd);
+            gy3.add(c3 * ryd);
+            lap3.add(d3 + c3);
+          }
         }
         if (S.has_bf) {
-          spline3<kSh>(S, row + PR_BF, rem, t, dt, ddt);
-          qx += t * rx;
-          qy += t * ry;
-          double c = dt * byr;
-          sbxx += t + c * rx * rx;
-          sbxy += c * rx * ry;
-          sbyy += t + c * ry * ry;
-          double w2 = dt * byr * 3.0 + ddt;
-          qbx += w2 * rx;
-          qby += w2 * ry;
+          double t, dt, ddt;
+          spline3<kSh>(Knots<double>(S), reinterpret_cast<const double *>(row + Lay::bf), remd, t,
+                       dt, ddt);
+          qx.add(t * rxd);
+          qy.add(t * ryd);
+          double c = dt * byrd;
+          sbxx.add(t + c * rxd * rxd);
+          sbxy.add(c * rxd * ryd);
+          sbyy.add(t + c * ryd * ryd);
+          double w2 = dt * byrd * 3.0 + ddt;
+          qbx.add(w2 * rxd);
+          qby.add(w2 * ryd);
           if (pout) {
             const size_t e = (size_t)i * N + j;
             pout[e] = t;
@@ -760,48 +924,58 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
             pout[2 * NN + e] = w2;
           }
         }
-        if (S.has_v2) vp += 0.5 * spline0<kSh>(S, row + PR_V2, S.tab_iexp[S.iv2[ti][tj]], rem, byr);
+        if (S.has_v2)
+          vp.add((R)0.5 * spline0<kSh>(K, row + Lay::v2, S.tab_iexp[S.iv2[ti][tj]], rem, byr));
       }
     }
-    ltf = group8_sum(ltf);
-    gx = group8_sum(gx);
-    gy = group8_sum(gy);
-    lap = group8_sum(lap);
-    vp = group8_sum(vp);
-    if (S.has_u3) {
-      Gx = group8_sum(Gx);
-      Gy = group8_sum(Gy);
-      s3xx = group8_sum(s3xx);
-      s3xy = group8_sum(s3xy);
-      s3yy = group8_sum(s3yy);
+    double ltf_v = ltf.value(), gx_v = gx.value(), gy_v = gy.value(), lap_v = lap.value();
+    if (!kF64 && S.has_u3) {
+      ltf_v += ltf3.value();
+      gx_v += gx3.value();
+      gy_v += gy3.value();
+      lap_v += lap3.value();
     }
+    const double ltf_s = group8_sum(ltf_v);
+    const double gx_s = group8_sum(gx_v);
+    const double gy_s = group8_sum(gy_v);
+    const double lap_s = group8_sum(lap_v);
+    const double vp_s = group8_sum(vp.value());
+    double Gx_s = 0, Gy_s = 0, s3xx_s = 0, s3xy_s = 0, s3yy_s = 0;
+    if (S.has_u3) {
+      Gx_s = group8_sum(Gx.value());
+      Gy_s = group8_sum(Gy.value());
+      s3xx_s = group8_sum(s3xx.value());
+      s3xy_s = group8_sum(s3xy.value());
+      s3yy_s = group8_sum(s3yy.value());
+    }
+    double qx_s = 0, qy_s = 0, sbxx_s = 0, sbxy_s = 0, sbyy_s = 0, qbx_s = 0, qby_s = 0;
     if (S.has_bf) {
-      qx = group8_sum(qx);
-      qy = group8_sum(qy);
-      sbxx = group8_sum(sbxx);
-      sbxy = group8_sum(sbxy);
-      sbyy = group8_sum(sbyy);
-      qbx = group8_sum(qbx);
-      qby = group8_sum(qby);
+      qx_s = group8_sum(qx.value());
+      qy_s = group8_sum(qy.value());
+      sbxx_s = group8_sum(sbxx.value());
+      sbxy_s = group8_sum(sbxy.value());
+      sbyy_s = group8_sum(sbyy.value());
+      qbx_s = group8_sum(qbx.value());
+      qby_s = group8_sum(qby.value());
     }
     if (valid && lane8 == 0) {
-      m.ltf[i] = ltf;
-      m.g[2 * i] = gx;
-      m.g[2 * i + 1] = gy;
-      m.lap[i] = lap;
-      m.vp[i] = vp;
-      m.G3[2 * i] = Gx;
-      m.G3[2 * i + 1] = Gy;
-      m.S3[3 * i] = s3xx;
-      m.S3[3 * i + 1] = s3xy;
-      m.S3[3 * i + 2] = s3yy;
-      m.q[2 * i] = m.x[2 * i] + qx;
-      m.q[2 * i + 1] = m.x[2 * i + 1] + qy;
-      m.Sb[3 * i] = sbxx;
-      m.Sb[3 * i + 1] = sbxy;
-      m.Sb[3 * i + 2] = sbyy;
-      m.qbd[2 * i] = qbx;
-      m.qbd[2 * i + 1] = qby;
+      m.ltf[i] = ltf_s;
+      m.g[2 * i] = gx_s;
+      m.g[2 * i + 1] = gy_s;
+      m.lap[i] = lap_s;
+      m.vp[i] = vp_s;
+      m.G3[2 * i] = Gx_s;
+      m.G3[2 * i + 1] = Gy_s;
+      m.S3[3 * i] = s3xx_s;
+      m.S3[3 * i + 1] = s3xy_s;
+      m.S3[3 * i + 2] = s3yy_s;
+      m.q[2 * i] = m.x[2 * i] + qx_s;
+      m.q[2 * i + 1] = m.x[2 * i + 1] + qy_s;
+      m.Sb[3 * i] = sbxx_s;
+      m.Sb[3 * i + 1] = sbxy_s;
+      m.Sb[3 * i + 2] = sbyy_s;
+      m.qbd[2 * i] = qbx_s;
+      m.qbd[2 * i + 1] = qby_s;
       m.gd[2 * i] = 0.0;
       m.gd[2 * i + 1] = 0.0;
       m.lapd[i] = 0.0;
@@ -812,7 +986,7 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
   sync();
   phase_mark(S, PH_PAIRS, tph, tid == 0);
 
-  // ---- pass B: u3 gradient and Laplacian from the G vectors.
+  // ---- pass B: u3 gradient and Laplacian from the G vectors (FP64).
   if (S.has_u3) {
     for (int base = 0; base < N; base += per_round) {
       int k = base + tid / kGroup;
@@ -826,9 +1000,11 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
           int tj = type_of(S, j);
           double rx, ry, r, byr, rem;
           int ind;
-          pair_geom(S, m.x, k, j, rx, ry, r, byr, ind, rem);
+          pair_geom(S, Knots<double>(S), m.x, k, j, rx, ry, r, byr, ind, rem);
           double t, dt, ddt;
-          spline3<kSh>(S, pair_row<kSh ? kPairRowSh : 16>(S, rows, tk, tj, ind) + PR_U3, rem, t, dt, ddt);
+          spline3<kSh>(Knots<double>(S),
+                       reinterpret_cast<const double *>(pair_row<RS>(S, rows, tk, tj, ind) + Lay::u3),
+                       rem, t, dt, ddt);
           double c = dt * byr;
           double mxx = t + c * rx * rx, mxy = c * rx * ry, myy = t + c * ry * ry;
           double dGx = Gkx - m.G3[2 * j], dGy = Gky - m.G3[2 * j + 1];
@@ -1358,10 +1534,11 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
 }
 
 // The whole evaluation of the configuration in m.x (compute_properties,
-// reptation.f:2661).
+// reptation.f:2661), with the u2 and v2 pair terms in precision R.
+template <class R = double>
 __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl, double *props,
                                   double *sign, long long &tph) {
-  eval_pairs<kThreads, false>(S, m, tph, nullptr, S.coef + S.cmb_off);
+  eval_pairs<kThreads, false>(S, m, tph, nullptr, pair_rows<R>(S));
   return eval_det(S, m, hl, props, sign, tph, nullptr);
 }
 

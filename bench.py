@@ -270,6 +270,7 @@ def b200_arm(args, rank, world, local_rank):
     delta = 0.05 * rs * rs
     x0 = sysobj.read_configs(d, ".0", 0, nw)
     h = q.Handle(sysobj, capacity=nw, seed=walker_seed, device=local_rank)
+    h.set_precision(args.precision)
     h.population_set(x0)
     h.vmc(args.equil, delta, 10 ** 9)  # seeded VMC equilibration
     h.block_reset()
@@ -376,8 +377,11 @@ def b200_arm(args, rank, world, local_rank):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f64 (f32 u2 and v2 pair terms)",
+            "data": "synthetic",
             "config": {"workload": CONFIG, "walkers_per_gpu": nw, "N": N, "rs": rs,
+                       "precision": args.precision,
                        "tau": delta, "mmstep": 1, "moves_per_step": nw * world,
                        "l2": "flushed between timed steps (256 MiB write)",
                        "parallelism": f"independent populations x{world}"},
@@ -417,6 +421,9 @@ def main():
     ap.add_argument("--equil", type=int, default=20)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="pair passes in FP64 (default), or u2 and real-space Ewald pair terms "
+                         "in FP32 with compensated sums")
     ap.add_argument("--phases", action="store_true",
                     help="print SM cycles per walker-move of each move-kernel phase instead")
     args = ap.parse_args()

@@ -176,6 +176,20 @@ int qmc2d_destroy(qmc2d_handle *h);
  * reference, which carries its walkers from one twist to the next. */
 int qmc2d_update_twist(qmc2d_handle *h, const qmc2d_system *sys);
 
+/* Precision of the pair passes in compute_properties, VMC and DMC
+ * (reptation stays FP64). QMC2D_PRECISION_FP64, the default: every
+ * operation in FP64, as the reference. QMC2D_PRECISION_MIXED: the two-body
+ * Jastrow pair terms (two_body, reptation.f:2981-3046) and the real-space
+ * Ewald pair potential (potential, reptation.f:3986-4030) are evaluated in
+ * FP32 from an FP32 copy of their tables, the pair vector coming from the
+ * FP64 minimum image; each thread's sums of those terms are compensated
+ * (Kahan) and read out in FP64. The u3 and backflow terms, the
+ * determinants and inverse, the k-space Ewald sum, energies, weights and
+ * accumulators stay FP64. The reference has no counterpart: it computes in
+ * FP64 only. */
+enum { QMC2D_PRECISION_FP64 = 0, QMC2D_PRECISION_MIXED = 1 };
+int qmc2d_set_precision(qmc2d_handle *h, int precision);
+
 /* compute_properties (reptation.f:2661): for nw configurations x (2*nptot
  * each) compute g = -grad ln psi (2*nptot), hlap = -lap ln psi per type
  * (ntypes), props (n_props) and the sign s. Host buffers, synchronous. */
