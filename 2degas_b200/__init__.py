@@ -72,6 +72,12 @@ class System:
     def set_twist(self, ith, jth):
         _capi.check(self.lib, self.lib.qmc2d_system_set_twist(self.ptr, ith, jth))
 
+    def footprint(self, capacity):
+        """Device bytes a Handle of this capacity allocates (no GPU needed)."""
+        b = ctypes.c_uint64(0)
+        _capi.check(self.lib, self.lib.qmc2d_footprint(self.ptr, capacity, ctypes.byref(b)))
+        return b.value
+
     def gvec(self):
         s = self.s
         return np.ctypeslib.as_array(s.gvec, shape=(2 * s.ngvec,)).reshape(-1, 2).copy()

@@ -202,6 +202,39 @@ int sync_status(qmc2d_handle *h, int nw) {
 
 int q2d_sync_status(qmc2d_handle *h, int n) { return sync_status(h, n); }
 
+// Device bytes qmc2d_create allocates for sys at this capacity (each
+// allocation rounded up to cudaMalloc's 512-byte granularity); the list is
+// the one qmc2d_create allocates, in the same order.
+size_t handle_bytes(const qmc2d_system *sys, const q2d::DevSys &hs, size_t ncoef, int cap) {
+  auto al = [](size_t n, size_t elem) { return ((std::max<size_t>(n, 1) * elem) + 511) & ~size_t(511); };
+  const size_t N = sys->nptot, nt = sys->ntypes, np = sys->n_props, c = cap;
+  size_t b = al(ncoef, 8) + al(2 * (size_t)std::max(1, sys->nk), 8) +
+             al(2 * (size_t)std::max(1, sys->ngvec), 8) + al(1, sizeof(q2d::DevSys));
+  const size_t pop = al(c * 2 * N, 8) * 2 + al(c * nt, 8) + al(c * np, 8) + al(c, 8) * 2;
+  b += 2 * pop;
+  b += al(c * np, 8) + al(c, 8) + al(c * 4, 8) + al(c, 8) + al(c, 4);  // blk norm cnt wate status
+  b += al(c, 8) * 2 + al(c, 4) * 4 + al(1, 4);                           // branch scratch
+  b += al(c * 2 * N, 8) * 2 + al(c * nt, 8) + al(c * np, 8) + al(c, 8);  // staging
+  b += al(c * q2d::move_scratch_doubles(hs), 8) + al(np + 1, 8);
+  return b;
+}
+
+extern "C" int qmc2d_footprint(const qmc2d_system *sys, int capacity, uint64_t *bytes) {
+  if (!sys || !bytes || capacity <= 0) {
+    q2d::set_error("qmc2d_footprint: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  if (sys->ndim != 2 || sys->ntypes < 1 || sys->ntypes > 2 || sys->nptot > QMC2D_MAX_NP) {
+    q2d::set_error("qmc2d_footprint: unsupported system size");
+    return QMC2D_ERR_LIMIT;
+  }
+  q2d::DevSys hs;
+  std::vector<double> coef;
+  build_devsys(sys, &hs, &coef);
+  *bytes = handle_bytes(sys, hs, coef.size(), capacity);
+  return QMC2D_OK;
+}
+
 extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
                             qmc2d_handle **out) {
   if (!sys || !opt || !out || opt->capacity <= 0) {

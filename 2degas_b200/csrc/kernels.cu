@@ -8,6 +8,9 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "kernels.cuh"
 #include "walker_eval.cuh"
@@ -530,9 +533,24 @@ __global__ void __launch_bounds__(256) block_reduce_kernel(const double *blk, co
 }
 
 // ------------------------------------------------------------ launchers
-static cudaError_t set_smem(const void *fn, size_t bytes) {
-  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+// The dynamic shared-memory limit of kernel fn on the current device is only
+// ever raised: handles of different systems driven from several host threads
+// launch the same kernels with different sizes, and a lower limit set by one
+// between another's set and launch would fail that launch.
+cudaError_t raise_smem_limit(const void *fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void *>, size_t> cur;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t &c = cur[{dev, fn}];
+  if (bytes <= c) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) c = bytes;
+  return e;
 }
+static cudaError_t set_smem(const void *fn, size_t bytes) { return raise_smem_limit(fn, bytes); }
 
 cudaError_t launch_eval(const DevSys &hs, const DevSys *ds, int nw, const double *x, double *g,
                         double *hl, double *props, double *s, int *status, cudaStream_t st) {

@@ -27,6 +27,10 @@ struct MoveArgs {
   int *status;        // nw status words (OR-ed)
 };
 
+// Raise (never lower) kernel fn's dynamic shared-memory limit on the current
+// device to bytes; safe to call from several host threads.
+cudaError_t raise_smem_limit(const void *fn, size_t bytes);
+
 // Evaluate nw configurations x (2N each) -> g, hl, props, s.
 cudaError_t launch_eval(const DevSys &hs, const DevSys *ds, int nw, const double *x, double *g,
                         double *hl, double *props, double *s, int *status, cudaStream_t st);

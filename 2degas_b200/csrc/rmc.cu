@@ -533,8 +533,7 @@ extern "C" int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params 
   RCK(cudaMemcpyAsync(dx, x, sizeof(double) * nx, cudaMemcpyHostToDevice, h->stream));
   q2d::RmcArgs a = rmc_args(h, 0);
   size_t sm = q2d::eval_smem_bytes(h->hs);
-  RCK(cudaFuncSetAttribute((const void *)q2d::rmc_eval_beads_kernel,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  RCK(q2d::raise_smem_limit((const void *)q2d::rmc_eval_beads_kernel, sm));
   q2d::rmc_eval_beads_kernel<<<nrep * r.ntau, q2d::kThreads, sm, h->stream>>>(h->ds, a, dx);
   RCK(cudaGetLastError());
   q2d::rmc_init_kernel<<<nrep, q2d::kThreads, sizeof(double) * np, h->stream>>>(h->ds, a);
@@ -556,8 +555,7 @@ extern "C" int qmc2d_rmc(qmc2d_handle *h, int nstp) {
   RCK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * h->rmc.nrep, h->stream));
   q2d::RmcArgs a = rmc_args(h, nstp);
   size_t sm = rmc_move_smem(h->hs);
-  RCK(cudaFuncSetAttribute((const void *)q2d::rmc_move_kernel,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  RCK(q2d::raise_smem_limit((const void *)q2d::rmc_move_kernel, sm));
   {
     ProfScope ps(h, QMC2D_KERNEL_RMC, h->stream);
     q2d::rmc_move_kernel<<<h->rmc.nrep, q2d::kThreads, sm, h->stream>>>(h->ds, a);

@@ -411,6 +411,68 @@ def b200_arm(args, rank, world, local_rank):
     return 0
 
 
+def serve_arm(args, rank, world):
+    """The serving stream: Poisson arrivals (20 requests/s, seeded) of
+    state points on the closed shells 26..162 that the kernels hold, r_s
+    uniform in [1, 40], polarisation 0 or 1, VMC or DMC, 512..4096 walkers,
+    target error bar 1e-4 Ry/electron; admitted by HBM footprint and run
+    together. Then the same requests one at a time on the FP64 path."""
+    import torch
+
+    if rank != 0:  # one GPU serves; further ranks would be further servers
+        return 0
+    serve = importlib.import_module("2degas_b200.serve")
+    unpol = [n for n in serve.closed_shells(81) if 26 <= 2 * n <= 162 and n <= 45]
+    pol = [n for n in serve.closed_shells(162) if 26 <= n <= 49]
+    kw = dict(block_steps=20, min_blocks=5, max_blocks=args.serve_blocks,
+              precision=args.precision)
+    stream = lambda: serve.poisson_stream(args.serve_requests, 20.0, 2026, unpol, pol,  # noqa: E731
+                                          **kw)
+    free, total = torch.cuda.mem_get_info()
+    budget = int(0.8 * free)
+    srv = serve.Server(budget, max_slots=args.serve_slots)
+    with Clocks(0) as clk:
+        res = srv.serve(stream())
+    sm = serve.summary(res)
+    seq = None
+    if not args.no_cpu:  # the same requests one at a time, FP64, as they arrive
+        reqs = stream()
+        for r in reqs:
+            r.precision = "fp64"
+        srv1 = serve.Server(budget, max_slots=1)
+        t0 = time.perf_counter()
+        res1 = srv1.serve(reqs, realtime=False)
+        wall1 = time.perf_counter() - t0
+        seq = serve.summary(res1, makespan=wall1)
+        seq["energy_agreement"] = [
+            (a.energy - b.energy) / max(math.hypot(a.error, b.error), 1e-300)
+            for a, b in zip(res, res1) if a.status != "rejected" and b.status != "rejected"]
+    line = {
+        "metric": "walker-moves/sec (serving stream)", "value": sm["walker_moves_per_s"],
+        "unit": UNIT, "n_gpus": 1, "steps": args.serve_requests, "warmup": 0,
+        "ms_per_step": 1e3 * sm["makespan_s"] / max(args.serve_requests, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f64 (f32 u2 and v2 pair terms)",
+        "data": "synthetic",
+        "config": {"workload": "serving_stream", "requests": args.serve_requests,
+                   "arrivals_per_s": 20.0, "unpolarised_per_spin": unpol, "polarised": pol,
+                   "rs": [1.0, 40.0], "walkers": [512, 4096], "target_ry_per_el": 1e-4,
+                   "block_steps": 20, "max_blocks": args.serve_blocks,
+                   "hbm_budget_bytes": budget, "slots": args.serve_slots,
+                   "precision": args.precision},
+        "serving": {**sm, "peak_active": srv.peak_active, "peak_hbm_bytes": srv.peak_used,
+                    "per_request": [dict(rid=r.rid, N=0, status=r.status, latency_s=r.latency,
+                                         energy=r.energy, error=r.error, blocks=r.blocks,
+                                         moves=r.moves, message=r.message[:80]) for r in res]},
+        "one_at_a_time_fp64": seq,
+        "clocks": clk.summary(),
+    }
+    for d, r in zip(line["serving"]["per_request"], stream()):
+        d["N"], d["rs"], d["method"], d["walkers"] = r.N, r.rs, r.method, r.walkers
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -424,6 +486,11 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="pair passes in FP64 (default), or u2 and real-space Ewald pair terms "
                          "in FP32 with compensated sums")
+    ap.add_argument("--workload", default="dmc", choices=["dmc", "serve"],
+                    help="dmc: the N=58 DMC generation (default); serve: the serving stream")
+    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-blocks", type=int, default=100)
+    ap.add_argument("--serve-slots", type=int, default=32)
     ap.add_argument("--phases", action="store_true",
                     help="print SM cycles per walker-move of each move-kernel phase instead")
     args = ap.parse_args()
@@ -434,6 +501,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return reference_arm(args, rank, world)
+    if args.workload == "serve":
+        return serve_arm(args, rank, world)
     return b200_arm(args, rank, world, local_rank)
 
 

@@ -170,6 +170,12 @@ typedef struct qmc2d_options {
 /* Copy the system's tables to the device and allocate walker storage. */
 int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt, qmc2d_handle **out);
 int qmc2d_destroy(qmc2d_handle *h);
+/* Device memory (bytes, each allocation rounded to 512) that qmc2d_create
+ * would allocate for sys at this capacity, computed on the host without a
+ * GPU; reptation storage (qmc2d_rmc_init) is not included. For admitting
+ * work by HBM footprint; the reference has no counterpart (it allocates
+ * its COMMON blocks statically). */
+int qmc2d_footprint(const qmc2d_system *sys, int capacity, uint64_t *bytes);
 /* After qmc2d_system_set_twist on the handle's system, make the handle's
  * orbitals use the new wave vectors (the gvec/gtens reset at each twist of
  * tabc, reptation.f:9581-9616); the population is left as it is, as in the
