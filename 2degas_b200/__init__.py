@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _capi
 
-__all__ = ["System", "Handle", "Stats", "tabc", "QMCError", "load_library", "_capi"]
+__all__ = ["System", "Handle", "Batch", "Stats", "tabc", "QMCError", "load_library", "_capi"]
 
 QMCError = _capi.QMCError
 
@@ -312,6 +312,47 @@ class Stats:
         _capi.check(self.lib, self.lib.qmc2d_stats_write_rhok(self.p, self.system.ptr, _pd(blk),
                                                               norm, str(directory).encode(),
                                                               runid.encode()))
+
+
+class Batch:
+    """Populations (Handles on one device) advanced together through one
+    CUDA graph per call (qmc2d_batch_*). Results equal the same vmc/dmc
+    calls made handle by handle."""
+
+    def __init__(self, handles):
+        self.handles = list(handles)
+        self.lib = self.handles[0].lib
+        arr = (ctypes.c_void_p * len(self.handles))(*[h.h.value for h in self.handles])
+        self.b = ctypes.c_void_p()
+        _capi.check(self.lib, self.lib.qmc2d_batch_create(arr, len(self.handles),
+                                                          ctypes.byref(self.b)))
+
+    def close(self):
+        if self.b:
+            self.lib.qmc2d_batch_destroy(self.b)
+            self.b = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def vmc(self, nstp, delta, mage=10 ** 9):
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(delta, float), (len(self.handles),)))
+        _capi.check(self.lib, self.lib.qmc2d_batch_vmc(self.b, nstp, _pd(d), mage))
+
+    def dmc(self, ngen, delta, etrial, mmult=2.0, mage=50):
+        n = len(self.handles)
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(delta, float), (n,)))
+        e = np.ascontiguousarray(np.broadcast_to(np.asarray(etrial, float), (n,)))
+        _capi.check(self.lib, self.lib.qmc2d_batch_dmc(self.b, ngen, _pd(d), _pd(e), mmult, mage))
 
 
 def tabc(handle, run, ntheta=None, resume=None, dmc_preequilibrate=None):

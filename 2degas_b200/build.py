@@ -15,7 +15,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 OUT = os.path.join(LIBDIR, "libqmc2d.so")
 
-SOURCES = ["input.cpp", "system.cpp", "io.cpp", "kernels.cu", "capi.cu", "rmc.cu", "noalloc.cu"]
+SOURCES = ["input.cpp", "system.cpp", "io.cpp", "kernels.cu", "capi.cu", "rmc.cu", "noalloc.cu",
+           "batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(kPairThreads, 1) pairs_kernel(const DevSys *sp
   __syncthreads();
   const GroupSync sync{1 + grp, kThreads};
   const int N = S.N, N2 = 2 * N;
-  const uint32_t step = a.step0;
+  const uint32_t step = a.step0 + (a.ctr ? a.ctr[0] : 0u);
   const double pi = 3.141592653589793;
   const MoveScratch L = move_scratch(S);
   for (int w = blockIdx.x * kPairGroups + grp; w < a.nw; w += gridDim.x * kPairGroups) {
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
   double wate = (a.dmc && !a.first) ? a.wate[w] : 1.0;
   double nacc = 0.0, nforced = 0.0;
   int status = 0;
-  const uint32_t step = a.step0;
+  const uint32_t step = a.step0 + (a.ctr ? a.ctr[0] : 0u);
   long long tph = clock64();
   double sn = 1.0;
   status |= eval_det(S, m, v.hn, v.pn, &v.sc[0], tph, S.has_bf ? o + L.pair : nullptr,
@@ -376,8 +376,10 @@ __device__ void block_exclusive_scan_ipartials(int *part, int n) {
 constexpr int kBranchThreads = 1024;
 
 __global__ void __launch_bounds__(kBranchThreads) branch_kernel(int nw, double *wate,
-                                                                uint64_t seed, uint32_t gen,
+                                                                uint64_t seed, uint32_t gen0,
+                                                                const uint32_t *ctr,
                                                                 BranchScratch b) {
+  const uint32_t gen = gen0 + (ctr ? ctr[1] : 0u);
   __shared__ double dpart[kBranchThreads];
   __shared__ int ipart[kBranchThreads];
   __shared__ int ipart2[kBranchThreads];
@@ -615,9 +617,9 @@ cudaError_t launch_block_reduce(const double *blk, const double *norm, int n, in
 }
 
 cudaError_t launch_branch(int nw, double *wate, uint64_t seed, uint32_t gen, BranchScratch b,
-                          cudaStream_t st) {
+                          cudaStream_t st, const uint32_t *ctr) {
   if (nw <= 0) return cudaSuccess;
-  branch_kernel<<<1, kBranchThreads, 0, st>>>(nw, wate, seed, gen, b);
+  branch_kernel<<<1, kBranchThreads, 0, st>>>(nw, wate, seed, gen, ctr, b);
   return cudaGetLastError();
 }
 
@@ -625,6 +627,16 @@ cudaError_t launch_gather(const DevSys &hs, DevPop from, DevPop to, const int *s
                           cudaStream_t st) {
   if (nw <= 0) return cudaSuccess;
   gather_kernel<<<nw, 128, 0, st>>>(from, to, src, 2 * hs.N, hs.nt, hs.nprops);
+  return cudaGetLastError();
+}
+
+__global__ void counters_add_kernel(uint32_t *ctr, uint32_t steps, uint32_t gens) {
+  ctr[0] += steps;
+  ctr[1] += gens;
+}
+
+cudaError_t launch_counters_add(uint32_t *ctr, uint32_t steps, uint32_t gens, cudaStream_t st) {
+  counters_add_kernel<<<1, 1, 0, st>>>(ctr, steps, gens);
   return cudaGetLastError();
 }
 

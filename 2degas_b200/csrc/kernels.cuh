@@ -25,6 +25,10 @@ struct MoveArgs {
   double *cnt;        // nw * 4: accepted, proposed, forced, nonzero status
   double *wate;       // nw DMC weights (product over the generation's moves)
   int *status;        // nw status words (OR-ed)
+  // Device counters {move, generation} added to step0 (and to the comb's
+  // generation) when non-null: a CUDA graph replays its launches with the
+  // same arguments, so the Philox counters that must advance are read here.
+  const uint32_t *ctr;
 };
 
 // Raise (never lower) kernel fn's dynamic shared-memory limit on the current
@@ -57,7 +61,9 @@ struct BranchScratch {
   int *ncapped;
 };
 cudaError_t launch_branch(int nw, double *wate, uint64_t seed, uint32_t gen, BranchScratch b,
-                          cudaStream_t st);
+                          cudaStream_t st, const uint32_t *ctr = nullptr);
+// ctr[0] += steps, ctr[1] += gens (one thread; ordered on st).
+cudaError_t launch_counters_add(uint32_t *ctr, uint32_t steps, uint32_t gens, cudaStream_t st);
 // new[j] = old[src[j]] for every walker field.
 cudaError_t launch_gather(const DevSys &hs, DevPop from, DevPop to, const int *src, int nw,
                           cudaStream_t st);

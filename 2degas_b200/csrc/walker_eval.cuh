@@ -90,8 +90,8 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
   t.x = (double *)take(sizeof(double) * 2 * N);
   t.g = (double *)take(sizeof(double) * 2 * N);
   t.q = (double *)take(sizeof(double) * 2 * N);
-  t.G3 = (double *)take(sizeof(double) * 2 * N);
-  t.S3 = (double *)take(sizeof(double) * 3 * N);
+  t.G3 = s.has_u3 ? (double *)take(sizeof(double) * 2 * N) : nullptr;  // u3 only
+  t.S3 = s.has_u3 ? (double *)take(sizeof(double) * 3 * N) : nullptr;
   t.Sb = (double *)take(sizeof(double) * 3 * N);
   t.qbd = (double *)take(sizeof(double) * 2 * N);
   t.lap = (double *)take(sizeof(double) * N);
@@ -170,8 +170,8 @@ __host__ __device__ inline size_t pair_carve(const DevSys &s, char *base, EvalSm
   t.x = (double *)take(sizeof(double) * 2 * N);
   t.g = (double *)take(sizeof(double) * 2 * N);
   t.q = (double *)take(sizeof(double) * 2 * N);
-  t.G3 = (double *)take(sizeof(double) * 2 * N);
-  t.S3 = (double *)take(sizeof(double) * 3 * N);
+  t.G3 = s.has_u3 ? (double *)take(sizeof(double) * 2 * N) : nullptr;  // u3 only
+  t.S3 = s.has_u3 ? (double *)take(sizeof(double) * 3 * N) : nullptr;
   t.Sb = (double *)take(sizeof(double) * 3 * N);
   t.qbd = (double *)take(sizeof(double) * 2 * N);
   t.lap = (double *)take(sizeof(double) * N);
@@ -964,11 +964,13 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
       m.g[2 * i + 1] = gy_s;
       m.lap[i] = lap_s;
       m.vp[i] = vp_s;
-      m.G3[2 * i] = Gx_s;
-      m.G3[2 * i + 1] = Gy_s;
-      m.S3[3 * i] = s3xx_s;
-      m.S3[3 * i + 1] = s3xy_s;
-      m.S3[3 * i + 2] = s3yy_s;
+      if (S.has_u3) {
+        m.G3[2 * i] = Gx_s;
+        m.G3[2 * i + 1] = Gy_s;
+        m.S3[3 * i] = s3xx_s;
+        m.S3[3 * i + 1] = s3xy_s;
+        m.S3[3 * i + 2] = s3yy_s;
+      }
       m.q[2 * i] = m.x[2 * i] + qx_s;
       m.q[2 * i + 1] = m.x[2 * i + 1] + qy_s;
       m.Sb[3 * i] = sbxx_s;

@@ -473,6 +473,86 @@ def serve_arm(args, rank, world):
     return 0
 
 
+def batch_arm(args, rank, world):
+    """Batched uneven populations: 64 DMC populations spanning N in {26, 42,
+    58, 90} and r_s in {1, 2, 5, 10, 20}, half unpolarised (N/2 per spin) and
+    half fully polarised (the nearest closed shell the kernels hold: 25, 45,
+    49, 49), backflow on, 1024 walkers each, advanced together through
+    qmc2d_batch_dmc (one CUDA graph per call), against the same generations
+    issued handle by handle."""
+    import torch
+
+    if rank != 0:
+        return 0
+    q = importlib.import_module("2degas_b200")
+    tables = importlib.import_module("2degas_b200.tables")
+    tmp = tempfile.mkdtemp(prefix="qmc2d_batch_")
+    Ns, rss = [26, 42, 58, 90], [1.0, 2.0, 5.0, 10.0, 20.0]
+    pol_of = {26: 25, 42: 45, 58: 49, 90: 49}
+    nw = args.batch_walkers
+    specs = []
+    for i in range(args.batch_pops):
+        N, pol, rs = Ns[i % 4], (i // 4) % 2, rss[(i // 8) % 5]
+        specs.append((pol_of[N], 0, rs) if pol else (N // 2, N // 2, rs))
+    systems, handles = {}, []
+    for k, (nu, nd, rs) in enumerate(specs):
+        key = (nu, nd, rs)
+        if key not in systems:
+            d = tables.make_run(os.path.join(tmp, f"s{len(systems)}"), "c", nu, nd, rs,
+                                backflow=(0.2, rs, 0.6 * rs))
+            systems[key] = q.System.read(d, "c")
+        s = systems[key]
+        h = q.Handle(s, capacity=nw, seed=1000 + k)
+        h.set_precision(args.precision)
+        L = s.s.el[0]
+        h.population_set(np.random.default_rng(k).uniform(-L / 2, L / 2, size=(nw, 2 * s.N)))
+        handles.append(h)
+    taus = [0.01 * rs * rs for (_, _, rs) in specs]
+    for h, (_, _, rs) in zip(handles, specs):
+        h.vmc(args.equil, 0.05 * rs * rs, 10 ** 9)
+    et = []
+    for h, t in zip(handles, taus):
+        h.block_reset()
+        h.vmc(4, t, 10 ** 9)
+        blk, norm = h.block_get()
+        et.append(blk[0] / norm)
+    K = args.steps
+    moves = K * nw * len(handles)
+    b = q.Batch(handles)
+    b.dmc(2, taus, et)  # warm-up and capture
+    torch.cuda.synchronize()
+    with Clocks(0) as clk:
+        t0 = time.perf_counter()
+        b.dmc(K, taus, et)
+        torch.cuda.synchronize()
+        t_batch = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for h, t, e in zip(handles, taus, et):  # the same work, one population at a time
+            h.dmc(K, 1, t, e, 2.0, 50)
+        torch.cuda.synchronize()
+        t_seq = time.perf_counter() - t0
+    line = {
+        "metric": "walker-moves/sec (64 uneven DMC populations, one graph per call)",
+        "value": moves / t_batch, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": 2,
+        "ms_per_step": 1e3 * t_batch / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f64 (f32 u2 and v2 pair terms)",
+        "data": "synthetic",
+        "config": {"workload": "batched_populations", "populations": len(handles),
+                   "walkers_each": nw, "N": Ns, "rs": rss, "polarised_shells": pol_of,
+                   "tau": "0.01 r_s^2", "precision": args.precision,
+                   "timing": "host wall clock around one qmc2d_batch_dmc call (synchronised)"},
+        "handle_by_handle": {"value": moves / t_seq, "seconds": t_seq},
+        "speedup_vs_handle_by_handle": t_seq / t_batch,
+        "clocks": clk.summary(),
+    }
+    b.close()
+    for h in handles:
+        h.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -486,8 +566,11 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="pair passes in FP64 (default), or u2 and real-space Ewald pair terms "
                          "in FP32 with compensated sums")
-    ap.add_argument("--workload", default="dmc", choices=["dmc", "serve"],
-                    help="dmc: the N=58 DMC generation (default); serve: the serving stream")
+    ap.add_argument("--workload", default="dmc", choices=["dmc", "serve", "batch"],
+                    help="dmc: the N=58 DMC generation (default); serve: the serving stream; "
+                         "batch: 64 uneven populations through one graph")
+    ap.add_argument("--batch-pops", type=int, default=64)
+    ap.add_argument("--batch-walkers", type=int, default=1024)
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-blocks", type=int, default=100)
     ap.add_argument("--serve-slots", type=int, default=32)
@@ -503,6 +586,8 @@ def main():
         return reference_arm(args, rank, world)
     if args.workload == "serve":
         return serve_arm(args, rank, world)
+    if args.workload == "batch":
+        return batch_arm(args, rank, world)
     return b200_arm(args, rank, world, local_rank)
 
 

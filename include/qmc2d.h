@@ -196,6 +196,27 @@ int qmc2d_update_twist(qmc2d_handle *h, const qmc2d_system *sys);
 enum { QMC2D_PRECISION_FP64 = 0, QMC2D_PRECISION_MIXED = 1 };
 int qmc2d_set_precision(qmc2d_handle *h, int precision);
 
+/* Batches: many independent populations (handles of different systems, on
+ * one device) advanced together. The reference runs one population per
+ * process and has no counterpart. A call captures one CUDA graph holding
+ * two steps of every population (each handle's launches on its own stream,
+ * forked from and joined to the batch's stream) and replays it; the
+ * populations' kernels overlap on the GPU. The Philox counters advance in
+ * device memory, so a batch call gives the walkers, block sums and
+ * counters that the same qmc2d_vmc / qmc2d_dmc calls made handle by handle
+ * give. The handles stay usable on their own between batch calls, and must
+ * outlive the batch. */
+typedef struct qmc2d_batch qmc2d_batch;
+int qmc2d_batch_create(qmc2d_handle *const *handles, int n, qmc2d_batch **out);
+int qmc2d_batch_destroy(qmc2d_batch *b);
+/* nstp VMC steps of every population; delta[k]: population k's time step
+ * (qmc2d_vmc per handle). */
+int qmc2d_batch_vmc(qmc2d_batch *b, int nstp, const double *delta, int mage);
+/* ngen DMC generations of one move each (qmc2d_dmc with mmstep 1 per
+ * handle); delta[k] and etrial[k] per population. */
+int qmc2d_batch_dmc(qmc2d_batch *b, int ngen, const double *delta, const double *etrial,
+                    double mmult, int mage);
+
 /* compute_properties (reptation.f:2661): for nw configurations x (2*nptot
  * each) compute g = -grad ln psi (2*nptot), hlap = -lap ln psi per type
  * (ntypes), props (n_props) and the sign s. Host buffers, synchronous. */
