@@ -239,6 +239,19 @@ class Handle:
         code = {"fp64": _capi.PRECISION_FP64, "mixed": _capi.PRECISION_MIXED}[precision]
         self._chk(self.lib.qmc2d_set_precision(self.h, code))
 
+    def set_launch(self, groups=0, stage=0):
+        """Pair-kernel launch choice: walker groups per CTA (1, 2; 0 default)
+        and pair-row staging (0 when it fits, 1 never)."""
+        self._chk(self.lib.qmc2d_set_launch(self.h, groups, stage))
+
+    def autotune(self):
+        """Time the pair kernel's launch choices on the current population,
+        keep the fastest; returns (groups, stage, ms per launch)."""
+        g, st, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self._chk(self.lib.qmc2d_autotune(self.h, ctypes.byref(g), ctypes.byref(st),
+                                          ctypes.byref(ms)))
+        return g.value, st.value, ms.value
+
     def update_twist(self):
         """After system.set_twist(ith, jth): the orbitals use the new wave vectors."""
         self._chk(self.lib.qmc2d_update_twist(self.h, self.system.ptr))

@@ -335,6 +335,65 @@ extern "C" int qmc2d_set_precision(qmc2d_handle *h, int precision) {
   return QMC2D_OK;
 }
 
+extern "C" int qmc2d_set_launch(qmc2d_handle *h, int groups, int stage) {
+  if (!h || groups < 0 || groups > 2 || stage < 0 || stage > 1) {
+    q2d::set_error("qmc2d_set_launch: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  h->hs.tune_groups = groups;
+  h->hs.tune_stage = stage;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *ms) {
+  if (!h) return QMC2D_ERR_ARG;
+  if (h->nw <= 0) {
+    q2d::set_error("qmc2d_autotune: empty population");
+    return QMC2D_ERR_STACK;
+  }
+  CK(cudaSetDevice(h->device));
+  q2d::MoveArgs a{};
+  a.nw = h->nw;
+  a.scr = h->d_mscr;
+  a.delta = h->hs.delta > 0.0 ? h->hs.delta : 0.01;
+  a.seed = h->seed;
+  a.step0 = h->move_counter;  // the next move's proposal; the scratch is rewritten by that move
+  a.blk = h->d_blk;
+  a.blk_norm = h->d_norm;
+  a.cnt = h->d_cnt;
+  a.status = h->d_status;
+  const int var[4][2] = {{2, 0}, {2, 1}, {1, 0}, {1, 1}};
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double best = 1e300;
+  int bg = 2, bs = 0;
+  for (const auto &v : var) {
+    h->hs.tune_groups = v[0];
+    h->hs.tune_stage = v[1];
+    CK(q2d::launch_pairs(h->hs, h->ds, h->pop[h->cur], a, h->stream));  // warm-up
+    CK(cudaEventRecord(e0, h->stream));
+    for (int r = 0; r < 3; r++) CK(q2d::launch_pairs(h->hs, h->ds, h->pop[h->cur], a, h->stream));
+    CK(cudaEventRecord(e1, h->stream));
+    CK(cudaEventSynchronize(e1));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    if (t / 3.0 < best) {
+      best = t / 3.0;
+      bg = v[0];
+      bs = v[1];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->hs.tune_groups = bg;
+  h->hs.tune_stage = bs;
+  if (groups) *groups = bg;
+  if (stage) *stage = bs;
+  if (ms) *ms = best;
+  return QMC2D_OK;
+}
+
 extern "C" int qmc2d_update_twist(qmc2d_handle *h, const qmc2d_system *sys) {
   if (!h || !sys || !sys->gvec || sys->ngvec <= 0 || sys->nptot != h->N) {
     q2d::set_error("qmc2d_update_twist: bad argument");

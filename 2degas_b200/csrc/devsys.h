@@ -49,6 +49,10 @@ struct DevSys {
   // Precision of the pair passes (qmc2d_set_precision): 0 FP64; 1 the u2
   // and v2 pair terms in FP32 with compensated sums read out in FP64.
   int pair_f32;
+  // Launch choices of the pair kernel (host side, qmc2d_autotune): walker
+  // groups per CTA (0: the default, 2) and the staging of the pair rows in
+  // shared memory (0: when they fit, 1: never).
+  int tune_groups, tune_stage;
   const double *coef;  // packed tables: ut rows (4 doubles each) and v_k lists
   const double *kvec;  // 2*nk
   const double *gvec;  // 2*ngvec

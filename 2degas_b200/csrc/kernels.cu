@@ -123,21 +123,24 @@ size_t move_smem_bytes(const DevSys &s) {
 // reverse move, metropolis_test and the averages, with the walker's state
 // in shared memory.
 //
-// pairs_kernel is persistent: one CTA per SM walks over the population with
-// kPairGroups independent groups of kThreads threads, each on its own walker
-// and its own named barrier, so one group's latency overlaps the other's.
-// Its random spline-row lookups (three per pair) go to a shared-memory copy
-// of the pair rows when they fit (stage_rows), made once per launch and
-// shared by the groups; random rows in global memory cost an L1 tag lookup
-// per lane, shared memory a few bank wavefronts per warp.
-constexpr int kPairGroups = 2;
-constexpr int kPairThreads = kPairGroups * kThreads;
+// pairs_kernel is persistent: its CTAs walk over the population with G
+// independent groups of kThreads threads each, every group on its own
+// walker and its own named barrier, so one group's latency overlaps the
+// other's. Its random spline-row lookups (three per pair) go to a
+// shared-memory copy of the pair rows when they fit and are wanted
+// (stage_rows), made once per launch and shared by the groups; random rows
+// in global memory cost an L1 tag lookup per lane, shared memory a few bank
+// wavefronts per warp. G and the staging are the launch choices that
+// qmc2d_autotune times (DevSys::tune_groups, tune_stage); by default G = 2
+// with the rows staged. Both caps keep 128 registers a thread (G = 2: one
+// 512-thread CTA per SM; G = 1: up to two 256-thread CTAs).
 
 //
 // R is the precision of the u2 and v2 pair terms (qmc2d_set_precision).
-template <class R>
-__global__ void __launch_bounds__(kPairThreads, 1) pairs_kernel(const DevSys *sp, DevPop pop,
-                                                                MoveArgs a, int stage_rows) {
+template <class R, int G>
+__global__ void __launch_bounds__(G * kThreads, 2 / G) pairs_kernel(const DevSys *sp, DevPop pop,
+                                                                    MoveArgs a, int stage_rows) {
+  constexpr int kPairGroups = G, kPairThreads = G * kThreads;
   __shared__ DevSys S;
   extern __shared__ __align__(16) char smem[];
   load_sys(S, sp);
@@ -569,6 +572,30 @@ cudaError_t launch_eval(const DevSys &hs, const DevSys *ds, int nw, const double
   return cudaGetLastError();
 }
 
+template <class R, int G>
+static cudaError_t launch_pairs_t(const DevSys &hs, const DevSys *ds, DevPop pop,
+                                  const MoveArgs &a, cudaStream_t st, int nsm, int optin) {
+  const void *k = (const void *)pairs_kernel<R, G>;
+  const size_t carve = G * ((pair_carve(hs, nullptr, nullptr, kThreads) + 127) & ~size_t(127));
+  const size_t rows =
+      sizeof(R) * RowLayout<R>::sstride * (size_t)hs.cmb_nblk * (hs.cmb_ng + 1);
+  const int stage =
+      hs.tune_stage != 1 && carve + rows + sizeof(DevSys) <= (size_t)optin ? 1 : 0;
+  const size_t sm = carve + (stage ? rows : 0);
+  cudaError_t e;
+  if ((e = set_smem(k, sm)) != cudaSuccess) return e;
+  int per_sm = 1;
+  if (G == 1 &&
+      (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G * kThreads, sm)) !=
+          cudaSuccess)
+    return e;
+  const int need = (a.nw + G - 1) / G;
+  const int cap = nsm * (per_sm > 0 ? per_sm : 1);
+  const int grid = need < cap ? need : cap;
+  pairs_kernel<R, G><<<grid, G * kThreads, sm, st>>>(ds, pop, a, stage);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_pairs(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
                          cudaStream_t st) {
   if (a.nw <= 0) return cudaSuccess;
@@ -580,23 +607,12 @@ cudaError_t launch_pairs(const DevSys &hs, const DevSys *ds, DevPop pop, const M
   if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) !=
       cudaSuccess)
     return e;
-  const size_t carve =
-      kPairGroups * ((pair_carve(hs, nullptr, nullptr, kThreads) + 127) & ~size_t(127));
-  const size_t rows = (hs.pair_f32 ? sizeof(float) * RowLayout<float>::sstride
-                                   : sizeof(double) * RowLayout<double>::sstride) *
-                      (size_t)hs.cmb_nblk * (hs.cmb_ng + 1);
-  const int stage = carve + rows + sizeof(DevSys) <= (size_t)optin ? 1 : 0;
-  const size_t sm = carve + (stage ? rows : 0);
-  const void *k =
-      hs.pair_f32 ? (const void *)pairs_kernel<float> : (const void *)pairs_kernel<double>;
-  if ((e = set_smem(k, sm)) != cudaSuccess) return e;
-  const int need = (a.nw + kPairGroups - 1) / kPairGroups;
-  const int grid = need < nsm ? need : nsm;
+  const bool one = hs.tune_groups == 1;
   if (hs.pair_f32)
-    pairs_kernel<float><<<grid, kPairThreads, sm, st>>>(ds, pop, a, stage);
-  else
-    pairs_kernel<double><<<grid, kPairThreads, sm, st>>>(ds, pop, a, stage);
-  return cudaGetLastError();
+    return one ? launch_pairs_t<float, 1>(hs, ds, pop, a, st, nsm, optin)
+               : launch_pairs_t<float, 2>(hs, ds, pop, a, st, nsm, optin);
+  return one ? launch_pairs_t<double, 1>(hs, ds, pop, a, st, nsm, optin)
+             : launch_pairs_t<double, 2>(hs, ds, pop, a, st, nsm, optin);
 }
 
 cudaError_t launch_move(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,

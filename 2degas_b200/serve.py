@@ -133,6 +133,7 @@ def run_request(p, device=0):
         h.population_set(x0)
         h.vmc(req.equil_steps, tau_vmc, 10 ** 9)  # from uniform positions
         moves += req.equil_steps * req.walkers
+        h.autotune()  # the pair kernel's launch choice for this population
         etrial = None
         if req.method == "dmc":
             h.block_reset()

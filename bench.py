@@ -273,6 +273,7 @@ def b200_arm(args, rank, world, local_rank):
     h.set_precision(args.precision)
     h.population_set(x0)
     h.vmc(args.equil, delta, 10 ** 9)  # seeded VMC equilibration
+    tuned = h.autotune()  # pair-kernel launch choice, timed on this population
     h.block_reset()
     h.vmc(10, delta, 10 ** 9)
     blk, norm = h.block_get()
@@ -382,6 +383,7 @@ def b200_arm(args, rank, world, local_rank):
             "data": "synthetic",
             "config": {"workload": CONFIG, "walkers_per_gpu": nw, "N": N, "rs": rs,
                        "precision": args.precision,
+                       "pair_launch": {"groups": tuned[0], "stage_rows": tuned[1] == 0},
                        "tau": delta, "mmstep": 1, "moves_per_step": nw * world,
                        "l2": "flushed between timed steps (256 MiB write)",
                        "parallelism": f"independent populations x{world}"},
@@ -510,6 +512,7 @@ def batch_arm(args, rank, world):
     taus = [0.01 * rs * rs for (_, _, rs) in specs]
     for h, (_, _, rs) in zip(handles, specs):
         h.vmc(args.equil, 0.05 * rs * rs, 10 ** 9)
+        h.autotune()
     et = []
     for h, t in zip(handles, taus):
         h.block_reset()

@@ -196,6 +196,17 @@ int qmc2d_update_twist(qmc2d_handle *h, const qmc2d_system *sys);
 enum { QMC2D_PRECISION_FP64 = 0, QMC2D_PRECISION_MIXED = 1 };
 int qmc2d_set_precision(qmc2d_handle *h, int precision);
 
+/* Launch choices of the pair kernel (the proposal and pair passes of a
+ * move): walker groups per CTA (1 or 2; 0 = the default, 2) and whether the
+ * pair rows are staged in shared memory (stage 0: when they fit; 1: never,
+ * read from global memory). Every choice computes the same values.
+ * qmc2d_autotune times the four choices on the handle's current population
+ * (three launches each after a warm-up; the population is not changed),
+ * keeps the fastest and returns it with its time per launch. The reference
+ * has no counterpart. */
+int qmc2d_set_launch(qmc2d_handle *h, int groups, int stage);
+int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *ms);
+
 /* Batches: many independent populations (handles of different systems, on
  * one device) advanced together. The reference runs one population per
  * process and has no counterpart. A call captures one CUDA graph holding

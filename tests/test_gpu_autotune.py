@@ -1,0 +1,47 @@
+"""Pair-kernel launch choices (qmc2d_set_launch) and their autotuner
+(qmc2d_autotune): every choice of walker groups per CTA and pair-row
+staging gives the same walkers bit for bit, and tuning leaves the
+population and the random streams where they were."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+DELTA = 0.05
+
+
+def _run(q, s, x, seed, launch=None, tune=False, nstp=3):
+    with q.Handle(s, capacity=len(x), seed=seed) as h:
+        h.population_set(x)
+        if launch:
+            h.set_launch(*launch)
+        got = None
+        if tune:
+            before = h.population_get()
+            got = h.autotune()
+            after = h.population_get()
+            assert np.array_equal(before["x"], after["x"])
+        h.vmc(nstp, DELTA, 10 ** 9)
+        return h.population_get(), got
+
+
+@pytest.mark.parametrize("launch", [(1, 0), (1, 1), (2, 1), (2, 0)])
+def test_every_launch_choice_gives_the_same_walkers(q, n26, n26_configs, launch):
+    ref, _ = _run(q, n26, n26_configs, 7)
+    got, _ = _run(q, n26, n26_configs, 7, launch=launch)
+    assert np.array_equal(got["x"], ref["x"]) and np.array_equal(got["p"], ref["p"])
+
+
+def test_autotune_picks_a_choice_and_changes_nothing(q, n26, n26_configs):
+    ref, _ = _run(q, n26, n26_configs, 9)
+    got, (g, st, ms) = _run(q, n26, n26_configs, 9, tune=True)
+    assert g in (1, 2) and st in (0, 1) and ms > 0
+    assert np.array_equal(got["x"], ref["x"]) and np.array_equal(got["p"], ref["p"])
+
+
+def test_set_launch_rejects_bad_choices(q, n26, n26_configs):
+    with q.Handle(n26, capacity=4, seed=1) as h:
+        with pytest.raises(q.QMCError):
+            h.set_launch(3, 0)
+        with pytest.raises(q.QMCError):
+            h.set_launch(1, 2)
