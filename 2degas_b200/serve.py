@@ -66,7 +66,7 @@ class Request:
     min_blocks: int = 5
     max_blocks: int = 500
     equil_steps: int = 100
-    tau: float = 0.0             # time step (Ry^-1); 0: 0.05 r_s^2 for VMC, 0.01 r_s^2 for DMC
+    tau: float = 0.0             # time step (Ry^-1); 0: chosen (see run_request)
     rid: int = -1
 
     @property
@@ -123,7 +123,7 @@ def run_request(p, device=0):
     q = importlib.import_module("2degas_b200")
     req, s = p.req, p.system
     tau_vmc = 0.05 * req.rs * req.rs
-    tau = req.tau or (0.01 if req.method == "dmc" else 0.05) * req.rs * req.rs
+    tau = req.tau or tau_vmc
     L = s.s.el[0]
     rng = np.random.default_rng(req.seed)
     x0 = rng.uniform(-0.5 * L, 0.5 * L, size=(req.walkers, 2 * s.N))
@@ -137,10 +137,15 @@ def run_request(p, device=0):
         etrial = None
         if req.method == "dmc":
             h.block_reset()
-            h.vmc(req.block_steps, tau, 10 ** 9)
+            h.vmc(req.block_steps, tau_vmc, 10 ** 9)
             moves += req.block_steps * req.walkers
             blk, norm = h.block_get()
             etrial = blk[0] / norm
+            if not req.tau:
+                # a DMC weight is exp(-tau N (E_L - E_T)) with E_L per electron: keep
+                # tau N sigma(E_L) near 0.1 so that the comb copies few walkers a step
+                sig = float(np.std(h.population_get()["p"][:, 0]))
+                tau = min(0.01 * req.rs * req.rs, 0.1 / max(s.N * sig, 1e-12))
         st = q.Stats(s)
         status, mean, err, nb = "max_blocks", float("nan"), float("nan"), 0
         for _ in range(req.max_blocks):

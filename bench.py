@@ -45,7 +45,7 @@ UNIT = "walker-moves/s"
 # walker records and the move scratch), plus the move scratch block the pair
 # kernel writes, which reaches DRAM at 4096 walkers (356 MB > L2) though not
 # in the 296-walker capture.
-MOVE_DRAM_READ_PER_WALKER = (0.956160e6 + 27.777792e6) / 296
+MOVE_DRAM_READ_PER_WALKER = (1.086976e6 + 28.344320e6) / 296
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum of pairs_kernel + move_kernel (296 walkers) "
                   "x walkers/296, + the move scratch written per walker")
 
@@ -576,7 +576,7 @@ def main():
     ap.add_argument("--batch-walkers", type=int, default=1024)
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-blocks", type=int, default=100)
-    ap.add_argument("--serve-slots", type=int, default=32)
+    ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--phases", action="store_true",
                     help="print SM cycles per walker-move of each move-kernel phase instead")
     args = ap.parse_args()
