@@ -277,6 +277,17 @@ class Handle:
                                               ctypes.byref(ib), ctypes.byref(et)))
         return ib.value, et.value
 
+    def restart_read_rmc(self, stats, directory, runid, ntau, ntauskip, mdelta, delta, etrial,
+                         mage, mage_r, rank=0):
+        """restart(0) + read_path for reptation: the stored paths become
+        ntau-bead reptiles; returns the stored block."""
+        ib = ctypes.c_int()
+        prm = _capi.RmcParams(ntau, ntauskip, mdelta, delta, etrial, mage, mage_r)
+        self._chk(self.lib.qmc2d_restart_read_rmc(self.h, self.system.ptr, stats.p,
+                                                  ctypes.byref(prm), str(directory).encode(),
+                                                  runid.encode(), rank, ctypes.byref(ib)))
+        return ib.value
+
 
 class Stats:
     """Cumulative block statistics of averages(3) (qmc2d_stats_*)."""

@@ -196,6 +196,8 @@ SIGNATURES = {
                                     ctypes.c_char_p, ctypes.c_char_p, c_int]),
     "qmc2d_restart_read": (c_int, [c_void_p, SYSP, c_void_p, ctypes.c_char_p, ctypes.c_char_p,
                                    ctypes.c_char_p, c_int, POINTER(c_int), PD]),
+    "qmc2d_restart_read_rmc": (c_int, [c_void_p, SYSP, c_void_p, POINTER(RmcParams),
+                                       ctypes.c_char_p, ctypes.c_char_p, c_int, POINTER(c_int)]),
     "qmc2d_vmc": (c_int, [c_void_p, c_int, c_double, c_int]),
     "qmc2d_dmc": (c_int, [c_void_p, c_int, c_int, c_double, c_double, c_double, c_int]),
     "qmc2d_rmc_init": (c_int, [c_void_p, c_int, POINTER(RmcParams), PD]),

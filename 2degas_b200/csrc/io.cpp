@@ -267,14 +267,14 @@ extern "C" int qmc2d_restart_write(qmc2d_handle *h, const qmc2d_system *sys,
   return QMC2D_OK;
 }
 
-extern "C" int qmc2d_restart_read(qmc2d_handle *h, const qmc2d_system *sys, qmc2d_stats *st,
-                                  const char *who, const char *dir, const char *runid, int rank,
-                                  int *iblk, double *etrial) {
-  if (!h || !sys || !st || !who || !runid || st->n_props != sys->n_props)
-    return fail(QMC2D_ERR_ARG, "qmc2d_restart_read: bad argument");
-  const std::string w(who);
-  if (w != "vmc" && w != "dmc")
-    return fail(QMC2D_ERR_ARG, "qmc2d_restart_read: who must be vmc or dmc");
+namespace {
+
+// restart(0) of who's .res file: the block, the cumulative sums into st and
+// the stream state into the handle; then every stored configuration (all
+// types' <x_file>.res.<rank> files) into *x, their count into *nconf.
+int read_res(qmc2d_handle *h, const qmc2d_system *sys, qmc2d_stats *st, const char *dir,
+             const char *runid, int rank, int *iblk, double *etrial, std::vector<double> *x,
+             int *nconf_out) {
   const std::string d = dir ? dir : "";
   const std::string res = join(d, std::string(runid) + ".res");
   std::ifstream f(res);
@@ -309,10 +309,47 @@ extern "C" int qmc2d_restart_read(qmc2d_handle *h, const qmc2d_system *sys, qmc2
     if (line.find_first_not_of(" \t\r") != std::string::npos) lines++;
   const int nconf = (int)(lines / sys->np[0]);
   if (nconf <= 0) return fail(QMC2D_ERR_PARSE, "no configurations in " + res);
-  std::vector<double> x((size_t)nconf * 2 * sys->nptot);
+  x->assign((size_t)nconf * 2 * sys->nptot, 0.0);
   int got = 0;
-  int s2 = qmc2d_read_configs(sys, d.c_str(), suffix.c_str(), 0, nconf, x.data(), &got);
+  int s2 = qmc2d_read_configs(sys, d.c_str(), suffix.c_str(), 0, nconf, x->data(), &got);
   if (s2) return s2;
   if (got != nconf) return fail(QMC2D_ERR_PARSE, "configuration files of unequal length");
+  *nconf_out = nconf;
+  return QMC2D_OK;
+}
+
+}  // namespace
+
+extern "C" int qmc2d_restart_read(qmc2d_handle *h, const qmc2d_system *sys, qmc2d_stats *st,
+                                  const char *who, const char *dir, const char *runid, int rank,
+                                  int *iblk, double *etrial) {
+  if (!h || !sys || !st || !who || !runid || st->n_props != sys->n_props)
+    return fail(QMC2D_ERR_ARG, "qmc2d_restart_read: bad argument");
+  const std::string w(who);
+  if (w != "vmc" && w != "dmc")
+    return fail(QMC2D_ERR_ARG, "qmc2d_restart_read: who must be vmc or dmc");
+  std::vector<double> x;
+  int nconf = 0;
+  int s2 = read_res(h, sys, st, dir, runid, rank, iblk, etrial, &x, &nconf);
+  if (s2) return s2;
   return qmc2d_population_set(h, nconf, x.data());
+}
+
+extern "C" int qmc2d_restart_read_rmc(qmc2d_handle *h, const qmc2d_system *sys,
+                                      qmc2d_stats *st, const qmc2d_rmc_params *prm,
+                                      const char *dir, const char *runid, int rank, int *iblk) {
+  if (!h || !sys || !st || !prm || !runid || st->n_props != sys->n_props || prm->ntau < 2)
+    return fail(QMC2D_ERR_ARG, "qmc2d_restart_read_rmc: bad argument");
+  std::vector<double> x;
+  int nconf = 0;
+  int s2 = read_res(h, sys, st, dir, runid, rank, iblk, nullptr, &x, &nconf);
+  if (s2) return s2;
+  if (nconf % prm->ntau != 0)
+    return fail(QMC2D_ERR_PARSE, "qmc2d_restart_read_rmc: " + std::to_string(nconf) +
+                                     " stored configurations are not whole paths of " +
+                                     std::to_string(prm->ntau) + " beads");
+  const uint32_t step = h->rmc.step;  // qmc2d_rmc_init starts the reptation counter at 0
+  if ((s2 = qmc2d_rmc_init(h, nconf / prm->ntau, prm, x.data()))) return s2;
+  h->rmc.step = step;
+  return QMC2D_OK;
 }

@@ -122,8 +122,6 @@ def run_request(p, device=0):
 
     q = importlib.import_module("2degas_b200")
     req, s = p.req, p.system
-    tau_vmc = 0.05 * req.rs * req.rs
-    tau = req.tau or tau_vmc
     L = s.s.el[0]
     rng = np.random.default_rng(req.seed)
     x0 = rng.uniform(-0.5 * L, 0.5 * L, size=(req.walkers, 2 * s.N))
@@ -131,21 +129,31 @@ def run_request(p, device=0):
     with q.Handle(s, capacity=req.walkers, seed=req.seed, device=device) as h:
         h.set_precision(req.precision)
         h.population_set(x0)
-        h.vmc(req.equil_steps, tau_vmc, 10 ** 9)  # from uniform positions
-        moves += req.equil_steps * req.walkers
+        # Equilibration from uniform positions, in chunks of 10 VMC steps with
+        # forced moves after 50 rejections (age, as the reference's mage):
+        # the all-electron step is scaled after each chunk toward 50%
+        # acceptance, which falls with N at a fixed step. At 0.05 r_s^2,
+        # N = 50 accepted 5% of moves and one stuck walker held the DMC
+        # population (the oracle shows the same).
+        dv = 0.05 * req.rs * req.rs
+        c0 = h.counters()
+        for _ in range(max(1, req.equil_steps // 10)):
+            h.vmc(10, dv, 50)
+            moves += 10 * req.walkers
+            c1 = h.counters()
+            acc = (c1["accepted"] - c0["accepted"]) / max(c1["proposed"] - c0["proposed"], 1.0)
+            c0 = c1
+            dv *= min(2.0, max(0.3, acc / 0.5))
         h.autotune()  # the pair kernel's launch choice for this population
+        # DMC at a tenth of the VMC step (acceptance near 97%)
+        tau = req.tau or (dv / 10.0 if req.method == "dmc" else dv)
         etrial = None
         if req.method == "dmc":
             h.block_reset()
-            h.vmc(req.block_steps, tau_vmc, 10 ** 9)
+            h.vmc(req.block_steps, dv, 50)
             moves += req.block_steps * req.walkers
             blk, norm = h.block_get()
             etrial = blk[0] / norm
-            if not req.tau:
-                # a DMC weight is exp(-tau N (E_L - E_T)) with E_L per electron: keep
-                # tau N sigma(E_L) near 0.1 so that the comb copies few walkers a step
-                sig = float(np.std(h.population_get()["p"][:, 0]))
-                tau = min(0.01 * req.rs * req.rs, 0.1 / max(s.N * sig, 1e-12))
         st = q.Stats(s)
         status, mean, err, nb = "max_blocks", float("nan"), float("nan"), 0
         for _ in range(req.max_blocks):
@@ -153,7 +161,7 @@ def run_request(p, device=0):
             if req.method == "dmc":
                 h.dmc(req.block_steps, 1, tau, etrial, 2.0, 50)
             else:
-                h.vmc(req.block_steps, tau, 10 ** 9)
+                h.vmc(req.block_steps, tau, 50)
             moves += req.block_steps * req.walkers
             blk, norm = h.block_get()
             st.add_block(blk, norm)

@@ -343,6 +343,13 @@ int qmc2d_restart_write(qmc2d_handle *h, const qmc2d_system *sys, const qmc2d_st
 int qmc2d_restart_read(qmc2d_handle *h, const qmc2d_system *sys, qmc2d_stats *st,
                        const char *who, const char *dir, const char *runid, int rank,
                        int *iblk, double *etrial);
+/* restart(0) for who "rmc" followed by read_path (reptation.f:4508-4540,
+ * 1775-1802): the .res file back into st and the handle's streams, the
+ * stored paths (nrep*prm->ntau configurations, reptile-major, as
+ * qmc2d_restart_write writes them) become prm->ntau-bead reptiles as
+ * qmc2d_rmc_init makes them: every bead evaluated again, the bead
+ * acceptances and path properties recomputed, ages zero, as read_path does.
+ * The reptation counter continues from the stored one. */
 
 /* VMC: nstp steps of move + metropolis_test + averages(2) on every walker
  * (vmc loop body, reptation.f:995-1003; move :4617; metropolis_test :2622).
@@ -373,6 +380,10 @@ int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params *prm,
 int qmc2d_rmc(qmc2d_handle *h, int nstp);
 /* Copy reptile r's path (ntau beads, x then props) out. */
 int qmc2d_rmc_get_path(qmc2d_handle *h, int r, double *x, double *props);
+/* Reptation restart: see the restart(0) comment above qmc2d_vmc. */
+int qmc2d_restart_read_rmc(qmc2d_handle *h, const qmc2d_system *sys, qmc2d_stats *st,
+                           const qmc2d_rmc_params *prm, const char *dir, const char *runid,
+                           int rank, int *iblk);
 
 /* ----------------------------------------------------- streams and timing
  * The reference has no timers; these expose device time per kernel. */

@@ -79,3 +79,61 @@ def test_tabc_visits_the_grid_in_order(q, n26, n26_configs):
     n26.set_twist(1, 1)
     assert done == seen == [(1, 1), (1, 2), (2, 1), (2, 2)]
     assert rest == [(2, 1), (2, 2)]
+
+
+def _state_line(path):
+    """The stream-state line of a .res file: seed words, move, generation and
+    reptation counters."""
+    lines = open(path).read().splitlines()
+    for ln in lines[2:]:
+        f = ln.split()
+        if len(f) == 8 and all(t.lstrip("-").isdigit() for t in f):
+            return [int(t) for t in f]
+    raise AssertionError("no state line")
+
+
+def test_reptation_restart_rebuilds_the_paths(q, n26, n26_configs, tmp_path):
+    """restart(1) of a reptation run, then restart(0) + read_path in a fresh
+    handle: the same paths, every bead evaluated again to the same values,
+    and the reptation counter carried on."""
+    nrep, ntau = 3, 8
+    prm = (ntau, 1, 2, 0.05, -0.43, 1000, 1000)
+    x0 = n26_configs[: nrep * ntau]
+    st = q.Stats(n26)
+    with q.Handle(n26, capacity=nrep, seed=21) as h:
+        h.rmc_init(nrep, x0, *prm)
+        h.block_reset()
+        h.rmc(4)
+        blk, norm = h.block_get()
+        st.add_block(blk, norm)
+        h.restart_write(st, 1, "rmc", tmp_path, "n26")
+        paths = [h.rmc_get_path(r, ntau) for r in range(nrep)]
+    assert _state_line(tmp_path / "n26.res")[4] == 4
+    st2 = q.Stats(n26)
+    out = tmp_path / "again"
+    out.mkdir()
+    with q.Handle(n26, capacity=nrep, seed=999) as h:
+        iblk = h.restart_read_rmc(st2, tmp_path, "n26", *prm)
+        assert iblk == 1
+        for r in range(nrep):
+            xr, pr = h.rmc_get_path(r, ntau)
+            assert np.array_equal(xr, paths[r][0])
+            keep = [i for i in range(14) if i != 2]  # jacc is recomputed, as read_path does
+            np.testing.assert_allclose(pr[:, keep], paths[r][1][:, keep], rtol=1e-12, atol=1e-14)
+        h.rmc(2)
+        h.restart_write(st2, 2, "rmc", out, "n26")
+    assert _state_line(out / "n26.res")[4] == 6
+    m1, _, n1, b1 = st.get()
+    m2, _, n2, b2 = st2.get()
+    np.testing.assert_allclose(m2, m1, rtol=1e-15)
+    assert (n2, b2) == (n1, b1)
+
+
+def test_reptation_restart_needs_whole_paths(q, n26, n26_configs, tmp_path):
+    st = q.Stats(n26)
+    with q.Handle(n26, capacity=16, seed=3) as h:
+        h.population_set(n26_configs[:10])
+        h.restart_write(st, 1, "vmc", tmp_path, "n26")
+    with q.Handle(n26, capacity=4, seed=3) as h:
+        with pytest.raises(q.QMCError):
+            h.restart_read_rmc(q.Stats(n26), tmp_path, "n26", 8, 1, 2, 0.05, -0.43, 1000, 1000)
