@@ -740,6 +740,8 @@ __device__ inline void gj_invert_reg(double2 *W, int ld, int n, int *perm, doubl
           bw = w;
         }
       }
+      // Every unused row's key has 255 - r in its low byte, so p is an unused
+      // row < n at every step, an exactly zero or NaN column included.
       const int p = 255 - (int)(best & 0xFFull);
       const double2 *ps = slots + (buf * G + bw) * sw;
       const double2 piv = ps[k];

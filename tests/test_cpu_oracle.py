@@ -197,3 +197,61 @@ def test_statistics_against_reference_block():
     # the oracle's wave function is spin-symmetric: kin_up = kin_down
     assert abs(mean[9] - mean[10]) < 5 * np.hypot(sd[9], sd[10])
     assert abs(gold[9] - gold[10]) > 0.4
+
+
+def _numpy_minus_log_psi(s, x):
+    """-ln psi of a Slater-Jastrow deck with an eta = 0 backflow table (so
+    q = x) and no u3, restated in numpy independently of the oracle's C: the
+    u2 spline of getf (reptation.f:4114) over minimum-image pairs, and
+    ln|det| of each spin's plane-wave matrix exp(i g_k . x_j) by LAPACK's LU
+    (numpy slogdet)."""
+    S = s.s
+    N, L = S.nptot, np.array([S.el[0], S.el[1]])
+    xy = x.reshape(N, 2)
+    u = 0.0
+    for a in range(S.ntypes):
+        for b in range(S.ntypes):
+            t = S.iu2[a][b]
+            tb = S.tables[t]
+            ut = np.ctypeslib.as_array(tb.ut, shape=(4 * (tb.ngrid + 1),)).reshape(-1, 4)
+            ia = range(S.ipfrst[a], S.ipfrst[a] + S.np[a])
+            ib = range(S.ipfrst[b], S.ipfrst[b] + S.np[b])
+            for i in ia:
+                for j in ib:
+                    if j <= i:
+                        continue
+                    d = xy[i] - xy[j]
+                    d -= L * np.round(d / L)
+                    r = np.hypot(d[0], d[1])
+                    ind = int(r * S.drti)
+                    rem = r - ind * S.drt
+                    c = ut[min(ind, tb.ngrid)]
+                    rm = rem * S.drti
+                    u += c[0] + rm * (c[1] + rm * (c[2] + rm * c[3]))
+    g = np.ctypeslib.as_array(S.gvec, shape=(2 * S.ngvec,)).reshape(-1, 2)
+    logdet = 0.0
+    for a in range(S.ntypes):
+        n, f = S.np[a], S.ipfrst[a]
+        A = np.exp(1j * (g[:n] @ xy[f:f + n].T))
+        logdet += np.linalg.slogdet(A)[1]
+    return u - logdet
+
+
+@pytest.mark.parametrize("deck", [(13, 13, 1.0), (5, 5, 2.0), (9, 0, 3.0), (1, 1, 1.5)])
+def test_minus_log_psi_against_numpy_slogdet(oracle_cls, q, tmp_path, deck):
+    """The oracle's -ln psi on plane-wave Slater-Jastrow decks (eta = 0
+    backflow tables) equals an independent numpy restatement (spline sum +
+    slogdet) to 1e-12 relative."""
+    import importlib
+
+    tables = importlib.import_module("2degas_b200.tables")
+    nu, nd, rs = deck
+    d = tables.make_run(os.path.join(tmp_path, "d"), "c", nu, nd, rs, nconf=6, seed=5,
+                        backflow=(0.0, rs, 0.6 * rs))
+    s = q.System.read(d, "c")
+    x = s.read_configs(d, ".0", 0, 6)
+    o = oracle_cls(s.ptr)
+    for k in range(len(x)):
+        _, _, p, _, _ = o.compute_properties(x[k])
+        want = _numpy_minus_log_psi(s, x[k])
+        assert abs(p[1] - want) <= 1e-12 * max(1.0, abs(want)), (deck, k, p[1], want)
