@@ -239,6 +239,11 @@ class Handle:
         code = {"fp64": _capi.PRECISION_FP64, "mixed": _capi.PRECISION_MIXED}[precision]
         self._chk(self.lib.qmc2d_set_precision(self.h, code))
 
+    def set_dmc_ecut(self, ecut):
+        """Clamp E_L in the DMC weight to etrial +- ecut (Ry/electron; 0: off,
+        the reference's weights)."""
+        self._chk(self.lib.qmc2d_set_dmc_ecut(self.h, ecut))
+
     def set_launch(self, groups=0, stage=0):
         """Pair-kernel launch choice: walker groups per CTA (1, 2; 0 default)
         and pair-row staging (0 when it fits, 1 never)."""

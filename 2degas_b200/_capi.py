@@ -176,6 +176,7 @@ SIGNATURES = {
     "qmc2d_update_twist": (c_int, [c_void_p, SYSP]),
     "qmc2d_set_precision": (c_int, [c_void_p, c_int]),
     "qmc2d_footprint": (c_int, [SYSP, c_int, ctypes.POINTER(c_uint64)]),
+    "qmc2d_set_dmc_ecut": (c_int, [c_void_p, c_double]),
     "qmc2d_set_launch": (c_int, [c_void_p, c_int, c_int]),
     "qmc2d_autotune": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), PD]),
     "qmc2d_batch_create": (c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p)]),

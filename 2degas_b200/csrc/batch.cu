@@ -76,6 +76,7 @@ cudaError_t enqueue(qmc2d_batch *b, int k, int g0, int ngen, int dmc, double del
     a.mage = mage;
     a.etrial = etrial;
     a.mmult = mmult;
+    a.ecut = dmc ? h->dmc_ecut : 0.0;
     a.seed = h->seed;
     a.step0 = (uint32_t)(g0 + g);
     a.blk = h->d_blk;
@@ -155,6 +156,7 @@ int run(qmc2d_batch *b, int n, int dmc, const double *delta, const double *etria
       key.push_back((double)b->h[k]->nw);
       key.push_back((double)b->h[k]->cur);
       key.push_back((double)(intptr_t)b->h[k]);
+      key.push_back(b->h[k]->dmc_ecut);
     }
     if (!b->exec || key != b->key) {
       if (b->exec) {

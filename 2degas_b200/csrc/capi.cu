@@ -335,6 +335,15 @@ extern "C" int qmc2d_set_precision(qmc2d_handle *h, int precision) {
   return QMC2D_OK;
 }
 
+extern "C" int qmc2d_set_dmc_ecut(qmc2d_handle *h, double ecut) {
+  if (!h || !(ecut >= 0.0)) {
+    q2d::set_error("qmc2d_set_dmc_ecut: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  h->dmc_ecut = ecut;
+  return QMC2D_OK;
+}
+
 extern "C" int qmc2d_set_launch(qmc2d_handle *h, int groups, int stage) {
   if (!h || groups < 0 || groups > 2 || stage < 0 || stage > 1) {
     q2d::set_error("qmc2d_set_launch: bad argument");
@@ -648,6 +657,7 @@ static int run_moves(qmc2d_handle *h, int nstp, int dmc, double delta, double et
   a.mage = mage;
   a.etrial = etrial;
   a.mmult = mmult;
+  a.ecut = dmc ? h->dmc_ecut : 0.0;
   a.seed = h->seed;
   a.step0 = h->move_counter;
   a.blk = h->d_blk;

@@ -30,6 +30,7 @@ struct qmc2d_handle {
   int device = 0;
   uint64_t seed = 0;
   uint32_t move_counter = 0, gen_counter = 0;
+  double dmc_ecut = 0.0;  // qmc2d_set_dmc_ecut (0: the reference's weights)
   q2d::RmcState rmc{};
   // per-kernel CUDA-event timing (qmc2d_profile)
   bool prof = false;

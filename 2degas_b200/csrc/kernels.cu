@@ -314,8 +314,12 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
   if (tid == 0) v.po[QMC2D_JACC] = p;
   double wgt = 1.0;
   if (a.dmc) {
-    // dmc weight (reptation.f:898-903), multiplied over the generation's moves
-    double peso = exp(-S.npnorm * (elocal - a.etrial) * a.delta);
+    // dmc weight (reptation.f:898-903), multiplied over the generation's moves;
+    // with ecut > 0 (qmc2d_set_dmc_ecut, not in the reference) the local
+    // energy in the weight is first clamped to etrial +- ecut
+    double el = elocal;
+    if (a.ecut > 0.0) el = fmin(fmax(el, a.etrial - a.ecut), a.etrial + a.ecut);
+    double peso = exp(-S.npnorm * (el - a.etrial) * a.delta);
     if (peso > a.mmult) peso = a.mmult;
     wate *= peso;
     wgt = wate;

@@ -17,6 +17,7 @@ struct MoveArgs {
   double delta;
   double mage;        // forced-move age (compared with ==, as the reference)
   double etrial, mmult;
+  double ecut;        // > 0: clamp E_L in the DMC weight to etrial +- ecut
   uint64_t seed;
   uint32_t step0;     // Philox c2 of this move
   double *scr;        // nw * move_scratch(s).stride doubles (MoveScratch blocks)

@@ -147,13 +147,23 @@ def run_request(p, device=0):
         h.autotune()  # the pair kernel's launch choice for this population
         # DMC at a tenth of the VMC step (acceptance near 97%)
         tau = req.tau or (dv / 10.0 if req.method == "dmc" else dv)
-        etrial = None
         if req.method == "dmc":
-            h.block_reset()
+            # local-energy cutoff of the weights, 0.2 sqrt(N / tau) in total
+            # energy (Umrigar, Nightingale and Runge, J. Chem. Phys. 99, 2865
+            # (1993)); per electron 0.2 / sqrt(N tau)
+            h.set_dmc_ecut(0.2 / np.sqrt(s.N * tau))
+        etrial = None
+
+        def median_el():
+            # the trial energy from the population's median E_L: one outlier
+            # in a block mean can put E_T below every walker's E_L, and then
+            # every weight exp(-tau N (E_L - E_T)) underflows to zero
+            return float(np.median(h.population_get()["p"][:, 0]))
+
+        if req.method == "dmc":
             h.vmc(req.block_steps, dv, 50)
             moves += req.block_steps * req.walkers
-            blk, norm = h.block_get()
-            etrial = blk[0] / norm
+            etrial = median_el()
         st = q.Stats(s)
         status, mean, err, nb = "max_blocks", float("nan"), float("nan"), 0
         for _ in range(req.max_blocks):
@@ -164,6 +174,9 @@ def run_request(p, device=0):
                 h.vmc(req.block_steps, tau, 50)
             moves += req.block_steps * req.walkers
             blk, norm = h.block_get()
+            if not (norm > 0.0 and np.isfinite(blk[0])):  # weights all underflowed: new E_T
+                etrial = median_el()
+                continue
             st.add_block(blk, norm)
             means.append(blk[0] / norm)
             m, e, _, nb = st.get()

@@ -196,6 +196,14 @@ int qmc2d_update_twist(qmc2d_handle *h, const qmc2d_system *sys);
 enum { QMC2D_PRECISION_FP64 = 0, QMC2D_PRECISION_MIXED = 1 };
 int qmc2d_set_precision(qmc2d_handle *h, int precision);
 
+/* DMC weight with a local-energy cutoff: with ecut > 0 (Ry per electron)
+ * qmc2d_dmc and qmc2d_batch_dmc clamp the E_L that enters the weight
+ * exp(-npnorm (E_L - etrial) delta) to etrial +- ecut, which keeps a rare
+ * walker with a very negative E_L (near a node or a coalescence) from taking
+ * over the population. The reference's dmc (reptation.f:898-903) has no
+ * such cutoff; ecut = 0, the default, gives its weights. */
+int qmc2d_set_dmc_ecut(qmc2d_handle *h, double ecut);
+
 /* Launch choices of the pair kernel (the proposal and pair passes of a
  * move): walker groups per CTA (1 or 2; 0 = the default, 2) and whether the
  * pair rows are staged in shared memory (stage 0: when they fit; 1: never,

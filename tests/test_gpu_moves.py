@@ -113,3 +113,26 @@ def test_reptation_moves(q, oracle_cls, n26, n26_configs):
             assert rel(pg[:, :14], paths[r][1][:, :14]) < 1e-9
     assert norm == nrep * nstp
     assert rel(blk[:14], blk_o[:14]) < 1e-9
+
+
+def test_dmc_ecut(q, n26, n26_configs):
+    """qmc2d_set_dmc_ecut: a cutoff no E_L reaches changes nothing; a small
+    one bounds every weight to exp(+-npnorm ecut delta) (capped at mmult)."""
+    nw, ngen, delta, et = 32, 4, 0.05, -0.43
+    x0 = n26_configs[:nw]
+    out = {}
+    for ecut in (0.0, 1e300, 1e-3):
+        with q.Handle(n26, capacity=nw, seed=SEED) as h:
+            h.set_dmc_ecut(ecut)
+            h.population_set(x0)
+            h.block_reset()
+            h.dmc(ngen, 1, delta, et, 5.0, 1000)
+            blk, norm = h.block_get()
+            out[ecut] = (h.population_get()["x"], blk, norm)
+    assert np.array_equal(out[1e300][0], out[0.0][0]) and np.array_equal(out[1e300][1], out[0.0][1])
+    lim = np.exp(n26.s.npnorm * 1e-3 * delta)
+    per_gen = out[1e-3][2] / (nw * ngen)
+    assert 1.0 / lim <= per_gen <= lim
+    with q.Handle(n26, capacity=4, seed=1) as h:
+        with pytest.raises(q.QMCError):
+            h.set_dmc_ecut(-1.0)
