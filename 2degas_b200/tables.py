@@ -19,6 +19,10 @@ reference's `spline`, reptation.f:5223-5245, last knot zeroed):
         k-space list v_k = e^2 2 pi erfc(k/(2 alpha)) / (k L^2) over the
         half-space k vectors and v0 = -e^2 (N alpha/sqrt(pi)
         + N^2 sqrt(pi)/(alpha L^2)) (self + neutralising background).
+The k vectors are listed as the reference's krlv lists them. The
+reference's own table generators are restated too: tgen with u2_ob_cos,
+u2_reatto and eta_yk, which regenerate tables the reference wrote from the
+routine name and parameters in their trailer.
 """
 import math
 import os
@@ -45,6 +49,154 @@ def hermite_table(f, df, drt):
     return t
 
 
+# ---- the reference's table generators: tgen (reptation.f:5007-5036) with
+# its pseudopotential routines u2_ob_cos (:5037-5116), u2_reatto
+# (:6517-6563) and eta_yk (:9474-9513). Each gives f and f' on the knots
+# r_i = i drt: its analytic form below x = drt (5 nt / 6, integer division),
+# and from the first knot at or beyond x the quartic tail of obsmooth
+# (:6564-6590), which matches the form's value, slope and curvature at x and
+# reaches zero value and slope at r = nt drt; the analytic part is shifted by
+# beta0 - g(x) to join it. The expressions follow the routines term by term
+# (including u2_ob_cos's curvature at x, ddg + ddc + 2 dg dc), so that a
+# table the reference wrote is regenerated from the routine name and
+# parameters in its trailer.
+
+
+def _tail(r, x, xi, g, dg, ddg):
+    """obsmooth: the quartic tail and beta0."""
+    b0 = -0.5 * dg * xi - ddg * xi ** 2 / 12.0
+    b1, b2 = dg, 0.5 * ddg
+    b3 = -dg / xi ** 2 - 2.0 / 3.0 * ddg / xi
+    b4 = 0.5 * dg / xi ** 3 + 0.25 * ddg / xi ** 2
+    d = r - x
+    f = b0 + b1 * d + b2 * d ** 2 + b3 * d ** 3 + b4 * d ** 4
+    df = b1 + 2.0 * b2 * d + 3.0 * b3 * d ** 2 + 4.0 * b4 * d ** 3
+    return f, df, b0
+
+
+def _join(nt, drt, x, xi, g, dg, ddg, form, rmin=None):
+    """f, f' on knots 0..nt: form(r) -> (f, f') below x, the tail beyond."""
+    f, df = np.zeros(nt + 1), np.zeros(nt + 1)
+    i = 0
+    while i <= nt:
+        r = i * drt
+        if rmin is not None:
+            r = max(r, rmin)
+        if not r < x:
+            break
+        f[i], df[i] = form(r)
+        i += 1
+    r = np.arange(i, nt + 1) * drt
+    f[i:], df[i:], b0 = _tail(r, x, xi, g, dg, ddg)
+    f[:i] += b0 - g
+    return f, df
+
+
+def eta_yk(p, drt, nt):
+    """Backflow eta(r) = l (1 + s r)/(r_B + w r + r^3.5) (Kwon et al. 1998),
+    p = (l, s, r_B, w); reptation.f:9474."""
+    p1, p2, p3, p4 = p[0], p[1], abs(p[2]), p[3]
+    c = drt * (nt * 5 // 6)
+    xi = drt * nt - c
+    g = p1 * (1 + p2 * c) / (p3 + p4 * c + c ** 3.5)
+    dg = (p2 * g - (p4 + 3.5 * c ** 2.5) * g ** 2 / p1) / (1 + p2 * c)
+    ddg = -(12 * c ** 2 * g ** 2 + 2 * g * dg * (p4 + 3.5 * c ** 2.5)) / (1 + p2 * c) / p1
+
+    def form(r):
+        f = p1 * (1 + p2 * r) / (p3 + p4 * r + r ** 3.5)
+        return f, (p2 * f - (p4 + 3.5 * r ** 2.5) * f ** 2 / p1) / (1 + p2 * r)
+
+    return _join(nt, drt, c, xi, g, dg, ddg, form)
+
+
+def u2_ob_cos(p, drt, nt):
+    """u(r) = [(a r + b r^2)/(1 + c^2 r + d^2 r^2) + e] [1 + sum_k e_k
+    (1 - cos(2 k pi r / (2 nt drt)))], p = (a, b, c, d, e, e_1, ..., e_n);
+    reptation.f:5037."""
+    n = len(p) - 5
+    p1, p2, p3, p4, p5 = p[0], p[1], p[2] ** 2, p[3] ** 2, p[4]
+    x = drt * (nt * 5 // 6)
+    xi = drt * nt - x
+    pl = math.acos(-1.0) / (2.0 * drt * nt)
+
+    def mod(r, second=False):
+        c, dc, ddc = 1.0, 0.0, 0.0
+        for k in range(1, n + 1):
+            kk = 2 * k * pl
+            c += p[4 + k] * (1 - math.cos(kk * r))
+            dc += p[4 + k] * math.sin(kk * r) * kk
+            ddc += p[4 + k] * math.cos(kk * r) * kk ** 2
+        return c, dc, ddc
+
+    D = 1 + p3 * x + p4 * x ** 2
+    c, dc, ddc = mod(x)
+    g = (p1 * x + p2 * x ** 2) / D + p5
+    dg = (p1 + 2 * p2 * x) / D - (p1 * x + p2 * x ** 2) * (p3 + 2 * p4 * x) / D ** 2
+    ddg = (2 * p2 / D - 2 * (p1 + 2 * p2 * x) * (p3 + 2 * p4 * x) / D ** 2
+           - (p1 * x + p2 * x ** 2) * 2 * p4 / D ** 2
+           + 2 * (p1 * x + p2 * x ** 2) * (p3 + 2 * p4 * x) ** 2 / D ** 3)
+    ddg = ddg + ddc + 2 * dg * dc
+    dg = g * dc + c * dg
+    g = g * c
+
+    def form(r):
+        c, dc, _ = mod(r)
+        Dr = 1 + p3 * r + p4 * r ** 2
+        f = (p1 * r + p2 * r ** 2) / Dr + p5
+        df = (p1 + 2 * p2 * r) / Dr - (p1 * r + p2 * r ** 2) * (p3 + 2 * p4 * r) / Dr ** 2
+        return f * c, df * c + f * dc
+
+    return _join(nt, drt, x, xi, g, dg, ddg, form, rmin=1e-10)
+
+
+def u2_reatto(p, drt, nt):
+    """u(r) = a/r^b + c exp(-d (r - e)^2) + f exp(-g (r - h)^2),
+    p = (a, b, c, d, e, f, g, h); reptation.f:6517."""
+    x = drt * (nt * 5 // 6)
+    xi = drt * nt - x
+
+    def parts(r):
+        e1 = math.exp(-p[3] * (r - p[4]) ** 2)
+        e2 = math.exp(-p[6] * (r - p[7]) ** 2)
+        f = p[0] / r ** p[1] + p[2] * e1 + p[5] * e2
+        df = (-p[1] * p[0] / r ** (p[1] + 1.0) - 2 * p[2] * p[3] * (r - p[4]) * e1
+              - 2 * p[5] * p[6] * (r - p[7]) * e2)
+        ddf = ((p[1] + 1.0) * p[1] * p[0] / r ** (p[1] + 2.0)
+               - (2 * p[2] * p[3] - 4 * p[2] * p[3] ** 2 * (r - p[4]) ** 2) * e1
+               - (2 * p[5] * p[6] - 4 * p[5] * p[6] ** 2 * (r - p[7]) ** 2) * e2)
+        return f, df, ddf
+
+    g, dg, ddg = parts(x)
+    return _join(nt, drt, x, xi, g, dg, ddg, lambda r: parts(r)[:2], rmin=1e-10)
+
+
+GENERATORS = {"eta_yk": eta_yk, "u2_ob_cos": u2_ob_cos, "u2_reatto": u2_reatto}
+
+
+def tgen(path, routine, params, drt, nt):
+    """tgen: the table of `routine` with `params` on nt+1 knots of drt,
+    splined as `spline` does (last knot zeroed), written in t_read's
+    format with the routine name and parameters as the trailer."""
+    f, df = GENERATORS[routine](params, drt, nt)
+    rows = hermite_table(f, df, drt)
+    write_table(path, rows, drt, routine, params)
+    return rows
+
+
+def read_table_file(path):
+    """A t_read table file: (rows (nt+1, 4), drt, routine, params)."""
+    with open(path) as fh:
+        lines = [ln for ln in fh.read().splitlines() if ln.strip()]
+    nt, drt = lines[0].split()
+    nt, drt = int(nt), float(drt.replace("D", "E").replace("d", "e"))
+    rows = np.array([[float(v.replace("D", "E").replace("d", "e")) for v in ln.split()]
+                     for ln in lines[1:nt + 2]])
+    routine = lines[nt + 2].strip()
+    jp = int(lines[nt + 3].split()[0])
+    params = [float(lines[nt + 4 + k].split()[0]) for k in range(jp)]
+    return rows, drt, routine, params
+
+
 def write_table(path, rows, drt, routine, params, kspace=None):
     with open(path, "w") as fh:
         fh.write(f" {rows.shape[0] - 1}  {_f(drt)}\n")
@@ -62,19 +214,45 @@ def write_table(path, rows, drt, routine, params, kspace=None):
             fh.write(f" {_f(vk0)}\n")
 
 
-def half_space_kvectors(L, nmax2):
-    """Half-space reciprocal vectors 2 pi/L (n1, n2), |n|^2 <= nmax2, by shells."""
+def krlv(L, cut):
+    """The reference's reciprocal-lattice list for a square cell of side L
+    (krlv, reptation.f, 2D branch): half-space vectors (first nonzero index
+    positive) with |g| <= cut * 2 pi / L, in its order. Points are visited
+    with the first index fastest; each vector is inserted before the first
+    one already listed with a strictly larger norm, the norms compared in
+    floating point as the reference forms them, so that vectors of one
+    shell keep the reference's order (rounding included)."""
+    pi = math.acos(-1.0)
+    vol = L * L - 0.0 * 0.0
+    arlv = [[L * 2 * pi / vol, -0.0 * 2 * pi / vol], [-0.0 * 2 * pi / vol, L * 2 * pi / vol]]
+    n1 = math.sqrt(arlv[0][0] ** 2 + arlv[0][1] ** 2)
+    n2 = math.sqrt(arlv[1][0] ** 2 + arlv[1][1] ** 2)
+    tpiba = min(n1, n2)
+    cut1 = cut * tpiba
+    cut2 = cut1 ** 2
+    small = 1e-7
+    theta = math.acos((arlv[0][0] * arlv[1][0] + arlv[0][1] * arlv[1][1]) / (n1 * n2))
+    span = [int(abs((cut1 + small) / (n1 * math.sin(theta)))),
+            int(abs((cut1 + small) / (n2 * math.sin(theta))))]
     out = []
-    m = int(math.isqrt(nmax2)) + 1
-    for n1 in range(0, m + 1):
-        for n2 in range(-m, m + 1):
-            if n1 == 0 and n2 <= 0:
+    for i2 in range(-span[1], span[1] + 1):
+        for i1 in range(-span[0], span[0] + 1):
+            ix = (i1, i2)
+            nzero = i1 if i1 != 0 else i2
+            g = [0.0, 0.0]
+            for idim in range(2):
+                for jdim in range(2):
+                    g[jdim] = g[jdim] + ix[idim] * arlv[idim][jdim]
+            g2 = g[0] * g[0] + g[1] * g[1]
+            if g2 > cut2 or nzero <= 0:
                 continue
-            if n1 * n1 + n2 * n2 <= nmax2:
-                out.append((n1 * n1 + n2 * n2, n1, n2))
-    out.sort()
-    g = 2.0 * math.pi / L
-    return np.array([[g * a, g * b] for _, a, b in out])
+            at = len(out)
+            for j, v in enumerate(out):
+                if g2 < v[0] * v[0] + v[1] * v[1]:
+                    at = j
+                    break
+            out.insert(at, (g[0], g[1]))
+    return np.array(out)
 
 
 def closed_shells(limit=200):
@@ -121,7 +299,7 @@ def make_run(directory, runid, n_up, n_down, rs, nknots=1000, backflow=None, u3=
     alpha = alpha_L / L
     f = e2 * np.array([math.erfc(alpha * x) for x in r])
     df = -e2 * 2.0 * alpha / math.sqrt(math.pi) * np.exp(-(alpha * r) ** 2)
-    kv = half_space_kvectors(L, nmax2)
+    kv = krlv(L, math.sqrt(nmax2 + 0.5))  # |n|^2 <= nmax2, in the reference's order
     kn = np.sqrt((kv ** 2).sum(1))
     vk = e2 * 2.0 * math.pi * np.array([math.erfc(k / (2 * alpha)) for k in kn]) / (kn * L * L)
     v0 = -e2 * (N * alpha / math.sqrt(math.pi) + N * N * math.sqrt(math.pi) / (alpha * L * L))
