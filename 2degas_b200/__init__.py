@@ -72,6 +72,13 @@ class System:
     def set_twist(self, ith, jth):
         _capi.check(self.lib, self.lib.qmc2d_system_set_twist(self.ptr, ith, jth))
 
+    def rmc_estimators_setup(self, ntau, ntauskip):
+        """mstar/cmass/itc setup of the deck's records for ntau-bead paths."""
+        est = _capi.RmcEstimators()
+        _capi.check(self.lib, self.lib.qmc2d_rmc_estimators_setup(self.ptr, ntau, ntauskip,
+                                                                  ctypes.byref(est)))
+        return est
+
     def footprint(self, capacity):
         """Device bytes a Handle of this capacity allocates (no GPU needed)."""
         b = ctypes.c_uint64(0)
@@ -224,6 +231,12 @@ class Handle:
 
     def rmc(self, nstp):
         self._chk(self.lib.qmc2d_rmc(self.h, nstp))
+
+    def rmc_estimators(self, est):
+        """The path estimators of the current reptiles, averaged over them."""
+        out = np.zeros(max(est.nvalues, 1))
+        self._chk(self.lib.qmc2d_rmc_path_estimators(self.h, ctypes.byref(est), _pd(out)))
+        return out[: est.nvalues]
 
     def rmc_get_path(self, rep, ntau):
         N, np_ = self.system.N, self.system.nprops

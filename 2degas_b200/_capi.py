@@ -13,6 +13,10 @@ LIB_PATH = os.path.join(HERE, "lib", "libqmc2d.so")
 MAX_TYPES = 2
 MAX_TABLES = 16
 NAME_LEN = 64
+MAX_EST = 4
+RECORD_LEN = 256
+MAX_ADD = 4
+MAX_CMSKIP = 8
 
 # status codes (enum qmc2d_status)
 OK = 0
@@ -113,6 +117,27 @@ class System(ctypes.Structure):
         ("n_props", c_int),
         ("jrhok", c_int),
         ("ref_underflow_return", c_int),
+        ("nmstar", c_int),
+        ("ncmass", c_int),
+        ("nitc", c_int),
+        ("mstar_record", (c_char * RECORD_LEN) * MAX_EST),
+        ("cmass_record", (c_char * RECORD_LEN) * MAX_EST),
+        ("itc_record", (c_char * RECORD_LEN) * MAX_EST),
+    ]
+
+
+class RmcEstimators(ctypes.Structure):
+    _fields_ = [
+        ("ntau", c_int), ("ntauskip", c_int),
+        ("nmstar", c_int), ("mstar_type", c_int * MAX_EST), ("mstar_tau_skip", c_int * MAX_EST),
+        ("ncmass", c_int), ("cmass_type", c_int * MAX_EST), ("cmass_tau_skip", c_int * MAX_EST),
+        ("cmass_nskip", c_int), ("cmass_ntauskip", (c_int * MAX_CMSKIP) * MAX_EST),
+        ("nitc", c_int), ("itc_add", c_int * MAX_EST), ("itc_start", (c_int * MAX_ADD) * MAX_EST),
+        ("itc_count", c_int * MAX_EST), ("itc_complex", c_int * MAX_EST),
+        ("jtc_add", c_int * MAX_EST), ("jtc_start", (c_int * MAX_ADD) * MAX_EST),
+        ("jtc_complex", c_int * MAX_EST), ("itc_tau_skip", c_int * MAX_EST),
+        ("jcmass_z", c_int), ("jcmass_d", c_int), ("jmstar", c_int), ("jitc", c_int),
+        ("nvalues", c_int),
     ]
 
 
@@ -177,6 +202,8 @@ SIGNATURES = {
     "qmc2d_set_precision": (c_int, [c_void_p, c_int]),
     "qmc2d_footprint": (c_int, [SYSP, c_int, ctypes.POINTER(c_uint64)]),
     "qmc2d_set_dmc_ecut": (c_int, [c_void_p, c_double]),
+    "qmc2d_rmc_estimators_setup": (c_int, [SYSP, c_int, c_int, POINTER(RmcEstimators)]),
+    "qmc2d_rmc_path_estimators": (c_int, [c_void_p, POINTER(RmcEstimators), PD]),
     "qmc2d_set_launch": (c_int, [c_void_p, c_int, c_int]),
     "qmc2d_autotune": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), PD]),
     "qmc2d_batch_create": (c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p)]),

@@ -255,6 +255,19 @@ extern "C" int qmc2d_system_read(const char *dir_c, const char *runid_c, qmc2d_s
       }
     } else if (k == "ntwists") {
       if (need(2)) fint(w[1], &s->ntheta);
+    } else if (k == "mstar" || k == "cmass" || k == "itc") {
+      // path-estimator records, set up when reptation starts
+      int *n = k == "mstar" ? &s->nmstar : k == "cmass" ? &s->ncmass : &s->nitc;
+      char(*rec)[QMC2D_RECORD_LEN] =
+          k == "mstar" ? s->mstar_record : k == "cmass" ? s->cmass_record : s->itc_record;
+      if (*n >= QMC2D_MAX_EST) {
+        st = fail(QMC2D_ERR_LIMIT, "too many '" + k + "' records");
+      } else {
+        std::string r;
+        for (size_t i = 1; i < w.size(); i++) r += (i > 1 ? " " : "") + w[i];
+        if (r.size() >= QMC2D_RECORD_LEN) st = fail(QMC2D_ERR_LIMIT, "'" + k + "' record too long");
+        else std::snprintf(rec[(*n)++], QMC2D_RECORD_LEN, "%s", r.c_str());
+      }
     } else {
       st = fail(QMC2D_ERR_UNSUPPORTED, "keyword outside the walker path: " + k);
     }

@@ -419,10 +419,137 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
   }
 }
 
+// The path estimators of path_props (reptation.f:1578-1737) of reptile r's
+// current path into rows[r * e.nvalues ..]: one CTA per reptile; every
+// output bin is summed by one thread in the reference's order (bead itau
+// ascending, then particles, then dimensions), so the result does not
+// depend on the thread count. cm: ncmass * ntau * 2 doubles of shared
+// memory, the centre of mass of each record's type in every bead (the
+// cmass_p properties of compute_properties, reptation.f:2696-2707).
+__global__ void __launch_bounds__(kThreads) rmc_estimators_kernel(const DevSys *sp, RmcArgs a,
+                                                                  qmc2d_rmc_estimators e,
+                                                                  double *rows) {
+  __shared__ DevSys S;
+  extern __shared__ double cm[];
+  load_sys(S, sp);
+  const int r = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
+  if (r >= a.nrep) return;
+  const int kfirst = a.ends[2 * r], ntau = a.ntau, nb = ntau - 2 * a.ntauskip;
+  double *row = rows + (size_t)r * e.nvalues;
+  auto xb = [&](int itau) { return bead(S, a, r, (kfirst + itau - 1) % a.nbuf).x; };
+  auto pb = [&](int itau) { return bead(S, a, r, (kfirst + itau - 1) % a.nbuf).p; };
+  const double pi = 3.141592653589793;
+  for (int item = tid; item < e.ncmass * ntau * 2; item += nth) {
+    const int c = item / (ntau * 2), itau = (item % (ntau * 2)) / 2 + 1, d = item & 1;
+    const int t = e.cmass_type[c];
+    const double *x = xb(itau);
+    double sum = 0.0;
+    for (int ip = S.ipfrst[t]; ip < S.ipfrst[t] + S.np[t]; ip++) sum += x[2 * ip + d];
+    cm[item] = sum / S.np[t];
+  }
+  __syncthreads();
+  // cmass z: the middle bead (itau = ntau/2 + 1)
+  for (int item = tid; item < e.ncmass * 2; item += nth) {
+    const int c = item / 2, d = item & 1, t = e.cmass_type[c];
+    const double v = cm[(c * ntau + ntau / 2) * 2 + d] * (2.0 * pi * S.eli[d]) * S.np[t];
+    row[e.jcmass_z + 4 * c + 2 * d] = cos(v);
+    row[e.jcmass_z + 4 * c + 2 * d + 1] = sin(v);
+  }
+  // cmass diffusion
+  int off = e.jcmass_d;
+  for (int c = 0; c < e.ncmass; c++)
+    for (int k = 0; k < e.cmass_nskip; k++) {
+      const int skip = e.cmass_ntauskip[c][k], ts = e.cmass_tau_skip[c];
+      const int nij = (ntau - 2 * skip) / ts;
+      for (int ij = tid; ij < nij; ij += nth) {
+        double re = 0.0, nrm = 0.0;
+        for (int itau = 1 + skip; itau + ij * ts <= ntau - skip; itau++) {
+          const int jtau = itau + ij * ts;
+          for (int d = 0; d < 2; d++) {
+            const double df = cm[(c * ntau + itau - 1) * 2 + d] - cm[(c * ntau + jtau - 1) * 2 + d];
+            re += df * df;
+          }
+          nrm += 1.0;
+        }
+        row[off + ij] = re / nrm;
+      }
+      off += nij;
+    }
+  // mstar
+  off = e.jmstar;
+  for (int i = 0; i < e.nmstar; i++) {
+    const int t = e.mstar_type[i], ts = e.mstar_tau_skip[i], nij = nb / ts;
+    for (int ij = tid; ij < nij; ij += nth) {
+      double re = 0.0, nrm = 0.0;
+      for (int itau = 1 + a.ntauskip; itau + ij * ts <= ntau - a.ntauskip; itau++) {
+        const double *xi = xb(itau), *xj = xb(itau + ij * ts);
+        for (int ip = S.ipfrst[t]; ip < S.ipfrst[t] + S.np[t]; ip++) {
+          for (int d = 0; d < 2; d++) {
+            const double df = xi[2 * ip + d] - xj[2 * ip + d];
+            re += df * df;
+          }
+          nrm += 1.0;
+        }
+      }
+      row[off + ij] = re / nrm;
+    }
+    off += nij;
+  }
+  // itc
+  off = e.jitc;
+  for (int i = 0; i < e.nitc; i++) {
+    const int ts = e.itc_tau_skip[i], nij = nb / ts, cplx = e.itc_complex[i] != 0;
+    const int nc = cplx ? e.itc_count[i] / 2 : e.itc_count[i];
+    for (int item = tid; item < nc * nij; item += nth) {
+      const int q = item / nij, ij = item - q * nij;
+      const int ic = cplx ? 2 * q : q;  // 0-based icount
+      double re = 0.0, im = 0.0, nrm = 0.0;
+      for (int itau = 1 + a.ntauskip; itau + ij * ts <= ntau - a.ntauskip; itau++) {
+        const double *p1 = pb(itau), *p2 = pb(itau + ij * ts);
+        double ri = 0.0, ii = 0.0, rj = 0.0, ij2 = 0.0;
+        for (int s2 = 0; s2 < e.itc_add[i]; s2++) {
+          ri += p1[e.itc_start[i][s2] + ic];
+          if (cplx) ii += p1[e.itc_start[i][s2] + ic + 1];
+        }
+        for (int s2 = 0; s2 < e.jtc_add[i]; s2++) {
+          rj += p2[e.jtc_start[i][s2] + ic];
+          if (cplx) ij2 += p2[e.jtc_start[i][s2] + ic + 1];
+        }
+        if (cplx) {
+          ii *= e.itc_complex[i];
+          ij2 *= e.jtc_complex[i];
+          re += ri * rj - ii * ij2;
+          im += ri * ij2 + ii * rj;
+        } else {
+          re += ri * rj;
+        }
+        nrm += 1.0;
+      }
+      if (cplx) {
+        row[off + 2 * q * nij + ij] = re / nrm;
+        row[off + 2 * q * nij + nij + ij] = im / nrm;
+      } else {
+        row[off + q * nij + ij] = re / nrm;
+      }
+    }
+    off += nij * e.itc_count[i];
+  }
+}
+
+// out[v] = the mean over reptiles of rows[r * nv + v], summed in reptile order.
+__global__ void rmc_estimators_mean_kernel(const double *rows, int nrep, int nv, double *out) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  double s = 0.0;
+  for (int r = 0; r < nrep; r++) s += rows[(size_t)r * nv + v];
+  out[v] = s / nrep;
+}
+
 }  // namespace
 
 void rmc_free(RmcState *r) {
-  void *b[] = {r->x, r->g, r->p, r->h, r->s, r->age_stack, r->w, r->ends, r->pp_old, r->age};
+  void *b[] = {r->x, r->g, r->p, r->h, r->s, r->age_stack, r->w, r->ends, r->pp_old, r->age,
+               r->est};
   for (void *p : b) cudaFree(p);
   *r = RmcState{};
 }
@@ -579,5 +706,44 @@ extern "C" int qmc2d_rmc_get_path(qmc2d_handle *h, int rep, double *x, double *p
     if (props)
       RCK(cudaMemcpy(props + i * np, r.p + b * np, sizeof(double) * np, cudaMemcpyDeviceToHost));
   }
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_rmc_path_estimators(qmc2d_handle *h, const qmc2d_rmc_estimators *est,
+                                         double *out) {
+  if (!h || !est || !out || est->nvalues < 0) return QMC2D_ERR_ARG;
+  q2d::RmcState &r = h->rmc;
+  if (r.nrep <= 0) {
+    q2d::set_error("qmc2d_rmc_path_estimators: no reptiles (call qmc2d_rmc_init)");
+    return QMC2D_ERR_STACK;
+  }
+  if (est->ntau != r.ntau || est->ntauskip != r.ntauskip || est->ncmass > QMC2D_MAX_EST ||
+      est->nmstar > QMC2D_MAX_EST || est->nitc > QMC2D_MAX_EST) {
+    q2d::set_error("qmc2d_rmc_path_estimators: set up for another path length");
+    return QMC2D_ERR_ARG;
+  }
+  if (est->nvalues == 0) return QMC2D_OK;
+  RCK(cudaSetDevice(h->device));
+  const size_t need = ((size_t)r.nrep + 1) * est->nvalues;
+  if (need > r.est_cap) {
+    RCK(cudaStreamSynchronize(h->stream));
+    cudaFree(r.est);
+    r.est = nullptr;
+    r.est_cap = 0;
+    RCK(cudaMalloc(&r.est, sizeof(double) * need));
+    r.est_cap = need;
+  }
+  q2d::RmcArgs a = rmc_args(h, 0);
+  const size_t sm = sizeof(double) * 2 * (size_t)r.ntau * est->ncmass;
+  RCK(q2d::raise_smem_limit((const void *)q2d::rmc_estimators_kernel, sm));
+  q2d::rmc_estimators_kernel<<<r.nrep, q2d::kThreads, sm, h->stream>>>(h->ds, a, *est, r.est);
+  RCK(cudaGetLastError());
+  double *mean = r.est + (size_t)r.nrep * est->nvalues;
+  q2d::rmc_estimators_mean_kernel<<<(est->nvalues + 255) / 256, 256, 0, h->stream>>>(
+      r.est, r.nrep, est->nvalues, mean);
+  RCK(cudaGetLastError());
+  RCK(cudaMemcpyAsync(out, mean, sizeof(double) * est->nvalues, cudaMemcpyDeviceToHost,
+                      h->stream));
+  RCK(cudaStreamSynchronize(h->stream));
   return QMC2D_OK;
 }

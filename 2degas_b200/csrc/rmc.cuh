@@ -22,6 +22,8 @@ struct RmcState {
   double *pp_old = nullptr;   // nrep * nprops
   double *age = nullptr;      // nrep
   uint32_t step = 0;
+  double *est = nullptr;  // path estimators: nrep rows and their mean (qmc2d_rmc_estimators)
+  size_t est_cap = 0;
 };
 
 void rmc_free(RmcState *r);

@@ -60,6 +60,8 @@ enum qmc2d_status {
 #define QMC2D_MAX_ORB 81          /* orbitals (electrons) per spin determinant */
 #define QMC2D_MAX_NK 512          /* half-space k vectors */
 #define QMC2D_NAME_LEN 64
+#define QMC2D_MAX_EST 4           /* path-estimator records of each kind */
+#define QMC2D_RECORD_LEN 256
 
 /* ------------------------------------------------------- property layout
  * Scalar properties, reference names and 1-based indices from
@@ -133,6 +135,12 @@ typedef struct qmc2d_system {
   int jrhok;                               /* first rhok index (0-based) */
   int ref_underflow_return;                /* 1: keep the reference's early return when
                                               exp(-2*(-ln psi)) underflows (reptation.f:10087) */
+  /* 'mstar', 'cmass' and 'itc' records of the deck (the words after the
+   * keyword, reptation.f:210-224), for qmc2d_rmc_estimators_setup */
+  int nmstar, ncmass, nitc;
+  char mstar_record[QMC2D_MAX_EST][QMC2D_RECORD_LEN];
+  char cmass_record[QMC2D_MAX_EST][QMC2D_RECORD_LEN];
+  char itc_record[QMC2D_MAX_EST][QMC2D_RECORD_LEN];
 } qmc2d_system;
 
 /* Read <dir>/<runid>.sy and every table it names (input, t_read, kread:
@@ -392,6 +400,51 @@ int qmc2d_rmc_get_path(qmc2d_handle *h, int r, double *x, double *props);
 int qmc2d_restart_read_rmc(qmc2d_handle *h, const qmc2d_system *sys, qmc2d_stats *st,
                            const qmc2d_rmc_params *prm, const char *dir, const char *runid,
                            int rank, int *iblk);
+
+/* ------------------------------------------------ reptation path estimators
+ * The imaginary-time estimators of path_props (reptation.f:1578-1737):
+ * - mstar: per type, the mean over particles and bead pairs of
+ *   |x(itau) - x(jtau)|^2 against the lag jtau - itau (in steps of the
+ *   record's tau skip), beads ntauskip+1 .. ntau-ntauskip;
+ * - cmass: per type, cos and sin of 2 pi np x_cm / L of the middle bead's
+ *   centre of mass (z), and the mean of |x_cm(itau) - x_cm(jtau)|^2
+ *   against the lag for each of the record's bead skips (diffusion);
+ * - itc: imaginary-time correlations sum_i a(itau) b(jtau) of stored bead
+ *   properties a, b (each a sum of named properties; complex pairs of
+ *   rhok entries when flagged 'complex', conjugated for 'conjg').
+ * The reference sets them up from the deck's records when rmc starts
+ * (cmass_setup, mstar_setup, itc_setup; reptation.f:1378-1553) and appends
+ * them to the path properties in that order: cmass z, cmass diffusion,
+ * mstar, itc. Here they form their own vector in the same order. */
+#define QMC2D_MAX_ADD 4           /* properties summed in one itc factor */
+#define QMC2D_MAX_CMSKIP 8        /* bead skips of one cmass record */
+typedef struct qmc2d_rmc_estimators {
+  int ntau, ntauskip;
+  int nmstar;
+  int mstar_type[QMC2D_MAX_EST], mstar_tau_skip[QMC2D_MAX_EST];
+  int ncmass;
+  int cmass_type[QMC2D_MAX_EST], cmass_tau_skip[QMC2D_MAX_EST];
+  int cmass_nskip;                                   /* bead skips (one count for all records) */
+  int cmass_ntauskip[QMC2D_MAX_EST][QMC2D_MAX_CMSKIP];
+  int nitc;
+  int itc_add[QMC2D_MAX_EST], itc_start[QMC2D_MAX_EST][QMC2D_MAX_ADD];
+  int itc_count[QMC2D_MAX_EST], itc_complex[QMC2D_MAX_EST];  /* 0, 1 complex, -1 conjg */
+  int jtc_add[QMC2D_MAX_EST], jtc_start[QMC2D_MAX_EST][QMC2D_MAX_ADD];
+  int jtc_complex[QMC2D_MAX_EST], itc_tau_skip[QMC2D_MAX_EST];
+  int jcmass_z, jcmass_d, jmstar, jitc, nvalues;     /* offsets in the estimator vector */
+} qmc2d_rmc_estimators;
+/* mstar_setup, cmass_setup and itc_setup on the system's records for paths
+ * of ntau beads with ntauskip skipped at each end (itc names: the scalar
+ * properties and rhok_<type>). */
+int qmc2d_rmc_estimators_setup(const qmc2d_system *sys, int ntau, int ntauskip,
+                               qmc2d_rmc_estimators *est);
+/* The estimators of every reptile's current path (after qmc2d_rmc_init or
+ * qmc2d_rmc), averaged over the reptiles, into out[est->nvalues]. The
+ * reference evaluates them in path_props on each proposed path and
+ * accumulates the accepted path's values once per step; calling this once
+ * per step after qmc2d_rmc(h, 1) gives the same per-step values (the
+ * reference refreshes the itc entries only every 100th path_props call). */
+int qmc2d_rmc_path_estimators(qmc2d_handle *h, const qmc2d_rmc_estimators *est, double *out);
 
 /* ----------------------------------------------------- streams and timing
  * The reference has no timers; these expose device time per kernel. */
