@@ -310,11 +310,14 @@ class Handle:
 class Stats:
     """Cumulative block statistics of averages(3) (qmc2d_stats_*)."""
 
-    def __init__(self, system):
+    def __init__(self, system, n=None):
+        """Statistics of the system's n_props properties, or of n values
+        (e.g. the reptation path estimators, n = est.nvalues)."""
         self.system = system
         self.lib = system.lib
+        self.n = system.nprops if n is None else n
         self.p = ctypes.c_void_p()
-        _capi.check(self.lib, self.lib.qmc2d_stats_create(system.nprops, ctypes.byref(self.p)))
+        _capi.check(self.lib, self.lib.qmc2d_stats_create(self.n, ctypes.byref(self.p)))
 
     def __del__(self):
         try:
@@ -330,12 +333,19 @@ class Stats:
 
     def get(self):
         """(cumulative means, errors, cml_norm, blocks)."""
-        n = self.system.nprops
+        n = self.n
         mean, err = np.zeros(n), np.zeros(n)
         norm, ib = ctypes.c_double(), ctypes.c_int()
         _capi.check(self.lib, self.lib.qmc2d_stats_get(self.p, _pd(mean), _pd(err),
                                                        ctypes.byref(norm), ctypes.byref(ib)))
         return mean, err, norm.value, ib.value
+
+    def write_estimators(self, est, blk, norm, directory, runid):
+        """The reptation estimator files of averages(3) for this block."""
+        blk = np.ascontiguousarray(blk, dtype=np.float64)
+        _capi.check(self.lib, self.lib.qmc2d_stats_write_estimators(
+            self.p, self.system.ptr, ctypes.byref(est), _pd(blk), norm,
+            str(directory).encode(), runid.encode()))
 
     def report(self, blk, norm, who):
         """The averages(3) block report text."""

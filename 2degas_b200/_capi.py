@@ -211,6 +211,8 @@ SIGNATURES = {
     "qmc2d_batch_vmc": (c_int, [c_void_p, c_int, PD, c_int]),
     "qmc2d_batch_dmc": (c_int, [c_void_p, c_int, PD, PD, c_double, c_int]),
     "qmc2d_stats_create": (c_int, [c_int, POINTER(c_void_p)]),
+    "qmc2d_stats_write_estimators": (c_int, [c_void_p, SYSP, POINTER(RmcEstimators), PD, c_double,
+                                             ctypes.c_char_p, ctypes.c_char_p]),
     "qmc2d_stats_destroy": (c_int, [c_void_p]),
     "qmc2d_stats_add_block": (c_int, [c_void_p, PD, c_double]),
     "qmc2d_stats_get": (c_int, [c_void_p, PD, PD, PD, POINTER(c_int)]),

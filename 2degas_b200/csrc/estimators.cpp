@@ -72,6 +72,26 @@ int complex_flag(const std::string &s) {
 
 }  // namespace
 
+// The file name itc_setup builds for itc record i: runid, then the first
+// factor's names joined by '.', '+', then the second's by '_', '+'
+// (reptation.f:1474-1530); empty if the record does not parse.
+std::string q2d_itc_filename(const qmc2d_system *sys, int i, const std::string &runid) {
+  const auto names = prop_names(sys);
+  auto w = words(sys->itc_record[i]);
+  std::string f = runid;
+  size_t iw = 0;
+  for (int sidx = 0; sidx < 2; sidx++) {
+    int add = 0;
+    if (iw >= w.size() || !to_int(w[iw++], &add)) return "";
+    for (int j = 0; j < add; j++) {
+      if (iw >= w.size() || names.find(w[iw]) == names.end()) return "";
+      f += (j == 0 ? (sidx == 0 ? "." : "_") : "+") + w[iw++];
+    }
+    if (iw < w.size() && complex_flag(w[iw]) != 0) iw++;
+  }
+  return f;
+}
+
 extern "C" int qmc2d_rmc_estimators_setup(const qmc2d_system *sys, int ntau, int ntauskip,
                                           qmc2d_rmc_estimators *est) {
   if (!sys || !est || ntau < 2 || ntauskip < 0 || ntau - 2 * ntauskip < 1)

@@ -197,6 +197,61 @@ extern "C" int qmc2d_stats_write_rhok(const qmc2d_stats *st, const qmc2d_system 
   return QMC2D_OK;
 }
 
+std::string q2d_itc_filename(const qmc2d_system *sys, int i, const std::string &runid);
+
+extern "C" int qmc2d_stats_write_estimators(const qmc2d_stats *st, const qmc2d_system *sys,
+                                           const qmc2d_rmc_estimators *est, const double *blk,
+                                           double blk_norm, const char *dir, const char *runid) {
+  if (!st || !sys || !est || !blk || !runid || st->n_props != est->nvalues || !(blk_norm > 0.0))
+    return fail(QMC2D_ERR_ARG, "qmc2d_stats_write_estimators: bad argument");
+  const std::string d = dir ? dir : "", rid = runid;
+  // write_nonscalar_props: n lines from index i of the estimator vector
+  auto put = [&](const std::string &name, int i, int n, const char *mode) {
+    const std::string path = join(d, name);
+    std::FILE *f = std::fopen(path.c_str(), mode);
+    if (!f) return fail(QMC2D_ERR_IO, "cannot write " + path);
+    for (int j = 1; j <= n; j++, i++)
+      std::fprintf(f, "%s%s%s%s %s%s\n", fe(blk[i] / blk_norm, 19, 11).c_str(),
+                   fe(st->cml_av[i] / st->cml_norm, 19, 11).c_str(),
+                   fe(err_of(st, i), 9, 2).c_str(), fe(blk_norm, 10, 3).c_str(),
+                   fa(" merea ", 7).c_str(), fi(j, 5).c_str());
+    if (std::fclose(f) != 0) return fail(QMC2D_ERR_IO, "cannot write " + path);
+    return (int)QMC2D_OK;
+  };
+  const int nb = est->ntau - 2 * est->ntauskip;
+  int st2;
+  int i = est->jmstar;
+  for (int j = 0; j < est->nmstar; j++) {
+    const int n = nb / est->mstar_tau_skip[j];
+    if ((st2 = put(rid + ".mstar_" + sys->type_name[est->mstar_type[j]], i, n, "w"))) return st2;
+    i += n;
+  }
+  // z_cmass: the reference leaves the unit open, so each block's lines follow
+  // the previous block's (the first block starts the file)
+  i = est->jcmass_z;
+  for (int j = 0; j < est->ncmass; j++, i += 4)
+    if ((st2 = put(rid + ".z_cmass_" + sys->type_name[est->cmass_type[j]], i, 4,
+                   st->iblk <= 1 ? "w" : "a")))
+      return st2;
+  i = est->jcmass_d;
+  for (int j = 0; j < est->ncmass; j++) {
+    int n = 0;
+    for (int k = 0; k < est->cmass_nskip; k++)
+      n += (est->ntau - 2 * est->cmass_ntauskip[j][k]) / est->cmass_tau_skip[j];
+    if ((st2 = put(rid + ".cmass_" + sys->type_name[est->cmass_type[j]], i, n, "w"))) return st2;
+    i += n;
+  }
+  i = est->jitc;
+  for (int j = 0; j < est->nitc; j++) {
+    const int n = (nb / est->itc_tau_skip[j]) * est->itc_count[j];
+    const std::string name = q2d_itc_filename(sys, j, rid);
+    if (name.empty()) return fail(QMC2D_ERR_PARSE, "qmc2d_stats_write_estimators: itc record");
+    if ((st2 = put(name, i, n, "w"))) return st2;
+    i += n;
+  }
+  return QMC2D_OK;
+}
+
 extern "C" int qmc2d_write_conf(qmc2d_handle *h, const qmc2d_system *sys, const char *dir,
                                 int rank) {
   if (!h || !sys || sys->nptot != h->N) return fail(QMC2D_ERR_ARG, "qmc2d_write_conf: bad argument");

@@ -445,6 +445,15 @@ int qmc2d_rmc_estimators_setup(const qmc2d_system *sys, int ntau, int ntauskip,
  * per step after qmc2d_rmc(h, 1) gives the same per-step values (the
  * reference refreshes the itc entries only every 100th path_props call). */
 int qmc2d_rmc_path_estimators(qmc2d_handle *h, const qmc2d_rmc_estimators *est, double *out);
+/* The estimator files of averages(3) (reptation.f:4377-4428, each in the
+ * format of write_nonscalar_props, :4582-4616) from a qmc2d_stats over the
+ * estimator vector (n_props = est->nvalues) and the block just added:
+ * <runid>.mstar_<type>, <runid>.cmass_<type> and the itc files (named as
+ * itc_setup names them) rewritten each block, <runid>.z_cmass_<type> with
+ * every block's lines after the previous ones. */
+int qmc2d_stats_write_estimators(const qmc2d_stats *st, const qmc2d_system *sys,
+                                 const qmc2d_rmc_estimators *est, const double *blk,
+                                 double blk_norm, const char *dir, const char *runid);
 
 /* ----------------------------------------------------- streams and timing
  * The reference has no timers; these expose device time per kernel. */

@@ -2,6 +2,8 @@
 and 'itc' records (mstar_setup, cmass_setup, itc_setup;
 reptation.f:1378-1553): fields, the estimator vector's layout, and the
 records that are rejected. Host only."""
+import os
+
 import pytest
 
 from variants import write_variant
@@ -44,3 +46,33 @@ def test_bad_records(q, tmp_path, rec):
     s = q.System.read(write_variant(tmp_path, "bad", extra=(rec,)), "bad")
     with pytest.raises(q.QMCError):
         s.rmc_estimators_setup(20, 2)
+
+
+def test_estimator_files(q, tmp_path):
+    """averages(3)'s estimator files: names, one line per value in
+    write_nonscalar_props' format, z_cmass lines following block by block."""
+    import numpy as np
+
+    s = q.System.read(write_variant(tmp_path, "est", extra=RECORDS), "est")
+    e = s.rmc_estimators_setup(20, 2)
+    st = q.Stats(s, e.nvalues)
+    rng = np.random.default_rng(1)
+    out = tmp_path / "out"
+    out.mkdir()
+    for b in range(2):
+        blk = rng.normal(size=e.nvalues) * 30.0
+        st.add_block(blk, 30.0)
+        st.write_estimators(e, blk, 30.0, out, "run")
+    names = sorted(os.listdir(out))
+    assert names == sorted(["run.mstar_up", "run.mstar_down", "run.z_cmass_up",
+                            "run.cmass_up", "run.rhok_up_rhok_up", "run.elocal+epot_ekin"])
+    lines = lambda n: open(out / n).read().splitlines()  # noqa: E731
+    assert len(lines("run.mstar_up")) == 16 and len(lines("run.mstar_down")) == 8
+    assert len(lines("run.cmass_up")) == 9 + 7
+    assert len(lines("run.z_cmass_up")) == 2 * 4  # two blocks
+    assert len(lines("run.rhok_up_rhok_up")) == 8 * 2 * s.s.nk
+    assert len(lines("run.elocal+epot_ekin")) == 16
+    ln = lines("run.mstar_up")[3]
+    assert len(ln) == 19 + 19 + 9 + 10 + 1 + 7 + 5 and ln[58:65] == " merea " and int(ln[65:]) == 4
+    mean, _, _, _ = st.get()
+    assert abs(float(ln[19:38]) - mean[e.jmstar + 3]) <= 1e-10 * abs(mean[e.jmstar + 3])
