@@ -216,6 +216,13 @@ size_t handle_bytes(const qmc2d_system *sys, const q2d::DevSys &hs, size_t ncoef
   b += al(c, 8) * 2 + al(c, 4) * 4 + al(1, 4);                           // branch scratch
   b += al(c * 2 * N, 8) * 2 + al(c * nt, 8) + al(c * np, 8) + al(c, 8);  // staging
   b += al(c * q2d::move_scratch_doubles(hs), 8) + al(np + 1, 8);
+  // determinants beyond shared memory (the B200's 227 KB opt-in per CTA)
+  const size_t smem = std::max(q2d::move_smem_bytes(hs), q2d::eval_smem_bytes(hs));
+  if (hs.gmat || (hs.has_bf && smem + sizeof(q2d::DevSys) > 232448)) {
+    q2d::DevSys g = hs;
+    g.gmat = 1;
+    b += al(c * q2d::gmat_doubles(g), 8);
+  }
   return b;
 }
 
@@ -264,6 +271,11 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
   int smem_max = 0;
   cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   size_t need = std::max(q2d::move_smem_bytes(h->hs), q2d::eval_smem_bytes(h->hs));
+  if (need + sizeof(q2d::DevSys) > (size_t)smem_max && h->hs.has_bf) {
+    // the determinant matrices go to a per-walker block of global memory
+    h->hs.gmat = 1;
+    need = std::max(q2d::move_smem_bytes(h->hs), q2d::eval_smem_bytes(h->hs));
+  }
   if (need + sizeof(q2d::DevSys) > (size_t)smem_max) {
     char buf[160];
     std::snprintf(buf, sizeof buf, "walker needs %zu bytes of shared memory, device has %d",
@@ -288,6 +300,12 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
   h->hs.kvec = h->d_kvec;
   h->hs.gvec = h->d_gvec;
   h->gvec_cap = std::max(1, sys->ngvec);
+  if (h->hs.gmat) {
+    h->hs.gmat_stride = (long long)q2d::gmat_doubles(h->hs);
+    if ((e = dalloc(&h->d_gmat, (size_t)h->cap * h->hs.gmat_stride)) != cudaSuccess)
+      return fail(cuda_fail(e, "cudaMalloc"));
+    h->hs.gmat_base = h->d_gmat;
+  }
   if ((e = dalloc(&h->ds, 1)) != cudaSuccess) return fail(cuda_fail(e, "alloc"));
   cudaMemcpy(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice);
   int cap = h->cap, N = h->N, nt = h->nt, np = h->nprops;
@@ -430,7 +448,7 @@ extern "C" int qmc2d_destroy(qmc2d_handle *h) {
   void *bufs[] = {h->ds, h->d_coef, h->d_kvec, h->d_gvec, h->d_blk, h->d_norm, h->d_cnt,
                   h->d_wate, h->d_status, h->br.delt, h->br.csum, h->br.mult, h->br.src,
                   h->br.ecum, h->br.zrank, h->br.ncapped, h->d_x, h->d_g, h->d_h, h->d_p,
-                  h->d_s, h->d_mscr, h->d_blksum, h->hs.phase};
+                  h->d_s, h->d_mscr, h->d_blksum, h->hs.phase, h->d_gmat};
   for (void *b : bufs) cudaFree(b);
   for (int k = 0; k < QMC2D_NKERNELS; k++)
     for (cudaEvent_t e : h->ev[k]) cudaEventDestroy(e);

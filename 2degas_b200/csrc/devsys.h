@@ -53,6 +53,13 @@ struct DevSys {
   // groups per CTA (0: the default, 2) and the staging of the pair rows in
   // shared memory (0: when they fit, 1: never).
   int tune_groups, tune_stage;
+  // Determinants too large for one CTA's shared memory (gmat = 1): the
+  // orbital, inversion, F and cross-term matrices of walker (CTA) b live at
+  // gmat_base + b * gmat_stride (doubles) in global memory; everything
+  // else stays in shared memory.
+  int gmat;
+  long long gmat_stride;
+  double *gmat_base;
   const double *coef;  // packed tables: ut rows (4 doubles each) and v_k lists
   const double *kvec;  // 2*nk
   const double *gvec;  // 2*ngvec
@@ -79,5 +86,9 @@ void pack_pair_rows(const qmc2d_system *sys, DevSys *s, std::vector<double> *row
 size_t eval_smem_bytes(const DevSys &s);
 // Extra shared memory a move kernel adds for the walker's own state.
 size_t move_smem_bytes(const DevSys &s);
+// Doubles of global memory per walker for the determinant matrices when
+// s.gmat is set (a multiple of 32, so that every block is 256-byte aligned);
+// 0 otherwise.
+size_t gmat_doubles(const DevSys &s);
 
 }  // namespace q2d

@@ -23,6 +23,7 @@ struct qmc2d_handle {
   int *d_status = nullptr;
   double *d_mscr = nullptr;  // move scratch: cap * move_scratch_doubles(hs)
   double *d_blksum = nullptr;  // n_props + 1: block sums over the population
+  double *d_gmat = nullptr;    // cap * hs.gmat_stride: determinant matrices (hs.gmat)
   q2d::BranchScratch br{};
   // staging for the batched evaluation entry point
   double *d_x = nullptr, *d_g = nullptr, *d_h = nullptr, *d_p = nullptr, *d_s = nullptr;

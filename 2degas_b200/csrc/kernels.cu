@@ -53,7 +53,7 @@ __device__ __forceinline__ void load_sys(DevSys &S, const DevSys *sp) {
 }
 
 // ---------------------------------------------------------------- eval
-template <class R>
+template <class R, bool kGmat>
 __global__ void __launch_bounds__(kThreads, 2) eval_kernel(const DevSys *sp, int nw,
                                                         const double *__restrict__ x, double *g,
                                                         double *hl, double *props, double *s,
@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(kThreads, 2) eval_kernel(const DevSys *sp, int
   extern __shared__ __align__(16) char smem[];
   load_sys(S, sp);
   EvalSmem m;
-  size_t off = eval_carve(S, smem, &m);
+  size_t off = eval_carve<kGmat>(S, smem, &m, kGmat ? gmat_block(S, blockIdx.x) : nullptr);
   double *pn = reinterpret_cast<double *>(smem + off);
   double *hn = pn + S.nprops;
   double *sn = hn + 2;
@@ -85,6 +85,13 @@ __global__ void __launch_bounds__(kThreads, 2) eval_kernel(const DevSys *sp, int
 
 size_t eval_smem_bytes(const DevSys &s) {
   return eval_carve(s, nullptr, nullptr) + align16(sizeof(double) * (s.nprops + 3));
+}
+
+size_t gmat_doubles(const DevSys &s) {
+  if (!s.gmat) return 0;
+  size_t g = 0;
+  eval_carve(s, nullptr, nullptr, nullptr, &g);
+  return ((g + 7) / 8 + 31) & ~size_t(31);
 }
 
 // ------------------------------------------------------------- the move
@@ -208,13 +215,14 @@ __global__ void __launch_bounds__(G * kThreads, 2 / G) pairs_kernel(const DevSys
 
 size_t move_scratch_doubles(const DevSys &hs) { return move_scratch(hs).stride; }
 
+template <bool kGmat>
 __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, DevPop pop,
                                                            MoveArgs a) {
   __shared__ DevSys S;
   extern __shared__ __align__(16) char smem[];
   load_sys(S, sp);
   EvalSmem m;
-  size_t off = eval_carve(S, smem, &m);
+  size_t off = eval_carve<kGmat>(S, smem, &m, kGmat ? gmat_block(S, blockIdx.x) : nullptr);
   MoveSmem v;
   move_carve(S, smem + off, &v);
   const int w = blockIdx.x, tid = threadIdx.x;
@@ -565,14 +573,11 @@ cudaError_t launch_eval(const DevSys &hs, const DevSys *ds, int nw, const double
                         double *hl, double *props, double *s, int *status, cudaStream_t st) {
   if (nw <= 0) return cudaSuccess;
   size_t sm = eval_smem_bytes(hs);
-  const void *k =
-      hs.pair_f32 ? (const void *)eval_kernel<float> : (const void *)eval_kernel<double>;
-  cudaError_t e = set_smem(k, sm);
+  auto k = hs.gmat ? (hs.pair_f32 ? eval_kernel<float, true> : eval_kernel<double, true>)
+                   : (hs.pair_f32 ? eval_kernel<float, false> : eval_kernel<double, false>);
+  cudaError_t e = set_smem((const void *)k, sm);
   if (e != cudaSuccess) return e;
-  if (hs.pair_f32)
-    eval_kernel<float><<<nw, kThreads, sm, st>>>(ds, nw, x, g, hl, props, s, status);
-  else
-    eval_kernel<double><<<nw, kThreads, sm, st>>>(ds, nw, x, g, hl, props, s, status);
+  k<<<nw, kThreads, sm, st>>>(ds, nw, x, g, hl, props, s, status);
   return cudaGetLastError();
 }
 
@@ -623,9 +628,10 @@ cudaError_t launch_move(const DevSys &hs, const DevSys *ds, DevPop pop, const Mo
                         cudaStream_t st) {
   if (a.nw <= 0) return cudaSuccess;
   size_t sm = move_smem_bytes(hs);
-  cudaError_t e = set_smem((const void *)move_kernel, sm);
+  auto k = hs.gmat ? move_kernel<true> : move_kernel<false>;
+  cudaError_t e = set_smem((const void *)k, sm);
   if (e != cudaSuccess) return e;
-  move_kernel<<<a.nw, kThreads, sm, st>>>(ds, pop, a);
+  k<<<a.nw, kThreads, sm, st>>>(ds, pop, a);
   return cudaGetLastError();
 }
 

@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_eval_beads_kernel(const DevSy
   extern __shared__ __align__(16) char smem[];
   load_sys(S, sp);
   EvalSmem m;
-  size_t off = eval_carve(S, smem, &m);
+  size_t off = eval_carve<0>(S, smem, &m);
   double *pn = reinterpret_cast<double *>(smem + off);
   double *hn = pn + S.nprops;
   double *sn = hn + 2;
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
   extern __shared__ __align__(16) char smem[];
   load_sys(S, sp);
   EvalSmem m;
-  size_t off = eval_carve(S, smem, &m);
+  size_t off = eval_carve<0>(S, smem, &m);
   double *pn = reinterpret_cast<double *>(smem + off);
   double *pp = pn + S.nprops;   // p_p_new
   double *ppo = pp + S.nprops;  // p_p_old
@@ -625,6 +625,11 @@ extern "C" int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params 
       prm->ntau - 2 * prm->ntauskip < 1 || !(prm->delta > 0.0)) {
     q2d::set_error("qmc2d_rmc_init: bad argument");
     return QMC2D_ERR_ARG;
+  }
+  if (h->hs.gmat) {
+    q2d::set_error("qmc2d_rmc_init: reptation keeps the determinants in shared memory, "
+                   "and this system's do not fit there");
+    return QMC2D_ERR_LIMIT;
   }
   RCK(cudaSetDevice(h->device));
   RCK(cudaStreamSynchronize(h->stream));

@@ -76,12 +76,26 @@ __host__ __device__ inline int xt_ldm(int n2) {
 }
 __host__ __device__ inline int xt_ldu(int n2) { return 8 * xt_row_tiles(n2) + 4; }
 
-// Carve the dynamic shared memory; returns bytes used.
-__host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSmem *m) {
-  size_t off = 0;
+// Carve the dynamic shared memory; returns bytes used. With s.gmat the
+// determinant matrices (A, W, F0 region) come from gbase instead, the
+// walker's block of global memory, and *gbytes (when given) receives its
+// size. kG fixes s.gmat at compile time in the kernels (0 off, 1 on); the
+// host's sizing reads it (-1).
+template <int kG = -1>
+__host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSmem *m,
+                                             char *gbase = nullptr, size_t *gbytes = nullptr) {
+  const bool gm = kG < 0 ? s.gmat != 0 : kG != 0;
+  size_t off = 0, goff = 0;
   auto take = [&](size_t bytes) -> char * {
     char *p = base ? base + off : nullptr;
     off += align16(bytes);
+    return p;
+  };
+  // the large matrices: shared memory, or the global block with s.gmat
+  auto mtake = [&](size_t bytes) -> char * {
+    if (!gm) return take(bytes);
+    char *p = gbase ? gbase + goff : nullptr;
+    goff += (bytes + 255) & ~size_t(255);
     return p;
   };
   int N = s.N, n = s.nmax > 0 ? s.nmax : 1, ld = ws_ld(n);
@@ -117,7 +131,7 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
 #pragma unroll
     for (int sp = 0; sp < 2; sp++) {
       if (sp >= nsp) continue;
-      t.A[sp] = (double2 *)take(awbytes > mbytes ? awbytes : mbytes);
+      t.A[sp] = (double2 *)mtake(awbytes > mbytes ? awbytes : mbytes);
       t.W[sp] = t.A[sp] ? t.A[sp] + n * n : nullptr;
       t.dk[sp] = (double *)take(sizeof(double) * n);
       t.perm[sp] = (int *)take(sizeof(int) * n);
@@ -135,7 +149,7 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
     size_t sbytes = (sizeof(double2) * slot_per_spin + sizeof(unsigned long long) * 2 * gw) * 2;
     size_t rbytes = fbytes > ubytes ? fbytes : ubytes;
     if (sbytes > rbytes) rbytes = sbytes;
-    t.F0 = (double2 *)take(rbytes);
+    t.F0 = (double2 *)mtake(rbytes);
     t.F1 = t.F0 ? t.F0 + n * n : nullptr;
     t.U = reinterpret_cast<double *>(t.F0);
     t.part = t.U ? t.U + (size_t)kChunk * ldu : nullptr;
@@ -152,7 +166,14 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
   t.gidx = (int *)take(sizeof(int) * 16);
   t.gval = (double *)take(sizeof(double) * 16);
   if (m) *m = t;
+  if (gbytes) *gbytes = goff;
   return off;
+}
+
+// The walker's block of global memory for the determinant matrices of
+// CTA b (gmat), or nullptr.
+__device__ __forceinline__ char *gmat_block(const DevSys &S, int b) {
+  return S.gmat ? reinterpret_cast<char *>(S.gmat_base + (size_t)b * S.gmat_stride) : nullptr;
 }
 
 // The pair passes alone (pairs_kernel): only the per-particle arrays they

@@ -299,7 +299,13 @@ def make_run(directory, runid, n_up, n_down, rs, nknots=1000, backflow=None, u3=
     alpha = alpha_L / L
     f = e2 * np.array([math.erfc(alpha * x) for x in r])
     df = -e2 * 2.0 * alpha / math.sqrt(math.pi) * np.exp(-(alpha * r) ** 2)
-    kv = krlv(L, math.sqrt(nmax2 + 0.5))  # |n|^2 <= nmax2, in the reference's order
+    # |n|^2 <= nmax2, in the reference's order; widened until the k set
+    # holds the orbitals of the larger determinant (2 nk + 1 plane waves)
+    nmax = max(n_up, n_down)
+    while sum(1 for a in range(-nmax, nmax + 1) for b in range(-nmax, nmax + 1)
+              if a * a + b * b <= nmax2) < nmax:
+        nmax2 += 1
+    kv = krlv(L, math.sqrt(nmax2 + 0.5))
     kn = np.sqrt((kv ** 2).sum(1))
     vk = e2 * 2.0 * math.pi * np.array([math.erfc(k / (2 * alpha)) for k in kn]) / (kn * L * L)
     v0 = -e2 * (N * alpha / math.sqrt(math.pi) + N * N * math.sqrt(math.pi) / (alpha * L * L))

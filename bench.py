@@ -75,11 +75,18 @@ def flops_per_move(N, ns, K, u3, backflow):
     return float(f)
 
 
-def make_config(tmp, nconf, seed):
+def make_config(tmp, nconf, seed, shell=None, rs=None):
+    """The headline deck, or with shell = (n_up, n_down) and rs another
+    closed shell and density with the same Jastrow and backflow forms.
+    Returns (directory, config, workload name)."""
     tables = importlib.import_module("2degas_b200.tables")
-    cfg = tables.CONFIGS[CONFIG]
-    d = tables.make_run(os.path.join(tmp, CONFIG), "c", nconf=nconf, seed=seed, **cfg)
-    return d, cfg
+    cfg, name = dict(tables.CONFIGS[CONFIG]), CONFIG
+    if shell is not None:
+        r = rs if rs is not None else cfg["rs"]
+        cfg.update(n_up=shell[0], n_down=shell[1], rs=r, backflow=(0.2, r, 0.6 * r))
+        name = f"dmc_bf_n{shell[0] + shell[1]}{'p' if shell[1] == 0 else ''}_rs{r:g}"
+    d = tables.make_run(os.path.join(tmp, name), "c", nconf=nconf, seed=seed, **cfg)
+    return d, cfg, name
 
 
 # ------------------------------------------------------------ CPU baseline
@@ -104,7 +111,7 @@ def _cpu_worker(args):
     return moves, time.perf_counter() - t0
 
 
-def cpu_rate(d, seconds, walkers_per_proc=8):
+def cpu_rate(d, seconds, walkers_per_proc=8, rs=None):
     """Oracle DMC on every host core (one process per core, spawn)."""
     import multiprocessing as mp
 
@@ -112,8 +119,9 @@ def cpu_rate(d, seconds, walkers_per_proc=8):
         ncores = len(os.sched_getaffinity(0))
     except AttributeError:
         ncores = os.cpu_count() or 1
-    cfg = importlib.import_module("2degas_b200.tables").CONFIGS[CONFIG]
-    delta = 0.05 * cfg["rs"] ** 2
+    if rs is None:
+        rs = importlib.import_module("2degas_b200.tables").CONFIGS[CONFIG]["rs"]
+    delta = 0.05 * rs ** 2
     ctx = mp.get_context("spawn")
     with ctx.Pool(ncores) as pool:
         res = pool.map(_cpu_worker, [(d, walkers_per_proc, 100 + i, seconds, delta, -0.3)
@@ -230,7 +238,7 @@ def reference_arm(args, rank, world):
     if rank != 0:
         return 0
     with tempfile.TemporaryDirectory() as tmp:
-        d, _ = make_config(tmp, 64, 1)
+        d, _, _ = make_config(tmp, 64, 1)
         secs = max(4.0, min(20.0, 0.4 * (args.steps + args.warmup)))
         rate, cores, sample = cpu_rate(d, secs)
     line = {
@@ -262,7 +270,8 @@ def b200_arm(args, rank, world, local_rank):
     nw = args.walkers
     tmp = tempfile.mkdtemp(prefix="qmc2d_bench_")
     cfg_seed, walker_seed = rank_seeds(rank)
-    d, cfg = make_config(tmp, nw, cfg_seed)
+    d, cfg, workload = make_config(tmp, nw, cfg_seed, args.shell, args.rs)
+    headline = workload == CONFIG
     sysobj = q.System.read(d, "c")
     N = sysobj.N
     ns = [sysobj.s.np[t] for t in range(sysobj.ntypes)]
@@ -299,7 +308,8 @@ def b200_arm(args, rank, world, local_rank):
         if rank == 0:
             print(json.dumps({"phases_cycles_per_move": {k: v / moves for k, v in ph.items() if v},
                               "share": {k: v / tot for k, v in ph.items() if v},
-                              "workload": CONFIG, "walkers": nw, "steps": args.steps}), flush=True)
+                              "workload": workload, "walkers": nw, "steps": args.steps}),
+                  flush=True)
         h.close()
         if dist:
             dist.barrier()
@@ -372,16 +382,19 @@ def b200_arm(args, rank, world, local_rank):
         peak = fp64_peak_tflops(torch)
         cpu = None
         if world == 1 and not args.no_cpu:
-            rate, cores, sample = cpu_rate(d, args.cpu_seconds)
+            rate, cores, sample = cpu_rate(d, args.cpu_seconds, rs=rs)
             cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
         launches = pair_n + move_n + br_n + ga_n
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": METRIC if headline else
+            (f"walker-moves/sec (DMC with backflow, N={N}{' polarised' if len(ns) == 1 else ''}"
+             f" r_s={rs:g}, {nw} walkers)"),
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f64 (f32 u2 and v2 pair terms)",
             "data": "synthetic",
-            "config": {"workload": CONFIG, "walkers_per_gpu": nw, "N": N, "rs": rs,
+            "config": {"workload": workload, "walkers_per_gpu": nw, "N": N, "rs": rs,
                        "precision": args.precision,
                        "pair_launch": {"groups": tuned[0], "stage_rows": tuned[1] == 0},
                        "tau": delta, "mmstep": 1, "moves_per_step": nw * world,
@@ -391,8 +404,9 @@ def b200_arm(args, rank, world, local_rank):
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": (MOVE_DRAM_READ_PER_WALKER + move_scratch_bytes(N, K)) * nw,
-                         "traffic_source": TRAFFIC_SOURCE,
+                         "traffic": ((MOVE_DRAM_READ_PER_WALKER + move_scratch_bytes(N, K)) * nw
+                                     if headline else None),
+                         "traffic_source": TRAFFIC_SOURCE if headline else None,
                          "kernel": "pairs_kernel + move_kernel",
                          "flops_per_move": fpm,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64)"},
@@ -424,8 +438,8 @@ def serve_arm(args, rank, world):
     if rank != 0:  # one GPU serves; further ranks would be further servers
         return 0
     serve = importlib.import_module("2degas_b200.serve")
-    unpol = [n for n in serve.closed_shells(81) if 26 <= 2 * n <= 162 and n <= 45]
-    pol = [n for n in serve.closed_shells(162) if 26 <= n <= 49]
+    unpol = [n for n in serve.closed_shells(81) if 26 <= 2 * n <= 162]
+    pol = [n for n in serve.closed_shells(162) if 26 <= n <= 162]
     kw = dict(block_steps=20, min_blocks=5, max_blocks=args.serve_blocks,
               precision=args.precision)
     stream = lambda: serve.poisson_stream(args.serve_requests, 20.0, 2026, unpol, pol,  # noqa: E731
@@ -477,9 +491,9 @@ def serve_arm(args, rank, world):
 
 def batch_arm(args, rank, world):
     """Batched uneven populations: 64 DMC populations spanning N in {26, 42,
-    58, 90} and r_s in {1, 2, 5, 10, 20}, half unpolarised (N/2 per spin) and
-    half fully polarised (the nearest closed shell the kernels hold: 25, 45,
-    49, 49), backflow on, 1024 walkers each, advanced together through
+    58, 90, 122} and r_s in {1, 2, 5, 10, 20}, half unpolarised (N/2 per
+    spin) and half fully polarised (the nearest closed shell: 25, 45, 57, 89,
+    121), backflow on, 1024 walkers each, advanced together through
     qmc2d_batch_dmc (one CUDA graph per call), against the same generations
     issued handle by handle."""
     import torch
@@ -489,12 +503,12 @@ def batch_arm(args, rank, world):
     q = importlib.import_module("2degas_b200")
     tables = importlib.import_module("2degas_b200.tables")
     tmp = tempfile.mkdtemp(prefix="qmc2d_batch_")
-    Ns, rss = [26, 42, 58, 90], [1.0, 2.0, 5.0, 10.0, 20.0]
-    pol_of = {26: 25, 42: 45, 58: 49, 90: 49}
+    Ns, rss = [26, 42, 58, 90, 122], [1.0, 2.0, 5.0, 10.0, 20.0]
+    pol_of = {26: 25, 42: 45, 58: 57, 90: 89, 122: 121}
     nw = args.batch_walkers
     specs = []
     for i in range(args.batch_pops):
-        N, pol, rs = Ns[i % 4], (i // 4) % 2, rss[(i // 8) % 5]
+        N, pol, rs = Ns[i % 5], (i // 5) % 2, rss[(i // 10) % 5]
         specs.append((pol_of[N], 0, rs) if pol else (N // 2, N // 2, rs))
     systems, handles = {}, []
     for k, (nu, nd, rs) in enumerate(specs):
@@ -572,6 +586,10 @@ def main():
     ap.add_argument("--workload", default="dmc", choices=["dmc", "serve", "batch"],
                     help="dmc: the N=58 DMC generation (default); serve: the serving stream; "
                          "batch: 64 uneven populations through one graph")
+    ap.add_argument("--shell", type=lambda v: tuple(int(t) for t in v.split(",")),
+                    default=None, metavar="NU,ND",
+                    help="dmc workload on another closed shell (electrons up, down)")
+    ap.add_argument("--rs", type=float, default=None, help="r_s with --shell")
     ap.add_argument("--batch-pops", type=int, default=64)
     ap.add_argument("--batch-walkers", type=int, default=1024)
     ap.add_argument("--serve-requests", type=int, default=24)

@@ -57,7 +57,7 @@ enum qmc2d_status {
 #define QMC2D_MAX_TYPES 2
 #define QMC2D_MAX_TABLES 16
 #define QMC2D_MAX_NP 162          /* electrons per walker */
-#define QMC2D_MAX_ORB 81          /* orbitals (electrons) per spin determinant */
+#define QMC2D_MAX_ORB 162         /* orbitals (electrons) per spin determinant */
 #define QMC2D_MAX_NK 512          /* half-space k vectors */
 #define QMC2D_NAME_LEN 64
 #define QMC2D_MAX_EST 4           /* path-estimator records of each kind */
