@@ -396,6 +396,10 @@ class Batch:
         except Exception:
             pass
 
+    def set_lanes(self, lanes):
+        """At most `lanes` populations in flight at a time (0: all)."""
+        _capi.check(self.lib, self.lib.qmc2d_batch_set_lanes(self.b, lanes))
+
     def vmc(self, nstp, delta, mage=10 ** 9):
         d = np.ascontiguousarray(np.broadcast_to(np.asarray(delta, float), (len(self.handles),)))
         _capi.check(self.lib, self.lib.qmc2d_batch_vmc(self.b, nstp, _pd(d), mage))

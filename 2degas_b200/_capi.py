@@ -208,6 +208,7 @@ SIGNATURES = {
     "qmc2d_autotune": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), PD]),
     "qmc2d_batch_create": (c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p)]),
     "qmc2d_batch_destroy": (c_int, [c_void_p]),
+    "qmc2d_batch_set_lanes": (c_int, [c_void_p, c_int]),
     "qmc2d_batch_vmc": (c_int, [c_void_p, c_int, PD, c_int]),
     "qmc2d_batch_dmc": (c_int, [c_void_p, c_int, PD, PD, c_double, c_int]),
     "qmc2d_stats_create": (c_int, [c_int, POINTER(c_void_p)]),

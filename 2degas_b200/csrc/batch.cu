@@ -3,14 +3,26 @@
 // N, density, polarisation and walker count); one call advances all of them
 // by the same number of VMC steps or DMC generations.
 //
-// One CUDA graph holds two generations of every population: the launches of
-// population k (pair kernel, move kernel and, for DMC, the comb and the
-// gather) go on handle k's stream, forked from and joined back to the
-// batch's capture stream, so the populations' kernels overlap on the GPU and
-// the host issues one graph launch per two generations instead of 4-8
-// launches per population per generation. Two generations, because the
-// gather ping-pongs between the handle's two population buffers: after two
-// the buffers are back where the graph began, so the same graph replays.
+// One CUDA graph holds an even number of generations of every population
+// (a call of n generations: n rounded down to even, at most
+// kMaxGraphGenerations): the launches of population k (pair kernel, move
+// kernel and, for DMC, the comb and the gather) go on handle k's stream,
+// forked from and joined back to the batch's capture stream, so the
+// populations' kernels overlap on the GPU and the host issues one graph
+// launch per replay instead of 4-8 launches per population per generation.
+// An even number, because the gather ping-pongs between the handle's two
+// population buffers: after an even number the buffers are back where the
+// graph began, so the same graph replays. The join at the end of a replay
+// waits for the slowest population, so longer graphs leave the GPU idle
+// less often when the populations' costs differ; what the graph does not
+// cover (an odd last generation, or the rest of n) is launched directly.
+//
+// Lanes (qmc2d_batch_set_lanes): by default every population forks from the
+// capture stream at once. With S lanes, at most S populations run at a
+// time: the populations are dealt to S chains, largest estimated cost
+// first onto the least loaded chain, and each waits for the one before it
+// in its chain. Fewer populations in flight keep fewer working sets (move
+// scratch, determinant blocks) competing for L2.
 //
 // A replay repeats the launches' arguments; the Philox move and comb
 // counters that must advance are read from a per-population device pair
@@ -24,6 +36,7 @@
 // energies, population sizes, buffer parity) differ from the cached one.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -32,6 +45,8 @@
 #include "common.h"
 #include "handle.h"
 #include "kernels.cuh"
+
+constexpr int kMaxGraphGenerations = 16;
 
 struct qmc2d_batch {
   std::vector<qmc2d_handle *> h;
@@ -42,6 +57,7 @@ struct qmc2d_batch {
   uint32_t *d_ctr = nullptr;  // 2 per population: {move, generation}
   cudaGraphExec_t exec = nullptr;
   std::vector<double> key;  // parameters the cached graph was captured with
+  int lanes = 0;             // concurrent chains of populations (0: all at once)
 };
 
 namespace {
@@ -99,15 +115,51 @@ cudaError_t enqueue(qmc2d_batch *b, int k, int g0, int ngen, int dmc, double del
   return cudaSuccess;
 }
 
-// One step of every population: fork from the master stream, enqueue,
-// advance the counters by the generations enqueued, join.
+// Estimated cost of one generation of population k: the pair terms and,
+// per spin, the determinant work (O(N n^2)).
+double pop_cost(const qmc2d_handle *h) {
+  double c = 0.5 * h->N * h->N;
+  for (int t = 0; t < h->hs.nt; t++) c += (double)h->N * h->hs.np[t] * h->hs.np[t];
+  return c * h->nw;
+}
+
+// The order to enqueue the populations in and, for each, the population it
+// waits for (-1: the fork), for the batch's lanes.
+void lane_plan(const qmc2d_batch *b, std::vector<int> *order, std::vector<int> *prev) {
+  const int np = (int)b->h.size();
+  const int S = b->lanes > 0 && b->lanes < np ? b->lanes : np;
+  order->resize(np);
+  prev->assign(np, -1);
+  for (int k = 0; k < np; k++) (*order)[k] = k;
+  if (S == np) return;
+  std::vector<double> cost(np);
+  for (int k = 0; k < np; k++) cost[k] = pop_cost(b->h[k]);
+  std::stable_sort(order->begin(), order->end(),
+                   [&](int a, int c) { return cost[a] > cost[c]; });
+  std::vector<double> load(S, 0.0);
+  std::vector<int> last(S, -1);
+  for (int k : *order) {
+    const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    (*prev)[k] = last[l];
+    last[l] = k;
+    load[l] += cost[k];
+  }
+}
+
+// One step of every population: fork from the master stream (or wait for
+// the population before it in its lane), enqueue, advance the counters by
+// the generations enqueued, join.
 cudaError_t enqueue_all(qmc2d_batch *b, int g0, int ngen, int dmc, const double *delta,
                         const double *etrial, double mmult, int mage) {
   cudaError_t e;
+  std::vector<int> order, prev;
+  lane_plan(b, &order, &prev);
   if ((e = cudaEventRecord(b->fork, b->master)) != cudaSuccess) return e;
-  for (size_t k = 0; k < b->h.size(); k++) {
+  for (int k : order) {
     qmc2d_handle *h = b->h[k];
-    if ((e = cudaStreamWaitEvent(h->stream, b->fork, 0)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(h->stream, prev[k] < 0 ? b->fork : b->join[prev[k]], 0)) !=
+        cudaSuccess)
+      return e;
     if ((e = enqueue(b, (int)k, g0, ngen, dmc, delta[k], dmc ? etrial[k] : 0.0, mmult, mage)) !=
         cudaSuccess)
       return e;
@@ -147,9 +199,11 @@ int run(qmc2d_batch *b, int n, int dmc, const double *delta, const double *etria
   // the counters and every handle's pending work precede the first replay
   BCK(cudaMemcpy(b->d_ctr, ctr.data(), sizeof(uint32_t) * 2 * np, cudaMemcpyHostToDevice));
   for (size_t k = 0; k < np; k++) BCK(cudaStreamSynchronize(b->h[k]->stream));
-  const int pairs = n / 2;
-  if (pairs > 0) {
-    std::vector<double> key = {(double)dmc, mmult, (double)mage};
+  const int gpg = std::min(n & ~1, kMaxGraphGenerations);  // generations per replay
+  const int replays = gpg > 0 ? n / gpg : 0;
+  if (replays > 0) {
+    std::vector<double> key = {(double)dmc, mmult, (double)mage, (double)gpg,
+                               (double)b->lanes};
     for (size_t k = 0; k < np; k++) {
       key.push_back(delta[k]);
       key.push_back(dmc ? etrial[k] : 0.0);
@@ -165,7 +219,7 @@ int run(qmc2d_batch *b, int n, int dmc, const double *delta, const double *etria
       }
       cudaGraph_t g = nullptr;
       BCK(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeRelaxed));
-      cudaError_t e = enqueue_all(b, 0, 2, dmc, delta, etrial, mmult, mage);
+      cudaError_t e = enqueue_all(b, 0, gpg, dmc, delta, etrial, mmult, mage);
       cudaError_t e2 = cudaStreamEndCapture(b->master, &g);
       if (e != cudaSuccess) {
         if (g) cudaGraphDestroy(g);
@@ -177,9 +231,10 @@ int run(qmc2d_batch *b, int n, int dmc, const double *delta, const double *etria
       BCK(e);
       b->key = key;
     }
-    for (int r = 0; r < pairs; r++) BCK(cudaGraphLaunch(b->exec, b->master));
+    for (int r = 0; r < replays; r++) BCK(cudaGraphLaunch(b->exec, b->master));
   }
-  if (n & 1) BCK(enqueue_all(b, 0, 1, dmc, delta, etrial, mmult, mage));
+  const int rest = n - replays * gpg;
+  if (rest > 0) BCK(enqueue_all(b, 0, rest, dmc, delta, etrial, mmult, mage));
   BCK(cudaStreamSynchronize(b->master));
   int worst = QMC2D_OK;
   for (size_t k = 0; k < np; k++) {
@@ -250,6 +305,15 @@ extern "C" int qmc2d_batch_destroy(qmc2d_batch *b) {
   if (b->master) cudaStreamDestroy(b->master);
   cudaFree(b->d_ctr);
   delete b;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_batch_set_lanes(qmc2d_batch *b, int lanes) {
+  if (!b || lanes < 0) {
+    q2d::set_error("qmc2d_batch_set_lanes: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  b->lanes = lanes;
   return QMC2D_OK;
 }
 

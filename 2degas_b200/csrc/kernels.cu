@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(kThreads, 2) eval_kernel(const DevSys *sp, int
   for (int j = threadIdx.x; j < N2; j += blockDim.x) m.x[j] = x[(size_t)w * N2 + j];
   __syncthreads();
   long long tph = clock64();
-  int st = eval_walker<R>(S, m, hn, pn, sn, tph);
+  int st = eval_walker<R, kGmat>(S, m, hn, pn, sn, tph);
   for (int j = threadIdx.x; j < N2; j += blockDim.x) g[(size_t)w * N2 + j] = m.g[j];
   for (int j = threadIdx.x; j < S.nprops; j += blockDim.x)
     props[(size_t)w * S.nprops + j] = pn[j];
@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
   const uint32_t step = a.step0 + (a.ctr ? a.ctr[0] : 0u);
   long long tph = clock64();
   double sn = 1.0;
-  status |= eval_det(S, m, v.hn, v.pn, &v.sc[0], tph, S.has_bf ? o + L.pair : nullptr,
+  status |= eval_det<kGmat>(S, m, v.hn, v.pn, &v.sc[0], tph, S.has_bf ? o + L.pair : nullptr,
                      o + L.rhok);
   sn = v.sc[0];
   // reverse move (reptation.f:4660-4674)

@@ -45,6 +45,8 @@ struct EvalSmem {
   // of every warp and the warps' pivot keys (inside the F0 region)
   double2 *gslot[2];
   unsigned long long *gkey[2];
+  // inversion in global memory (gmat): column k of each spin's W
+  double2 *fcol[2];
 };
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
@@ -123,6 +125,7 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
   t.D2 = t.U = t.part = t.gsh = t.fdg = nullptr;
   t.dk[0] = t.dk[1] = nullptr;
   t.perm[0] = t.perm[1] = t.used[0] = t.used[1] = nullptr;
+  t.fcol[0] = t.fcol[1] = nullptr;
   if (s.has_bf) {
     // A[s] and W[s] are adjacent: the 2n x 2n real cross-term matrix of spin
     // s (row stride xt_ldm) overlays them once F0/F1 are formed.
@@ -136,6 +139,7 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
       t.dk[sp] = (double *)take(sizeof(double) * n);
       t.perm[sp] = (int *)take(sizeof(int) * n);
       t.used[sp] = (int *)take(sizeof(int) * n);
+      t.fcol[sp] = gm ? (double2 *)take(sizeof(double2) * n) : nullptr;
     }
     // F0/F1 are dead once the cross-term matrix is built, so the cross
     // term's Jacobian columns U and partial sums share their space.
@@ -687,6 +691,108 @@ __device__ inline void gj_invert(double2 *W, int ld, int n, int *perm, double *d
 }
 
 // The same inversion (same pivot rule, same outputs perm, dk, W and the
+// singular flag) for W in global memory (determinants held in HBM): the
+// lanes of a warp take consecutive columns of a row, so every row access is
+// coalesced, and the warps of the group take the rows in turn. Column k is
+// gathered into fcol (n entries of shared memory) at the start of step k:
+// it supplies the pivot search and every row's multiplier.
+__device__ inline void gj_invert_gmem(double2 *W, int ld, int n, int *perm, double *dk,
+                                      int *used, int *singular, int gt, int G, int bar_id,
+                                      double *gval, int *gidx, double2 *fcol) {
+  const int nthr = 32 * G, lane = gt & 31, wg = gt >> 5;
+  auto gsync = [&]() {
+    if (G == 1) __syncwarp();
+    else asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthr) : "memory");
+  };
+  for (int r = gt; r < n; r += nthr) used[r] = 0;
+  gsync();
+  for (int k = 0; k < n; k++) {
+    double best = -1.0;
+    int bi = n;
+    for (int r = gt; r < n; r += nthr) {
+      const double2 v = W[(size_t)r * ld + k];
+      fcol[r] = v;
+      if (!used[r]) {
+        const double a = cabs1(v);
+        if (a > best) {
+          best = a;
+          bi = r;
+        }
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (G > 1 && lane == 0) {
+      gval[wg] = best;
+      gidx[wg] = bi;
+    }
+    gsync();  // fcol and the warps' candidates
+    if (G > 1) {
+      best = gval[0];
+      bi = gidx[0];
+      for (int w = 1; w < G; w++)
+        if (gval[w] > best || (gval[w] == best && gidx[w] < bi)) {
+          best = gval[w];
+          bi = gidx[w];
+        }
+    }
+    const int p = bi < n ? bi : k;  // bi == n only if every candidate is NaN
+    const double2 piv = fcol[p];
+    const double d = piv.x * piv.x + piv.y * piv.y;
+    const double rd = 1.0 / d;
+    const double2 inv = make_double2(piv.x * rd, -piv.y * rd);
+    double2 *prow = W + (size_t)p * ld;
+    for (int c = gt; c < n; c += nthr) prow[c] = (c == k) ? inv : cmul(prow[c], inv);
+    gsync();  // the scaled pivot row; gval and gidx are read
+    if (gt == 0) {
+      perm[k] = p;
+      dk[k] = d;
+      used[p] = 1;
+      if (!(best > 0.0)) *singular = 1;
+    }
+    // four rows per warp at a time, so that four row loads are in flight
+    for (int r0 = wg; r0 < n; r0 += 4 * G) {
+      bool on[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int r = r0 + i * G;
+        on[i] = r < n && r != p;
+      }
+#pragma unroll 2
+      for (int c = lane; c < n; c += 32) {
+        const double2 a = prow[c];
+        double2 v[4], fi[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) fi[i] = on[i] ? fcol[r0 + i * G] : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+          v[i] = on[i] ? W[(size_t)(r0 + i * G) * ld + c] : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          if (c == k) {
+            const double2 t = cmul(fi[i], inv);
+            v[i] = make_double2(-t.x, -t.y);
+          } else {
+            v[i].x -= fi[i].x * a.x - fi[i].y * a.y;
+            v[i].y -= fi[i].x * a.y + fi[i].y * a.x;
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+          if (on[i]) W[(size_t)(r0 + i * G) * ld + c] = v[i];
+      }
+    }
+    gsync();
+  }
+}
+
+// The same inversion (same pivot rule, same outputs perm, dk, W and the
 // singular flag) with every row held in registers: thread gt of the
 // 32G-thread group owns row r = gt / L and the columns s + L j (s = gt % L,
 // j < kGjCols) with L = gj_reg_lanes(n, 32G). Per step k:
@@ -1059,6 +1165,7 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
 // F, drift, Laplacian with the cross term), rho_k, assembly. With pin, the
 // backflow Jacobian blocks take the pair spline values written by
 // eval_pairs(pout) instead of evaluating them again.
+template <bool kGmat = false>
 __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, double *props,
                                double *sign, long long &tph, const double *pin,
                                const double *rhok_in = nullptr) {
@@ -1104,8 +1211,9 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
     // inversion: every warp in registers when each spin's matrix fits that
     // layout (then rho_k), else half the CTA per shared-memory inversion
     // with rho_k on the other warps
+    // (determinants in HBM: every warp, coalesced rows, then rho_k)
     const int Gr = gj_reg_warps(nt);
-    bool reg_path = true;
+    bool reg_path = !kGmat;
     for (int sp = 0; sp < nt; sp++) reg_path = reg_path && gj_reg_lanes(S.np[sp], 32 * Gr) > 0;
     if (reg_path) {
       const int sp = nt > 1 ? (tid >> 5) / Gr : 0, gt = tid - sp * 32 * Gr;
@@ -1118,14 +1226,21 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
       __syncthreads();
     } else {
       // warps per spin: half the CTA for the inversions, the rest for rho_k
-      const int G = (kThreads / 32) / (2 * nt) > 0 ? (kThreads / 32) / (2 * nt) : 1;
+      const int G = kGmat ? (kThreads / 32) / nt
+                          : ((kThreads / 32) / (2 * nt) > 0 ? (kThreads / 32) / (2 * nt) : 1);
       const int w = tid >> 5;
       if (w < G * nt) {
         const int sp = w / G, gt = tid - sp * 32 * G;
         const int ns = S.np[sp];
-        gj_invert(sp ? m.W[1] : m.W[0], ws_ld(ns), ns, sp ? m.perm[1] : m.perm[0],
-                  sp ? m.dk[1] : m.dk[0], sp ? m.used[1] : m.used[0], &m.iscal[sp], gt,
-                  G, 1 + sp, m.gval + 8 * sp, m.gidx + 8 * sp);
+        if (kGmat)
+          gj_invert_gmem(sp ? m.W[1] : m.W[0], ws_ld(ns), ns, sp ? m.perm[1] : m.perm[0],
+                         sp ? m.dk[1] : m.dk[0], sp ? m.used[1] : m.used[0], &m.iscal[sp], gt,
+                         G, 1 + sp, m.gval + 8 * sp, m.gidx + 8 * sp,
+                         sp ? m.fcol[1] : m.fcol[0]);
+        else
+          gj_invert(sp ? m.W[1] : m.W[0], ws_ld(ns), ns, sp ? m.perm[1] : m.perm[0],
+                    sp ? m.dk[1] : m.dk[0], sp ? m.used[1] : m.used[0], &m.iscal[sp], gt,
+                    G, 1 + sp, m.gval + 8 * sp, m.gidx + 8 * sp);
       } else {
         rhok(tid - G * nt * 32, kThreads - G * nt * 32);
       }
@@ -1560,11 +1675,11 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
 
 // The whole evaluation of the configuration in m.x (compute_properties,
 // reptation.f:2661), with the u2 and v2 pair terms in precision R.
-template <class R = double>
+template <class R = double, bool kGmat = false>
 __device__ inline int eval_walker(const DevSys &S, const EvalSmem &m, double *hl, double *props,
                                   double *sign, long long &tph) {
   eval_pairs<kThreads, false>(S, m, tph, nullptr, pair_rows<R>(S));
-  return eval_det(S, m, hl, props, sign, tph, nullptr);
+  return eval_det<kGmat>(S, m, hl, props, sign, tph, nullptr);
 }
 
 }  // namespace q2d

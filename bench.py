@@ -536,13 +536,18 @@ def batch_arm(args, rank, world):
     K = args.steps
     moves = K * nw * len(handles)
     b = q.Batch(handles)
-    b.dmc(2, taus, et)  # warm-up and capture
-    torch.cuda.synchronize()
+    sweep = {}
     with Clocks(0) as clk:
-        t0 = time.perf_counter()
-        b.dmc(K, taus, et)
-        torch.cuda.synchronize()
-        t_batch = time.perf_counter() - t0
+        for lanes in args.batch_lanes:  # concurrent chains of populations (0: all)
+            b.set_lanes(lanes)
+            b.dmc(max(2, min(K - K % 2, 16)), taus, et)  # warm-up and capture (the graph of K)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            b.dmc(K, taus, et)
+            torch.cuda.synchronize()
+            sweep[lanes] = time.perf_counter() - t0
+        best = min(sweep, key=sweep.get)
+        t_batch = sweep[best]
         t0 = time.perf_counter()
         for h, t, e in zip(handles, taus, et):  # the same work, one population at a time
             h.dmc(K, 1, t, e, 2.0, 50)
@@ -557,7 +562,8 @@ def batch_arm(args, rank, world):
         "data": "synthetic",
         "config": {"workload": "batched_populations", "populations": len(handles),
                    "walkers_each": nw, "N": Ns, "rs": rss, "polarised_shells": pol_of,
-                   "tau": "0.01 r_s^2", "precision": args.precision,
+                   "tau": "0.01 r_s^2", "precision": args.precision, "lanes": best,
+                   "lanes_sweep_s": sweep,
                    "timing": "host wall clock around one qmc2d_batch_dmc call (synchronised)"},
         "handle_by_handle": {"value": moves / t_seq, "seconds": t_seq},
         "speedup_vs_handle_by_handle": t_seq / t_batch,
@@ -592,6 +598,9 @@ def main():
     ap.add_argument("--rs", type=float, default=None, help="r_s with --shell")
     ap.add_argument("--batch-pops", type=int, default=64)
     ap.add_argument("--batch-walkers", type=int, default=1024)
+    ap.add_argument("--batch-lanes", type=lambda v: [int(t) for t in v.split(",")],
+                    default=[0, 4, 8, 16], metavar="S,S,...",
+                    help="populations in flight at a time to try (0: all); the best is kept")
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-blocks", type=int, default=100)
     ap.add_argument("--serve-slots", type=int, default=4)

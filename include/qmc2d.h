@@ -225,9 +225,10 @@ int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *ms);
 
 /* Batches: many independent populations (handles of different systems, on
  * one device) advanced together. The reference runs one population per
- * process and has no counterpart. A call captures one CUDA graph holding
- * two steps of every population (each handle's launches on its own stream,
- * forked from and joined to the batch's stream) and replays it; the
+ * process and has no counterpart. A call of n steps captures one CUDA
+ * graph holding min(n rounded down to even, 16) steps of every population
+ * (each handle's launches on its own stream, forked from and joined to the
+ * batch's stream), replays it, and launches the rest directly; the
  * populations' kernels overlap on the GPU. The Philox counters advance in
  * device memory, so a batch call gives the walkers, block sums and
  * counters that the same qmc2d_vmc / qmc2d_dmc calls made handle by handle
@@ -236,6 +237,11 @@ int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *ms);
 typedef struct qmc2d_batch qmc2d_batch;
 int qmc2d_batch_create(qmc2d_handle *const *handles, int n, qmc2d_batch **out);
 int qmc2d_batch_destroy(qmc2d_batch *b);
+/* At most `lanes` populations in flight at a time (0, the default: all):
+ * the populations are dealt to that many chains, largest estimated cost
+ * (walkers x (N^2/2 + N sum n^2)) first onto the least loaded chain, each
+ * waiting for the one before it. Results do not depend on it. */
+int qmc2d_batch_set_lanes(qmc2d_batch *b, int lanes);
 /* nstp VMC steps of every population; delta[k]: population k's time step
  * (qmc2d_vmc per handle). */
 int qmc2d_batch_vmc(qmc2d_batch *b, int nstp, const double *delta, int mage);

@@ -2,8 +2,9 @@
 density and polarisation advanced together through one CUDA graph per call
 give the walkers, block sums and counters of the same qmc2d_vmc /
 qmc2d_dmc calls made handle by handle, bit for bit, for even step counts
-(graph replays only) and odd ones (one more generation launched directly),
-and across calls that reuse or recapture the graph."""
+(graph replays only), odd ones (one more generation launched directly) and
+counts beyond one graph (replays of 16 generations, the rest launched
+directly), and across calls that reuse or recapture the graph."""
 import importlib
 import os
 
@@ -57,7 +58,7 @@ def _same(a, b):
     assert a[4] == b[4]
 
 
-@pytest.mark.parametrize("ngen", [4, 3])
+@pytest.mark.parametrize("ngen", [4, 3, 37])
 def test_batch_dmc_equals_handle_by_handle(q, systems, ngen):
     taus = [0.01 * rs * rs for _, rs, _ in systems]
     et = [-0.3, -0.1, 0.4, -0.05]
@@ -85,5 +86,20 @@ def test_batch_vmc_and_graph_reuse(q, systems):
         b.vmc(4, taus)  # the cached graph replays
         b.dmc(2, [0.2 * t for t in taus], -0.2)
         b.dmc(2, [0.2 * t for t in taus], -0.25)  # a new trial energy: captured again
+    for h, r in zip(hs, ref):
+        _same(_state(h), _state(r))
+
+
+@pytest.mark.parametrize("lanes", [1, 2])
+def test_batch_lanes_do_not_change_results(q, systems, lanes):
+    taus = [0.01 * rs * rs for _, rs, _ in systems]
+    et = [-0.3, -0.1, 0.4, -0.05]
+    ref = _start(q, systems)
+    for h, t, e in zip(ref, taus, et):
+        h.dmc(5, 1, t, e, 2.0, 50)
+    hs = _start(q, systems)
+    with q.Batch(hs) as b:
+        b.set_lanes(lanes)
+        b.dmc(5, taus, et, 2.0, 50)
     for h, r in zip(hs, ref):
         _same(_state(h), _state(r))
