@@ -45,7 +45,8 @@ struct EvalSmem {
   // of every warp and the warps' pivot keys (inside the F0 region)
   double2 *gslot[2];
   unsigned long long *gkey[2];
-  // inversion in global memory (gmat): column k of each spin's W
+  // inversion in global memory (gmat): each spin's panel, multipliers and
+  // scaled pivot rows (gj_invert_gmem)
   double2 *fcol[2];
 };
 
@@ -58,6 +59,14 @@ __host__ __device__ inline int ws_ld(int n) { return n | 1; }
 // lanes per row L (a power of two) with kGjCols*L >= n and one row per
 // thread of an nthr-thread group; 0 when n does not fit that layout.
 constexpr int kGjCols = 8;
+// Pivot steps per pass over a determinant held in HBM (gj_invert_gmem),
+// and the shared memory that inversion takes per spin: the panel (later
+// the scaled pivot rows), the multipliers, the pivots' reciprocals and rows.
+constexpr int kGjBlock = 8;
+__host__ __device__ inline size_t gj_gmem_scratch(int n) {
+  return sizeof(double2) * (2 * (size_t)kGjBlock * n + kGjBlock) + sizeof(int) * kGjBlock;
+}
+
 __host__ __device__ inline int gj_reg_lanes(int n, int nthr) {
   for (int L = 1; L <= 32; L *= 2)
     if (kGjCols * L >= n && nthr / L >= n) return L;
@@ -139,7 +148,7 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
       t.dk[sp] = (double *)take(sizeof(double) * n);
       t.perm[sp] = (int *)take(sizeof(int) * n);
       t.used[sp] = (int *)take(sizeof(int) * n);
-      t.fcol[sp] = gm ? (double2 *)take(sizeof(double2) * n) : nullptr;
+      t.fcol[sp] = gm ? (double2 *)take(gj_gmem_scratch(n)) : nullptr;
     }
     // F0/F1 are dead once the cross-term matrix is built, so the cross
     // term's Jacobian columns U and partial sums share their space.
@@ -691,101 +700,158 @@ __device__ inline void gj_invert(double2 *W, int ld, int n, int *perm, double *d
 }
 
 // The same inversion (same pivot rule, same outputs perm, dk, W and the
-// singular flag) for W in global memory (determinants held in HBM): the
-// lanes of a warp take consecutive columns of a row, so every row access is
-// coalesced, and the warps of the group take the rows in turn. Column k is
-// gathered into fcol (n entries of shared memory) at the start of step k:
-// it supplies the pivot search and every row's multiplier.
+// singular flag, the same operations on every element in the same order)
+// for W in global memory (determinants held in HBM), kGjBlock pivot steps
+// per pass over the matrix, so that each element crosses L2 once per block
+// instead of once per step. Per block of steps k0 .. k0+nb-1:
+//   * panel: columns k0.. of every row are copied to shared memory (P) and
+//     the nb steps run there alone: pivot search, the multipliers of every
+//     row (F[j][r], the row's column-k entry before step k) and the
+//     panel's own elimination; the panel then goes back to W;
+//   * pivot rows: for every column c outside the panel, the pivot row of
+//     step j as it is scaled at step j, Q[j][c] = (W(p_j, c) - sum over
+//     earlier steps j' of F[j'][p_j] Q[j'][c]) / pivot_j (Q takes P's
+//     place);
+//   * every row, lanes on consecutive columns (coalesced) and four rows in
+//     flight per warp: W(r, c) -= F[j][r] Q[j][c] for the block's steps in
+//     order (a pivot row starts from its Q and takes the later steps only).
+// scr: gj_gmem_scratch(n) bytes of shared memory.
 __device__ inline void gj_invert_gmem(double2 *W, int ld, int n, int *perm, double *dk,
                                       int *used, int *singular, int gt, int G, int bar_id,
-                                      double *gval, int *gidx, double2 *fcol) {
+                                      double *gval, int *gidx, double2 *scr) {
+  constexpr int B = kGjBlock;
   const int nthr = 32 * G, lane = gt & 31, wg = gt >> 5;
+  double2 *P = scr;              // P[r * B + j]: panel
+  double2 *Q = scr;              // Q[j * n + c]: scaled pivot rows (after the panel)
+  double2 *F = scr + B * n;      // F[j * n + r]: multipliers
+  double2 *I = scr + 2 * B * n;  // I[j]: 1 / pivot of step j
+  int *PJ = reinterpret_cast<int *>(I + B);  // PJ[j]: pivot row of step j
   auto gsync = [&]() {
     if (G == 1) __syncwarp();
     else asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthr) : "memory");
   };
+  auto sub = [](double2 &v, double2 f, double2 a) {
+    v.x -= f.x * a.x - f.y * a.y;
+    v.y -= f.x * a.y + f.y * a.x;
+  };
   for (int r = gt; r < n; r += nthr) used[r] = 0;
-  gsync();
-  for (int k = 0; k < n; k++) {
-    double best = -1.0;
-    int bi = n;
-    for (int r = gt; r < n; r += nthr) {
-      const double2 v = W[(size_t)r * ld + k];
-      fcol[r] = v;
-      if (!used[r]) {
-        const double a = cabs1(v);
-        if (a > best) {
-          best = a;
-          bi = r;
+  for (int k0 = 0; k0 < n; k0 += B) {
+    const int nb = min(B, n - k0);
+    for (int e = gt; e < n * nb; e += nthr) {
+      const int r = e / nb, j = e - r * nb;
+      P[r * B + j] = W[(size_t)r * ld + k0 + j];
+    }
+    gsync();
+    for (int j = 0; j < nb; j++) {
+      const int k = k0 + j;
+      double best = -1.0;
+      int bi = n;
+      for (int r = gt; r < n; r += nthr)
+        if (!used[r]) {
+          const double a = cabs1(P[r * B + j]);
+          if (a > best) {
+            best = a;
+            bi = r;
+          }
+        }
+      for (int o = 16; o > 0; o >>= 1) {
+        double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
         }
       }
+      if (G > 1) {
+        if (lane == 0) {
+          gval[wg] = best;
+          gidx[wg] = bi;
+        }
+        gsync();
+        best = gval[0];
+        bi = gidx[0];
+        for (int w = 1; w < G; w++)
+          if (gval[w] > best || (gval[w] == best && gidx[w] < bi)) {
+            best = gval[w];
+            bi = gidx[w];
+          }
+      }
+      const int p = bi < n ? bi : k;  // bi == n only if every candidate is NaN
+      const double2 piv = P[p * B + j];
+      const double d = piv.x * piv.x + piv.y * piv.y;
+      const double rd = 1.0 / d;
+      const double2 inv = make_double2(piv.x * rd, -piv.y * rd);
+      for (int r = gt; r < n; r += nthr) F[j * n + r] = P[r * B + j];
+      gsync();  // F; gval and gidx are read
+      if (gt == 0) {
+        perm[k] = p;
+        dk[k] = d;
+        used[p] = 1;
+        I[j] = inv;
+        PJ[j] = p;
+        if (!(best > 0.0)) *singular = 1;
+      }
+      if (gt < nb) P[p * B + gt] = (gt == j) ? inv : cmul(P[p * B + gt], inv);
+      gsync();
+      for (int e = gt; e < n * nb; e += nthr) {
+        const int r = e / nb, jj = e - r * nb;
+        if (r == p) continue;
+        const double2 fi = F[j * n + r];
+        double2 v;
+        if (jj == j) {
+          const double2 t = cmul(fi, inv);
+          v = make_double2(-t.x, -t.y);
+        } else {
+          v = P[r * B + jj];
+          sub(v, fi, P[p * B + jj]);
+        }
+        P[r * B + jj] = v;
+      }
+      gsync();
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      double ob = __shfl_xor_sync(0xffffffffu, best, o);
-      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ob > best || (ob == best && oi < bi)) {
-        best = ob;
-        bi = oi;
+    for (int e = gt; e < n * nb; e += nthr) {
+      const int r = e / nb, j = e - r * nb;
+      W[(size_t)r * ld + k0 + j] = P[r * B + j];
+    }
+    gsync();  // P is free: Q takes its place
+    // the block's pivot rows outside the panel, as scaled at their step
+    for (int c = gt; c < n; c += nthr) {
+      if (c >= k0 && c < k0 + nb) continue;
+      for (int j = 0; j < nb; j++) {
+        const int pr = PJ[j];
+        double2 x = W[(size_t)pr * ld + c];
+        for (int jj = 0; jj < j; jj++) sub(x, F[jj * n + pr], Q[jj * n + c]);
+        Q[j * n + c] = cmul(x, I[j]);
       }
     }
-    if (G > 1 && lane == 0) {
-      gval[wg] = best;
-      gidx[wg] = bi;
-    }
-    gsync();  // fcol and the warps' candidates
-    if (G > 1) {
-      best = gval[0];
-      bi = gidx[0];
-      for (int w = 1; w < G; w++)
-        if (gval[w] > best || (gval[w] == best && gidx[w] < bi)) {
-          best = gval[w];
-          bi = gidx[w];
-        }
-    }
-    const int p = bi < n ? bi : k;  // bi == n only if every candidate is NaN
-    const double2 piv = fcol[p];
-    const double d = piv.x * piv.x + piv.y * piv.y;
-    const double rd = 1.0 / d;
-    const double2 inv = make_double2(piv.x * rd, -piv.y * rd);
-    double2 *prow = W + (size_t)p * ld;
-    for (int c = gt; c < n; c += nthr) prow[c] = (c == k) ? inv : cmul(prow[c], inv);
-    gsync();  // the scaled pivot row; gval and gidx are read
-    if (gt == 0) {
-      perm[k] = p;
-      dk[k] = d;
-      used[p] = 1;
-      if (!(best > 0.0)) *singular = 1;
-    }
-    // four rows per warp at a time, so that four row loads are in flight
+    gsync();
+    // every row, outside the panel: the block's steps in order
     for (int r0 = wg; r0 < n; r0 += 4 * G) {
-      bool on[4];
+      int role[4];  // -2: no row, -1: not a pivot of the block, j: pivot of step j
 #pragma unroll
       for (int i = 0; i < 4; i++) {
         const int r = r0 + i * G;
-        on[i] = r < n && r != p;
+        role[i] = r < n ? -1 : -2;
+        for (int j = 0; j < nb; j++)
+          if (PJ[j] == r) role[i] = j;
       }
-#pragma unroll 2
       for (int c = lane; c < n; c += 32) {
-        const double2 a = prow[c];
-        double2 v[4], fi[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) fi[i] = on[i] ? fcol[r0 + i * G] : make_double2(0.0, 0.0);
+        if (c >= k0 && c < k0 + nb) continue;
+        double2 v[4];
 #pragma unroll
         for (int i = 0; i < 4; i++)
-          v[i] = on[i] ? W[(size_t)(r0 + i * G) * ld + c] : make_double2(0.0, 0.0);
+          v[i] = role[i] == -2  ? make_double2(0.0, 0.0)
+                 : role[i] >= 0 ? Q[role[i] * n + c]
+                                : W[(size_t)(r0 + i * G) * ld + c];
+        for (int j = 0; j < nb; j++) {
+          const double2 a = Q[j * n + c];
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-          if (c == k) {
-            const double2 t = cmul(fi[i], inv);
-            v[i] = make_double2(-t.x, -t.y);
-          } else {
-            v[i].x -= fi[i].x * a.x - fi[i].y * a.y;
-            v[i].y -= fi[i].x * a.y + fi[i].y * a.x;
-          }
+          for (int i = 0; i < 4; i++)
+            if (role[i] != -2 && j > role[i]) sub(v[i], F[j * n + r0 + i * G], a);
         }
 #pragma unroll
         for (int i = 0; i < 4; i++)
-          if (on[i]) W[(size_t)(r0 + i * G) * ld + c] = v[i];
+          if (role[i] != -2) W[(size_t)(r0 + i * G) * ld + c] = v[i];
       }
     }
     gsync();
