@@ -216,9 +216,12 @@ size_t handle_bytes(const qmc2d_system *sys, const q2d::DevSys &hs, size_t ncoef
   b += al(c, 8) * 2 + al(c, 4) * 4 + al(1, 4);                           // branch scratch
   b += al(c * 2 * N, 8) * 2 + al(c * nt, 8) + al(c * np, 8) + al(c, 8);  // staging
   b += al(c * q2d::move_scratch_doubles(hs), 8) + al(np + 1, 8);
-  // determinants beyond shared memory (the B200's 227 KB opt-in per CTA)
+  // determinants beyond shared memory: qmc2d_create moves them to HBM when
+  // the walker exceeds the device's opt-in shared memory per block; this
+  // count is made without a device, at the B200's 227 KB
+  constexpr size_t kSmemOptinB200 = 232448;
   const size_t smem = std::max(q2d::move_smem_bytes(hs), q2d::eval_smem_bytes(hs));
-  if (hs.gmat || (hs.has_bf && smem + sizeof(q2d::DevSys) > 232448)) {
+  if (hs.gmat || (hs.has_bf && smem + sizeof(q2d::DevSys) > kSmemOptinB200)) {
     q2d::DevSys g = hs;
     g.gmat = 1;
     b += al(c * q2d::gmat_doubles(g), 8);
