@@ -110,7 +110,9 @@ def prepare_request(req, workdir):
     tables = importlib.import_module("2degas_b200.tables")
     d = os.path.join(workdir, f"req{req.rid}")
     bf = (0.2, 1.0 * req.rs, 0.6 * req.rs) if req.backflow else None
-    tables.make_run(d, "s", req.n_up, req.n_down, req.rs, backflow=bf)
+    # the optimised Ewald breakup: the plain split at alpha = 5/L is off by
+    # a few 1e-4 Ry per electron, more than the error bars served here
+    tables.make_run(d, "s", req.n_up, req.n_down, req.rs, backflow=bf, ewald="fitpn")
     s = q.System.read(d, "s")
     return Prepared(req, s, s.footprint(req.walkers), d)
 

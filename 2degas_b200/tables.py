@@ -270,8 +270,10 @@ def closed_shells(limit=200):
 
 
 def make_run(directory, runid, n_up, n_down, rs, nknots=1000, backflow=None, u3=False,
-             alpha_L=5.0, nmax2=37, twist=False, nconf=0, seed=1):
-    """Write the run directory; returns its path. backflow = (lam, r0_bohr, w_bohr)."""
+             alpha_L=5.0, nmax2=37, twist=False, nconf=0, seed=1, ewald="erfc"):
+    """Write the run directory; returns its path. backflow = (lam, r0_bohr, w_bohr).
+    ewald: "erfc" (the plain split above) or "fitpn" (the setup program's
+    optimised breakup, breakup.py, over the same k vectors)."""
     os.makedirs(directory, exist_ok=True)
     N = n_up + n_down
     L = math.sqrt(N * math.pi)
@@ -309,8 +311,22 @@ def make_run(directory, runid, n_up, n_down, rs, nknots=1000, backflow=None, u3=
     kn = np.sqrt((kv ** 2).sum(1))
     vk = e2 * 2.0 * math.pi * np.array([math.erfc(k / (2 * alpha)) for k in kn]) / (kn * L * L)
     v0 = -e2 * (N * alpha / math.sqrt(math.pi) + N * N * math.sqrt(math.pi) / (alpha * L * L))
-    write_table(os.path.join(directory, f"{runid}.v"), hermite_table(f, df, drt), drt, "ewald",
-                [alpha], kspace=(vk, 0.0))
+    if ewald == "fitpn":
+        # the k-space list of the fit covers exactly the shells of the k file
+        from . import breakup
+
+        n2 = sorted({int(round((x * x + y * y) * (L / (2.0 * math.pi)) ** 2)) for x, y in kv})
+        kcut = 2.0 * math.pi / L * math.sqrt(n2[-1])
+        fit = breakup.ewald_fitpn(N, rs, nknots, cutk=max(8.0, 1.5 * kcut), nlamb=len(n2))
+        text, v0n = breakup.v_table_text(fit, N, drt, ifv0=1)
+        with open(os.path.join(directory, f"{runid}.v"), "w") as fh:
+            fh.write(text)
+        v0 = v0n * N
+    elif ewald == "erfc":
+        write_table(os.path.join(directory, f"{runid}.v"), hermite_table(f, df, drt), drt,
+                    "ewald", [alpha], kspace=(vk, 0.0))
+    else:
+        raise ValueError(f"ewald must be 'erfc' or 'fitpn', not {ewald!r}")
     with open(os.path.join(directory, f"{runid}.k"), "w") as fh:
         for k in kv:
             fh.write(f" {_f(k[0])} {_f(k[1])}\n")

@@ -5,6 +5,8 @@ n26/ (N=26, 13 up + 13 down, r_s=1), with its input files, spline tables and
 the outputs of one VMC block: n26.res (block sums, final RNG state, twist)
 and n26.{up,down}.x.res.0 (the final configuration of rank 0). The
 10,000-configuration start files n26.{up,down}.x.0 are inside n26.tar.gz.
+te.vrk is the setup program's intermediate Ewald-breakup file for the same
+deck.
 
 This script copies the text inputs and golden outputs verbatim and keeps
 only the first NCONF start configurations, so the fixtures stay small. It is
@@ -24,6 +26,9 @@ COPY = [
     "n26.sy", "n26.sy_vmc", "n26.in", "n26.u2", "n26.u3", "n26.b", "n26.v", "n26.k",
     "seed", "runid", "n26.res", "n26.up.x.res.0", "n26.down.x.res.0",
     "n26.up.x.res.1", "n26.down.x.res.1", "n26.rhok_up", "n26.rhok_down",
+    # the setup program's Ewald breakup for this deck (fitpn's table, from
+    # which traduci wrote n26.v)
+    "te.vrk",
 ]
 
 
