@@ -18,7 +18,9 @@ reference's `spline`, reptation.f:5223-5245, last knot zeroed):
     v   plain 2D Ewald: r v_sr(r) = e^2 erfc(alpha r), iexp = 1, with the
         k-space list v_k = e^2 2 pi erfc(k/(2 alpha)) / (k L^2) over the
         half-space k vectors and v0 = -e^2 (N alpha/sqrt(pi)
-        + N^2 sqrt(pi)/(alpha L^2)) (self + neutralising background).
+        + N^2 sqrt(pi)/(alpha L^2)) (self + neutralising background);
+        or, with ewald="fitpn", the setup program's optimised breakup over
+        the same k vectors (breakup.py).
 The k vectors are listed as the reference's krlv lists them. The
 reference's own table generators are restated too: tgen with u2_ob_cos,
 u2_reatto and eta_yk, which regenerate tables the reference wrote from the
