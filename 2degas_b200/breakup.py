@@ -188,9 +188,13 @@ def ewald_fitpn(N, rs, nt, cutk=8.0, npoly=10, argek=14.0, nlamb=18):
     v2 = v2 * (x - 1.0) ** npow + npow * (x - 1.0) ** (npow - 1) * v1
     v1 = v1 * (x - 1.0) ** npow
     mult = [int(0.5 * w[s] + 1e-4) for s in range(1, nlamb + 1)]
-    return dict(r=rv, v=v1, dv=v2 / a, self_energy=(-1.0) ** npow * (b[1] - npow * b[0]),
-                constant=vk[0], vk_shells=vk[1:nlamb + 1], mult=mult, k=k[:nlamb + 1],
-                poly=b, rms=rms, nk=len(k), a=a)
+    self_energy = (-1.0) ** npow * (b[1] - npow * b[0])
+    # fitpn's check of the split: the self energy plus the weighted sum of
+    # the k-space remainders over every fitted point (the Madelung energy)
+    madelung = self_energy + float(w @ vk)
+    return dict(r=rv, v=v1, dv=v2 / a, self_energy=self_energy, constant=vk[0],
+                vk_shells=vk[1:nlamb + 1], mult=mult, k=k[:nlamb + 1], poly=b, rms=rms,
+                nk=len(k), a=a, madelung=madelung)
 
 
 def hermite_rows(v, dv, drt):

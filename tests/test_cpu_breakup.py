@@ -19,6 +19,10 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden", "n26")
 TE_OS_NK = 91
 TE_OS_RMS = 3.94776845e-07
 TE_OS_POLY = [-0.442587, -0.130688, 0.935727, 0.689471, -0.838311, -1.13999, 0.913706]
+TE_OS_K = [0.0, 0.695213598, 0.983180499, 1.3904272, 1.55454486, 1.966361, 2.08564079,
+           2.19845843, 2.50662827, 2.78085439, 2.8664391, 2.9495415, 3.10908973,
+           3.47606799, 3.5449077, 3.7438398, 3.932722, 4.05375705, 4.17128159]
+TE_OS_MADELUNG = -0.86310248  # "computed madelung constant"
 
 
 @pytest.fixture(scope="module")
@@ -29,6 +33,8 @@ def fit():
 def test_fit_reproduces_the_reference_vrk(fit):
     g = breakup.read_vrk(os.path.join(GOLD, "te.vrk"))
     assert fit["nk"] == TE_OS_NK
+    assert np.allclose(fit["k"], TE_OS_K, rtol=1e-8, atol=0)
+    assert fit["madelung"] == pytest.approx(TE_OS_MADELUNG, rel=1e-7)
     assert fit["rms"] == pytest.approx(TE_OS_RMS, rel=1e-6)
     assert np.allclose(fit["poly"], TE_OS_POLY, rtol=2e-5, atol=0)
     # te.vrk holds 9 significant digits
