@@ -95,6 +95,22 @@ def _ewald(x, L, e2, alpha, nimg=3, kmax=14):
     return e2 * (E + 0.5 * N * xi) / N
 
 
+def test_fitpn_deck_at_the_benchmark_shell(tmp_path):
+    """N = 58 at r_s = 5 (the fit's shells and grid scale with the cell):
+    within 1e-8 Ry per electron of the independent sum."""
+    q = importlib.import_module("2degas_b200")
+    tables = importlib.import_module("2degas_b200.tables")
+    from oracle_lib import Oracle
+
+    d = tables.make_run(str(tmp_path / "f58"), "c", 29, 29, 5.0, nconf=1, seed=5,
+                        ewald="fitpn")
+    s = q.System.read(d, "c")
+    x = s.read_configs(d, ".0", 0, 1)
+    pot = Oracle(s.ptr).compute_properties(x[0])[2][q._capi.JPOT0]
+    L = math.sqrt(58 * math.pi)
+    assert abs(pot - _ewald(x[0].reshape(-1, 2), L, 0.4, 4.0 / L)) < 1e-8
+
+
 def test_fitpn_deck_gives_the_ewald_potential(tmp_path):
     q = importlib.import_module("2degas_b200")
     tables = importlib.import_module("2degas_b200.tables")
