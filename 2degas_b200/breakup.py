@@ -235,8 +235,8 @@ def read_vrk(path):
     """The setup program's intermediate file (te.vrk: writetb's r table,
     then the self, constant and k-space energies). Returns a dict like
     ewald_fitpn's, with the k-space values already expanded."""
-    toks = open(path).read().split("\n")
-    lines = [t.strip() for t in toks]
+    with open(path) as fh:
+        lines = [t.strip() for t in fh.read().split("\n")]
     n = int(lines[0].split()[2])
     i = 3
     v = np.array([float(x) for x in lines[i:i + n]])
