@@ -197,6 +197,40 @@ def ewald_fitpn(N, rs, nt, cutk=8.0, npoly=10, argek=14.0, nlamb=18):
                 nk=len(k), a=a, madelung=madelung)
 
 
+def madelung(L, e2, p=1.0, ndim=2):
+    """Madelung energy of one charge in the square (cubic) lattice of side
+    L for an r^-p interaction, e2 times the Ewald sum with the splitting
+    alpha = pi / vol^(2/ndim) (mdlng, setup.f:996-1031): the real-space
+    images weighted by Gamma(p/2, alpha r^2) / Gamma(p/2), the reciprocal
+    ones by Gamma((ndim-p)/2, k^2/(4 alpha)), over |n_l| <= 3 in every
+    direction, plus the self and background terms. The upper incomplete
+    gamma function is scipy's (the reference evaluates it with its own
+    series and continued fraction, gammi)."""
+    from scipy.special import gamma, gammaincc
+
+    def ginc(a, x):
+        return gammaincc(a, x) * gamma(a)
+
+    limit = int(1 + math.sqrt(-math.log(1e-9) / math.pi))
+    vol = L ** ndim
+    alpha = math.pi * vol ** (-2.0 / ndim)
+    g0 = gamma(0.5 * p)
+    v = (-2.0 * alpha ** (0.5 * p) / (p * g0)
+         - 2.0 * math.pi ** (0.5 * ndim) / ((ndim - p) * vol * g0 * alpha ** (0.5 * (ndim - p))))
+    rng = range(-limit, limit + 1)
+    pts = [(i, j) for j in rng for i in rng] if ndim == 2 else \
+        [(i, j, l) for l in rng for j in rng for i in rng]
+    for n in pts:
+        r2 = sum((c * L) ** 2 for c in n)
+        if r2 <= 0:
+            continue
+        rk2 = sum((2.0 * math.pi * c / L) ** 2 for c in n)
+        v += (math.pi ** (0.5 * ndim) * (4.0 / rk2) ** (0.5 * (ndim - p))
+              * ginc(0.5 * (ndim - p), rk2 / (4.0 * alpha)) / (vol * g0)
+              + ginc(0.5 * p, alpha * r2) / (g0 * r2 ** (0.5 * p)))
+    return v * e2
+
+
 def hermite_rows(v, dv, drt):
     """traduci's table (pspline, setup.f:2316-2327): per knot the value, the
     derivative times drt and the cubic's two higher coefficients from the

@@ -23,6 +23,7 @@ TE_OS_K = [0.0, 0.695213598, 0.983180499, 1.3904272, 1.55454486, 1.966361, 2.085
            2.19845843, 2.50662827, 2.78085439, 2.8664391, 2.9495415, 3.10908973,
            3.47606799, 3.5449077, 3.7438398, 3.932722, 4.05375705, 4.17128159]
 TE_OS_MADELUNG = -0.86310248  # "computed madelung constant"
+TE_OS_IDEAL = -0.863102734  # "ideal square madelung constant" (closed form and mdlng)
 
 
 @pytest.fixture(scope="module")
@@ -45,6 +46,13 @@ def test_fit_reproduces_the_reference_vrk(fit):
     vk = np.array([v for v, m in zip(fit["vk_shells"], fit["mult"]) for _ in range(m)])
     assert len(vk) == len(g["vk"]) == 56
     assert np.abs(vk - g["vk"]).max() < 1e-10
+
+
+def test_madelung_of_the_square_lattice():
+    L = math.sqrt(26 * math.pi)
+    v = breakup.madelung(L, 2.0)
+    assert v == pytest.approx(TE_OS_IDEAL, rel=1e-8)
+    assert v == pytest.approx(-3.90026492 * 2.0 / L, rel=1e-8)  # ocpset's closed form
 
 
 def test_traduci_reproduces_the_reference_v_table():
