@@ -16,6 +16,13 @@ library's stream (inputs resident in HBM, L2 flushed between steps);
 copied from and to pinned host memory every step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Other workloads (not the headline line): --shell NU,ND [--rs R] runs the
+same DMC generation on another closed shell (up to 81 + 81 or 161
+polarised); --workload batch times 64 uneven populations through
+qmc2d_batch_dmc (--batch-lanes sweeps the populations in flight);
+--workload serve runs the serving stream; --phases prints the move
+kernel's per-phase SM cycles instead of timing.
 """
 import argparse
 import json
