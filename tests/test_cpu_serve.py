@@ -107,3 +107,15 @@ def test_poisson_stream_and_summary():
     sm = serve.summary(res)
     assert sm["p50_s"] == pytest.approx(50.5) and sm["p99_s"] == pytest.approx(99.01)
     assert sm["walker_moves_per_s"] == pytest.approx(1000 / 100.0)
+
+
+def test_requests_are_prepared_on_the_host_with_the_optimised_breakup(tmp_path):
+    import importlib
+    import os
+
+    serve = importlib.import_module("2degas_b200.serve")
+    small = serve.prepare_request(serve.Request(13, 13, 2.0, walkers=512, rid=0), str(tmp_path))
+    large = serve.prepare_request(serve.Request(81, 81, 3.0, walkers=512, rid=1), str(tmp_path))
+    assert 0 < small.footprint < large.footprint
+    with open(os.path.join(small.directory, "s.v")) as fh:
+        assert "fitpn" in fh.read().split("\n")[1002]
