@@ -175,12 +175,18 @@ typedef struct qmc2d_options {
   uint64_t seed;         /* Philox key for the device random streams */
 } qmc2d_options;
 
-/* Copy the system's tables to the device and allocate walker storage. */
+/* Copy the system's tables to the device and allocate walker storage.
+ * When one walker's evaluation does not fit a CTA's shared memory (backflow
+ * determinants above 45 electrons per spin unpolarised, 49 polarised), each
+ * walker slot also gets a block of device memory for its determinant
+ * matrices; QMC2D_ERR_LIMIT only if the rest does not fit either. */
 int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt, qmc2d_handle **out);
 int qmc2d_destroy(qmc2d_handle *h);
 /* Device memory (bytes, each allocation rounded to 512) that qmc2d_create
  * would allocate for sys at this capacity, computed on the host without a
- * GPU; reptation storage (qmc2d_rmc_init) is not included. For admitting
+ * GPU (the per-walker determinant blocks included, sized for the B200's
+ * 227 KB of shared memory per CTA); reptation storage (qmc2d_rmc_init) is
+ * not included. For admitting
  * work by HBM footprint; the reference has no counterpart (it allocates
  * its COMMON blocks statically). */
 int qmc2d_footprint(const qmc2d_system *sys, int capacity, uint64_t *bytes);
