@@ -146,6 +146,10 @@ class Handle:
         self._chk(self.lib.qmc2d_compute_properties_dev(self.h, nw, x_ptr, g_ptr, h_ptr, p_ptr,
                                                         s_ptr, stream))
 
+    def compute_properties_dev_status(self, nw, stream=None):
+        """Wait for the last compute_properties_dev and raise on a failed walker."""
+        self._chk(self.lib.qmc2d_compute_properties_dev_status(self.h, nw, stream))
+
     def population_set(self, x):
         x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float64)
         self._chk(self.lib.qmc2d_population_set(self.h, x.shape[0], _pd(x)))

@@ -186,6 +186,8 @@ SIGNATURES = {
                                              c_void_p, c_void_p, c_void_p]),
     "qmc2d_compute_properties_noalloc": (c_int, [SYSP, c_int, c_void_p, c_void_p, c_void_p,
                                                  c_void_p, c_void_p, c_void_p]),
+    "qmc2d_compute_properties_noalloc_status": (c_int, [c_int, c_void_p]),
+    "qmc2d_compute_properties_dev_status": (c_int, [c_void_p, c_int, c_void_p]),
     "qmc2d_population_set": (c_int, [c_void_p, c_int, PD]),
     "qmc2d_population_size": (c_int, [c_void_p, POINTER(c_int)]),
     "qmc2d_population_get": (c_int, [c_void_p, PD, PD, PD, PD, PD, PD]),

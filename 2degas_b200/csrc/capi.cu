@@ -522,10 +522,21 @@ extern "C" int qmc2d_compute_properties_dev(qmc2d_handle *h, int nw, const doubl
   }
   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
   CK(cudaSetDevice(h->device));
+  if (nw > 0) CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * nw, st));
   ProfScope ps(h, QMC2D_KERNEL_EVAL, st);
   CK(q2d::launch_eval(h->hs, h->ds, nw, x_dev, g_dev, hl_dev, props_dev, s_dev, h->d_status,
                       st));
   return QMC2D_OK;
+}
+
+extern "C" int qmc2d_compute_properties_dev_status(qmc2d_handle *h, int nw, void *stream) {
+  if (!h || nw < 0 || nw > h->cap) {
+    q2d::set_error("qmc2d_compute_properties_dev_status: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  if (stream) CK(cudaStreamSynchronize((cudaStream_t)stream));
+  return sync_status(h, nw);
 }
 
 extern "C" int qmc2d_compute_properties(qmc2d_handle *h, int nw, const double *x, double *g,

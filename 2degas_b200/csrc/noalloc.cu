@@ -85,6 +85,32 @@ extern "C" int qmc2d_compute_properties_noalloc(const qmc2d_system *sys, int nw,
     q2d::set_error("qmc2d_compute_properties_noalloc: unsupported system size");
     return QMC2D_ERR_LIMIT;
   }
+  // Every array the copies below read must be there: a missing one would
+  // leave the previous call's contents of the shared array in its place.
+  if ((sys->nk > 0 && !sys->kvec) || (sys->ngvec > 0 && !sys->gvec) || sys->ntables < 0 ||
+      sys->ntables > QMC2D_MAX_TABLES) {
+    q2d::set_error("qmc2d_compute_properties_noalloc: system without its k or wave vectors");
+    return QMC2D_ERR_ARG;
+  }
+  for (int t = 0; t < sys->ntables; t++)
+    if (!sys->tables[t].ut || (sys->tables[t].nk_ewald > 0 && !sys->tables[t].vk)) {
+      q2d::set_error("qmc2d_compute_properties_noalloc: table without coefficients");
+      return QMC2D_ERR_ARG;
+    }
+  // The copies below read pageable host memory that is gone when the call
+  // returns; a captured graph would replay them from freed memory.
+  {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t ce = cudaStreamIsCapturing((cudaStream_t)stream, &cap);
+    if (ce != cudaSuccess) {
+      q2d::set_error(std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(ce));
+      return QMC2D_ERR_CUDA;
+    }
+    if (cap != cudaStreamCaptureStatusNone) {
+      q2d::set_error("qmc2d_compute_properties_noalloc: not allowed while the stream is captured");
+      return QMC2D_ERR_ARG;
+    }
+  }
   // The device view of the system, built on the stack; offsets count doubles
   // from the start of the scratch array.
   q2d::DevSys s;
@@ -169,6 +195,29 @@ extern "C" int qmc2d_compute_properties_noalloc(const qmc2d_system *sys, int nw,
     q2d::set_error(buf);
     return QMC2D_ERR_LIMIT;
   }
+  // One walker's evaluation must fit one CTA's shared memory: there is no
+  // room here for the per-walker determinant blocks that a handle puts in
+  // device memory for larger shells.
+  {
+    int dev = 0, optin = 0;
+    cudaError_t ce = cudaGetDevice(&dev);
+    if (ce == cudaSuccess)
+      ce = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (ce != cudaSuccess) {
+      q2d::set_error(std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(ce));
+      return QMC2D_ERR_CUDA;
+    }
+    const size_t need = q2d::eval_smem_bytes(s) + sizeof(q2d::DevSys);
+    if (need > (size_t)optin) {
+      char buf[200];
+      std::snprintf(buf, sizeof buf,
+                    "qmc2d_compute_properties_noalloc: one walker needs %zu bytes of shared "
+                    "memory, the device gives %d (determinants this large need a handle)",
+                    need, optin);
+      q2d::set_error(buf);
+      return QMC2D_ERR_LIMIT;
+    }
+  }
   double *base = nullptr;
   int st = scratch_address(&base);
   if (st) return st;
@@ -213,5 +262,43 @@ extern "C" int qmc2d_compute_properties_noalloc(const qmc2d_system *sys, int nw,
   if ((e = q2d::launch_eval(s, reinterpret_cast<const q2d::DevSys *>(base), nw, x_dev, g_dev,
                             hl_dev, props_dev, s_dev, status, cs)) != cudaSuccess)
     return fail(e, "eval kernel");
+  return QMC2D_OK;
+}
+
+// Status of the last qmc2d_compute_properties_noalloc call: waits for
+// `stream`, then ORs the first nw per-walker status words of the shared
+// array, 1024 at a time through a buffer on the host stack.
+extern "C" int qmc2d_compute_properties_noalloc_status(int nw, void *stream) {
+  if (nw < 0 || nw > kMaxWalkers) {
+    q2d::set_error("qmc2d_compute_properties_noalloc_status: bad walker count");
+    return QMC2D_ERR_ARG;
+  }
+  double *base = nullptr;
+  int st = scratch_address(&base);
+  if (st) return st;
+  cudaStream_t cs = (cudaStream_t)stream;
+  const int *status = reinterpret_cast<const int *>(base + (kScratchDoubles - kStatusDoubles));
+  int words[1024];
+  int any = 0;
+  cudaError_t e = cudaStreamSynchronize(cs);
+  for (int i = 0; e == cudaSuccess && i < nw; i += 1024) {
+    const int n = nw - i < 1024 ? nw - i : 1024;
+    e = cudaMemcpyAsync(words, status + i, sizeof(int) * n, cudaMemcpyDeviceToHost, cs);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+    for (int k = 0; e == cudaSuccess && k < n; k++) any |= words[k];
+  }
+  if (e != cudaSuccess) {
+    q2d::set_error(std::string("qmc2d_compute_properties_noalloc_status: ") +
+                   cudaGetErrorString(e));
+    return QMC2D_ERR_CUDA;
+  }
+  if (any & q2d::ST_SINGULAR) {
+    q2d::set_error("zero pivot in a Slater matrix");
+    return QMC2D_ERR_SINGULAR;
+  }
+  if (any & q2d::ST_NONFINITE) {
+    q2d::set_error("non-finite local energy or -ln psi");
+    return QMC2D_ERR_NONFINITE;
+  }
   return QMC2D_OK;
 }

@@ -267,6 +267,11 @@ int qmc2d_compute_properties(qmc2d_handle *h, int nw, const double *x,
 int qmc2d_compute_properties_dev(qmc2d_handle *h, int nw, const double *x_dev,
                                  double *g_dev, double *hlap_dev, double *props_dev,
                                  double *s_dev, void *stream);
+/* Status of the last qmc2d_compute_properties_dev call on nw walkers: waits
+ * for `stream` (NULL: the handle's stream) and reports QMC2D_ERR_SINGULAR
+ * or QMC2D_ERR_NONFINITE if any walker had a zero pivot or a non-finite
+ * result (the reference stops there, reptation.f:10318), else QMC2D_OK. */
+int qmc2d_compute_properties_dev_status(qmc2d_handle *h, int nw, void *stream);
 
 /* No counterpart in the reference. The same evaluation as
  * qmc2d_compute_properties_dev for callers that cannot allocate device
@@ -279,13 +284,25 @@ int qmc2d_compute_properties_dev(qmc2d_handle *h, int nw, const double *x_dev,
  * and outputs; the call is asynchronous on `stream` (NULL: the legacy default
  * stream). Limits: at most 65536 walkers per call and tables, k vectors and
  * orbital wave vectors of at most 229376 doubles together; larger requests
- * return QMC2D_ERR_LIMIT. The first call on a device looks up the array's
- * device address, so make that first call before any stream capture. All
+ * return QMC2D_ERR_LIMIT, and so does a system whose determinants are too
+ * large for one CTA's shared memory (backflow above 45 electrons per spin
+ * unpolarised, 49 polarised: a handle keeps those in device memory it
+ * allocates). The call copies the system from pageable host memory, so it
+ * must never be made while `stream` is being captured into a CUDA graph
+ * (QMC2D_ERR_ARG). The first call on a device looks up the array's
+ * device address. All
  * calls share the array: calls that overlap on the GPU (other streams, other
  * threads) race on it and must be serialised by the caller. */
 int qmc2d_compute_properties_noalloc(const qmc2d_system *sys, int nw, const double *x_dev,
                                      double *g_dev, double *hlap_dev, double *props_dev,
                                      double *s_dev, void *stream);
+/* No counterpart in the reference. Status of the last
+ * qmc2d_compute_properties_noalloc call on nw walkers, read from the same
+ * fixed array without allocating device memory: waits for `stream`, then
+ * returns QMC2D_ERR_SINGULAR or QMC2D_ERR_NONFINITE if any walker had a
+ * zero pivot or a non-finite result, else QMC2D_OK. A later call on the
+ * array overwrites the words, so read them before the next call. */
+int qmc2d_compute_properties_noalloc_status(int nw, void *stream);
 
 /* ---------------------------------------------------------- populations
  * A population is the reference's walker stack (x_stack, g_stack, h_stack,

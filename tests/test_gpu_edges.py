@@ -82,3 +82,26 @@ def test_bad_configurations_are_status_codes(q, oracle_cls, n26, n26_configs):
     for k in range(4):
         go, ho, po, so, _ = o.compute_properties(x[k])
         assert close(p[k], po) < 1e-10
+
+
+def test_device_entry_point_reports_failed_walkers(q, n26, n26_configs):
+    """compute_properties_dev is asynchronous; its status words come back
+    through compute_properties_dev_status, cleared at every call."""
+    import ctypes
+
+    import torch
+
+    x = n26_configs[:4].copy()
+    x[1, 5] = np.nan
+    xd = torch.tensor(x, dtype=torch.float64, device="cuda")
+    out = [torch.zeros(4 * k, dtype=torch.float64, device="cuda")
+           for k in (2 * n26.N, n26.ntypes, n26.nprops, 1)]
+    ptrs = [ctypes.c_void_p(t.data_ptr()) for t in [xd] + out]
+    with q.Handle(n26, capacity=4, seed=1) as h:
+        torch.cuda.synchronize()
+        h.compute_properties_dev(4, *ptrs)
+        _expect(q, lambda: h.compute_properties_dev_status(4), (ERR_NONFINITE,))
+        xd.copy_(torch.tensor(n26_configs[:4], dtype=torch.float64))
+        torch.cuda.synchronize()
+        h.compute_properties_dev(4, *ptrs)
+        h.compute_properties_dev_status(4)
