@@ -33,9 +33,11 @@ def _pd(a):
 class System:
     """A qmc2d_system read from a reference run directory (input, t_read, kread)."""
 
-    def __init__(self, ptr, lib):
+    def __init__(self, ptr, lib, directory=None, runid=None):
         self.ptr = ptr
         self.lib = lib
+        self.directory, self.runid = directory, runid
+        self.twist = None  # (ith, jth) after set_twist; None: as read
 
     @classmethod
     def read(cls, directory, runid):
@@ -43,7 +45,7 @@ class System:
         sp = _capi.SYSP()
         _capi.check(lib, lib.qmc2d_system_read(str(directory).encode(), runid.encode(),
                                                ctypes.byref(sp)))
-        return cls(sp, lib)
+        return cls(sp, lib, str(directory), runid)
 
     def __del__(self):
         try:
@@ -71,6 +73,7 @@ class System:
 
     def set_twist(self, ith, jth):
         _capi.check(self.lib, self.lib.qmc2d_system_set_twist(self.ptr, ith, jth))
+        self.twist = (ith, jth)
 
     def rmc_estimators_setup(self, ntau, ntauskip):
         """mstar/cmass/itc setup of the deck's records for ntau-bead paths."""

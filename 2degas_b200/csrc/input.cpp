@@ -118,6 +118,12 @@ int finish(qmc2d_system *s) {
   bool backflow = s->iub[0][0] >= 0;
   if (backflow) {
     if (s->nk <= 0) return fail(QMC2D_ERR_PARSE, "backflow needs kspace");
+    // input builds the Gamma-point wave vectors only when ibckf != 0
+    // (reptation.f:679): with ibckf 0 and no twists every orbital would be
+    // the k = 0 constant and the determinant singular
+    if (s->ntheta == 0 && s->ibckf == 0)
+      return fail(QMC2D_ERR_UNSUPPORTED,
+                  "backflow with ibckf 0 at the Gamma point: no orbital wave vectors");
     for (int it = 0; it < s->ntypes; it++)
       if (s->np[it] > QMC2D_MAX_ORB || s->np[it] > 2 * s->nk + 1)
         return fail(QMC2D_ERR_LIMIT, "not enough orbitals for the determinant");

@@ -101,12 +101,12 @@ def _cpu_worker(args):
     """One host process: the oracle's DMC on its own sub-population for
     `seconds` of wall time; returns walker-moves done and seconds."""
     d, nw, seed, seconds, delta, etrial = args
-    q = importlib.import_module("2degas_b200")
-    from oracle_lib import Oracle
+    from oracle_lib import Oracle, OracleSystem
 
-    s = q.System.read(d, "c")
+    # the oracle reads the deck itself: this process loads only liboracle.so
+    s = OracleSystem.read(d, "c")
     x = s.read_configs(d, ".0", 0, nw)
-    o = Oracle(s.ptr)
+    o = Oracle(s)
     pop = o.population_init(x)
     o.vmc_philox(pop, 2, delta, 10 ** 9, seed, 0)
     t0 = time.perf_counter()

@@ -46,6 +46,18 @@ void oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t
 void oracle_philox_uniform2(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c2,
                             uint32_t c3, double u[2]);
 
+/* ---- the oracle's own reader of a run directory (oracle_input.c): input,
+ * readwords, t_read, kread, twistg/SORTTF and read_conf restated
+ * (reptation.f:12-708, 4689-4842, 9514, 9818, 2452). Independent of the
+ * product library's reader; the data layout is include/qmc2d.h's. */
+int oracle_system_read(const char *dir, const char *runid, qmc2d_system **out);
+void oracle_system_free(qmc2d_system *sys);
+/* Orbital wave vectors of twist (ith, jth); 0, 0: the Gamma-point list. */
+int oracle_system_set_twist(qmc2d_system *sys, int ith, int jth);
+int oracle_read_configs(const qmc2d_system *sys, const char *dir, const char *suffix,
+                        int first, int count, double *x, int *nread);
+void oracle_system_sizes(const qmc2d_system *sys, int *nptot, int *ntypes, int *n_props);
+
 /* ---- per-evaluation scratch (the reference's /c_dist/, /scratch/ commons) */
 typedef struct oracle_work oracle_work;
 oracle_work *oracle_work_new(const qmc2d_system *sys);

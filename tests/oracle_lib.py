@@ -26,12 +26,77 @@ def _ptr(a):
     return a.ctypes.data_as(PD)
 
 
+def _load():
+    if not os.path.exists(ORACLE_SO):
+        build()
+    lib = ctypes.CDLL(ORACLE_SO)
+    lib.oracle_system_read.restype = c_int
+    lib.oracle_system_read.argtypes = [ctypes.c_char_p, ctypes.c_char_p, POINTER(c_void_p)]
+    lib.oracle_system_free.argtypes = [c_void_p]
+    lib.oracle_system_set_twist.restype = c_int
+    lib.oracle_system_set_twist.argtypes = [c_void_p, c_int, c_int]
+    lib.oracle_read_configs.restype = c_int
+    lib.oracle_read_configs.argtypes = [c_void_p, ctypes.c_char_p, ctypes.c_char_p, c_int, c_int,
+                                        PD, PI]
+    lib.oracle_system_sizes.argtypes = [c_void_p, PI, PI, PI]
+    return lib
+
+
+class OracleSystem:
+    """A run directory read by the oracle's own reader (oracle_input.c),
+    independently of the product library's qmc2d_system_read."""
+
+    def __init__(self, directory, runid, twist=None):
+        self.lib = _load()
+        self.ptr = c_void_p()
+        self.directory, self.runid = str(directory), runid
+        st = self.lib.oracle_system_read(self.directory.encode(), runid.encode(),
+                                         ctypes.byref(self.ptr))
+        if st:
+            raise RuntimeError(f"oracle reader: status {st} on {directory}/{runid}.sy")
+        if twist is not None:
+            self.set_twist(*twist)
+        n, t, p = c_int(), c_int(), c_int()
+        self.lib.oracle_system_sizes(self.ptr, ctypes.byref(n), ctypes.byref(t), ctypes.byref(p))
+        self.N, self.ntypes, self.nprops = n.value, t.value, p.value
+
+    @classmethod
+    def read(cls, directory, runid):
+        return cls(directory, runid)
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                self.lib.oracle_system_free(self.ptr)
+                self.ptr = c_void_p()
+        except Exception:
+            pass
+
+    def set_twist(self, ith, jth):
+        st = self.lib.oracle_system_set_twist(self.ptr, ith, jth)
+        if st:
+            raise RuntimeError(f"oracle set_twist: status {st}")
+
+    def read_configs(self, directory, suffix, first, count):
+        x = np.zeros((count, 2 * self.N))
+        n = c_int(0)
+        st = self.lib.oracle_read_configs(self.ptr, str(directory).encode(), suffix.encode(),
+                                          first, count, _ptr(x), ctypes.byref(n))
+        if st:
+            raise RuntimeError(f"oracle read_configs: status {st}")
+        return x[: n.value]
+
+
 class Oracle:
-    def __init__(self, sysp):
-        """sysp: ctypes POINTER(System) from qmc2d_system_read."""
-        if not os.path.exists(ORACLE_SO):
-            build()
-        self.lib = lib = ctypes.CDLL(ORACLE_SO)
+    def __init__(self, system):
+        """system: an OracleSystem, or any object with `directory`, `runid`
+        and `twist` (the product's System): the oracle then reads the same run
+        directory itself and sets the same twist."""
+        if not isinstance(system, OracleSystem):
+            system = OracleSystem(system.directory, system.runid,
+                                  getattr(system, "twist", None))
+        self.system = system
+        self.lib = lib = _load()
         lib.oracle_work_new.restype = c_void_p
         lib.oracle_work_new.argtypes = [c_void_p]
         lib.oracle_work_free.argtypes = [c_void_p]
@@ -66,12 +131,10 @@ class Oracle:
         lib.oracle_savern.argtypes = [c_void_p, PI]
         lib.oracle_rannyu.restype = c_double
         lib.oracle_rannyu.argtypes = [c_void_p]
-        self.sysp = sysp
-        s = sysp.contents
-        self.N = s.nptot
-        self.nt = s.ntypes
-        self.nprops = s.n_props
-        self.work = lib.oracle_work_new(ctypes.cast(sysp, c_void_p))
+        self.N = system.N
+        self.nt = system.ntypes
+        self.nprops = system.nprops
+        self.work = lib.oracle_work_new(system.ptr)
 
     def __del__(self):
         try:
@@ -81,7 +144,7 @@ class Oracle:
 
     @property
     def _s(self):
-        return ctypes.cast(self.sysp, c_void_p)
+        return self.system.ptr
 
     def compute_properties(self, x):
         """x: (2N,) float64 -> (g, h, p, s, underflow)."""

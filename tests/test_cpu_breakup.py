@@ -114,7 +114,7 @@ def test_fitpn_deck_at_the_benchmark_shell(tmp_path):
                         ewald="fitpn")
     s = q.System.read(d, "c")
     x = s.read_configs(d, ".0", 0, 1)
-    pot = Oracle(s.ptr).compute_properties(x[0])[2][q._capi.JPOT0]
+    pot = Oracle(s).compute_properties(x[0])[2][q._capi.JPOT0]
     L = math.sqrt(58 * math.pi)
     assert abs(pot - _ewald(x[0].reshape(-1, 2), L, 0.4, 4.0 / L)) < 1e-8
 
@@ -130,7 +130,7 @@ def test_fitpn_deck_gives_the_ewald_potential(tmp_path):
         d = tables.make_run(str(tmp_path / ew), "c", 13, 13, 1.0, nconf=2, seed=3, ewald=ew)
         s = q.System.read(d, "c")
         x = s.read_configs(d, ".0", 0, 2)
-        o = Oracle(s.ptr)
+        o = Oracle(s)
         pots[ew] = [o.compute_properties(x[k])[2][q._capi.JPOT0] for k in range(2)]
     for k in range(2):
         exact = _ewald(x[k].reshape(-1, 2), L, e2, 4.0 / L)

@@ -40,7 +40,7 @@ def fd_check(o, x, dx=1e-5):
 
 
 def test_drift_is_gradient_of_minus_log_psi(oracle_cls, n26, n26_configs):
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     for k in (0, 5):
         g, gfd, h, lap = fd_check(o, n26_configs[k].copy())
         assert np.abs(g - gfd).max() < 1e-6 * max(1.0, np.abs(g).max())
@@ -52,14 +52,14 @@ def test_drift_without_backflow_and_twist(oracle_cls, q, tmp_path, n26_configs):
 
     d = write_variant(tmp_path, "nb", backflow=False, ntwists=0)
     s = q.System.read(d, "nb")
-    o = oracle_cls(s.ptr)
+    o = oracle_cls(s)
     g, gfd, h, lap = fd_check(o, n26_configs[3].copy())
     assert np.abs(g - gfd).max() < 1e-6 * max(1.0, np.abs(g).max())
     assert np.abs(h - lap).max() < 1e-5 * max(1.0, np.abs(h).max())
 
 
 def test_spin_swap_and_translation(oracle_cls, n26, n26_configs):
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     x = n26_configs[2].copy()
     _, h, p, _, _ = o.compute_properties(x)
     xs = np.concatenate([x[26:], x[:26]])
@@ -73,7 +73,7 @@ def test_spin_swap_and_translation(oracle_cls, n26, n26_configs):
 
 
 def test_rannyu_is_the_48bit_lcg(oracle_cls, n26):
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     seed = [3535, 3467, 3262, 2 * 1549 + 1]
     draws, state = o.rannyu_stream(seed, 1000)
     m = (502 << 36) | (1521 << 24) | (4071 << 12) | 2107
@@ -124,7 +124,7 @@ def branch2_python(wate, r):
 
 
 def test_branch2_comb(oracle_cls, n26):
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     rng = np.random.default_rng(5)
     for trial in range(20):
         nw = int(rng.integers(5, 300))
@@ -139,7 +139,7 @@ def test_branch2_comb(oracle_cls, n26):
 
 def test_branch2_is_unbiased(oracle_cls, n26):
     """E[mult_i] = nw w_i / sum w for the systematic comb."""
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     rng = np.random.default_rng(9)
     nw = 40
     wate = rng.uniform(0.2, 3.0, nw)
@@ -164,7 +164,7 @@ def _vmc_block(args):
     q = importlib.import_module("2degas_b200")
     s = q.System.read(N26, "n26")
     x = s.read_configs(N26, ".0", 0, 1)[0]
-    o = Oracle(s.ptr)
+    o = Oracle(s)
     blk, xf, so, nacc = o.vmc_rannyu(x, 20000, 0.05, 200000, seed, 0)
     return blk[:14] / 20000.0
 
@@ -250,7 +250,7 @@ def test_minus_log_psi_against_numpy_slogdet(oracle_cls, q, tmp_path, deck):
                         backflow=(0.0, rs, 0.6 * rs))
     s = q.System.read(d, "c")
     x = s.read_configs(d, ".0", 0, 6)
-    o = oracle_cls(s.ptr)
+    o = oracle_cls(s)
     for k in range(len(x)):
         _, _, p, _, _ = o.compute_properties(x[k])
         want = _numpy_minus_log_psi(s, x[k])

@@ -53,7 +53,7 @@ def test_tgen_tables_run_through_the_reader(q, oracle_cls, tmp_path):
     s0 = q.System.read(N26, "n26")
     s1 = q.System.read(d, "n26")
     x = s0.read_configs(N26, ".0", 0, 4)
-    o0, o1 = oracle_cls(s0.ptr), oracle_cls(s1.ptr)
+    o0, o1 = oracle_cls(s0), oracle_cls(s1)
     for k in range(len(x)):
         _, _, p0, _, _ = o0.compute_properties(x[k])
         _, _, p1, _, _ = o1.compute_properties(x[k])

@@ -58,7 +58,7 @@ def deck(request, q, tmp_path):
 
 def test_evaluation_parity(q, oracle_cls, deck):
     name, s, x = deck
-    o = oracle_cls(s.ptr)
+    o = oracle_cls(s)
     with q.Handle(s, capacity=len(x), seed=3) as h:
         g, hl, p, sg = h.compute_properties(x)
     for k in range(len(x)):
@@ -73,7 +73,7 @@ def test_vmc_parity(q, oracle_cls, deck):
     name, s, x = deck
     nw, nstp = len(x), 3
     delta = 0.02 * CASES[name]["rs"] ** 2
-    o = oracle_cls(s.ptr)
+    o = oracle_cls(s)
     pop = o.population_init(x)
     blk_o, nacc_o = o.vmc_philox(pop, nstp, delta, 1000, SEED, 0)
     with q.Handle(s, capacity=nw, seed=SEED) as h:

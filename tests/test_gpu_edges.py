@@ -37,7 +37,7 @@ def small(q, tmp_path, request):
 
 def test_smallest_shells_match_the_oracle(q, oracle_cls, small):
     s, x, rs = small
-    o = oracle_cls(s.ptr)
+    o = oracle_cls(s)
     with q.Handle(s, capacity=len(x), seed=1) as h:
         g, hl, p, sg = h.compute_properties(x)
     for k in range(len(x)):
@@ -63,7 +63,7 @@ def _expect(q, call, codes):
 
 def test_bad_configurations_are_status_codes(q, oracle_cls, n26, n26_configs):
     x = n26_configs[:4].copy()
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     nan = x.copy()
     nan[1, 5] = np.nan
     inf = x.copy()

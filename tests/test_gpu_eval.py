@@ -24,7 +24,7 @@ def close(a, b, rtol=RTOL):
 
 
 def check_parity(q, oracle_cls, sysobj, x, rtol=RTOL):
-    o = oracle_cls(sysobj.ptr)
+    o = oracle_cls(sysobj)
     with q.Handle(sysobj, capacity=len(x), seed=7) as h:
         g, hl, p, s = h.compute_properties(x)
     for k in range(len(x)):

@@ -39,7 +39,7 @@ def large(q, tmp_path_factory, request):
 
 def test_properties_match_the_oracle(q, oracle_cls, large):
     s, x, _ = large
-    o = oracle_cls(s.ptr)
+    o = oracle_cls(s)
     with q.Handle(s, capacity=len(x), seed=1) as h:
         g, hl, p, sg = h.compute_properties(x)
     for k in range(len(x)):
@@ -50,7 +50,7 @@ def test_properties_match_the_oracle(q, oracle_cls, large):
 
 def test_vmc_and_dmc_match_the_oracle(q, oracle_cls, large):
     s, x, rs = large
-    o = oracle_cls(s.ptr)
+    o = oracle_cls(s)
     delta = 0.01 * rs * rs
     ref = o.population_init(x)
     _, nacc = o.vmc_philox(ref, 2, delta, 1000, SEED, 0)

@@ -47,7 +47,7 @@ def _deck(q, tmp_path, name):
 @pytest.mark.parametrize("name", ["n26"] + sorted(DECKS))
 def test_evaluation_error_against_fp64_oracle(q, oracle_cls, tmp_path, name):
     s, x = _deck(q, tmp_path, name)
-    o = oracle_cls(s.ptr)
+    o = oracle_cls(s)
     with q.Handle(s, capacity=len(x), seed=1) as h:
         h.set_precision("mixed")
         g, hl, p, sg = h.compute_properties(x)
@@ -63,7 +63,7 @@ def test_evaluation_error_against_fp64_oracle(q, oracle_cls, tmp_path, name):
 
 def test_fp64_is_the_default_and_restorable(q, oracle_cls, n26, n26_configs):
     x = n26_configs[:8]
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     with q.Handle(n26, capacity=8, seed=1) as h:
         g0, _, p0, _ = h.compute_properties(x)
         h.set_precision("mixed")
@@ -79,7 +79,7 @@ def test_fp64_is_the_default_and_restorable(q, oracle_cls, n26, n26_configs):
 def test_vmc_takes_the_fp64_decisions(q, oracle_cls, tmp_path):
     s, x = _deck(q, tmp_path, "n58_bf")
     nw, nstp, delta = len(x), 3, 0.02 * 25.0
-    o = oracle_cls(s.ptr)
+    o = oracle_cls(s)
     pop = o.population_init(x)
     blk_o, nacc_o = o.vmc_philox(pop, nstp, delta, 1000, SEED, 0)
     with q.Handle(s, capacity=nw, seed=SEED) as h:

@@ -28,7 +28,7 @@ def test_vmc_steps(q, oracle_cls, tmp_path, n26_configs, backflow):
     sysobj = q.System.read(d, "v")
     nw, nstp, delta, mage = 8, 6, 0.05, 1000
     x0 = n26_configs[:nw]
-    o = oracle_cls(sysobj.ptr)
+    o = oracle_cls(sysobj)
     pop = o.population_init(x0)
     blk_o, nacc_o = o.vmc_philox(pop, nstp, delta, mage, SEED, 0)
     with q.Handle(sysobj, capacity=nw, seed=SEED) as h:
@@ -51,7 +51,7 @@ def test_vmc_forced_moves(q, oracle_cls, n26, n26_configs):
     """mage = 0 forces every move (move, reptation.f:4650-4653)."""
     nw = 4
     x0 = n26_configs[:nw]
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     pop = o.population_init(x0)
     o.vmc_philox(pop, 3, 0.05, 0, SEED, 0)
     with q.Handle(n26, capacity=nw, seed=SEED) as h:
@@ -69,7 +69,7 @@ def test_dmc_generations(q, oracle_cls, n26, n26_configs):
     nw, ngen, mmstep, delta = 32, 3, 2, 0.05
     etrial, mmult, mage = -0.43, 5.0, 1000
     x0 = n26_configs[:nw]
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     pop = o.population_init(x0)
     blk_o, norm_o, _ = o.dmc_philox(pop, ngen, mmstep, delta, etrial, mmult, mage, SEED)
     with q.Handle(n26, capacity=nw, seed=SEED) as h:
@@ -93,7 +93,7 @@ def test_reptation_moves(q, oracle_cls, n26, n26_configs):
     nrep, ntau, mdelta, nstp = 2, 8, 2, 6
     prm = capi.RmcParams(ntau, 1, mdelta, 0.05, -0.43, 1000, 1000)
     x = n26_configs[: nrep * ntau]
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     blk_o = np.zeros(n26.nprops)
     paths = []
     for r in range(nrep):

@@ -47,7 +47,7 @@ def test_vmc_energy(q, oracle_cls, n26, equilibrated):
     often."""
     x = equilibrated
     mage = 50
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     pop = o.population_init(x)
     o.vmc_philox(pop, 100, 0.05, mage, 0x1111, 0)
     cpu = []
@@ -69,7 +69,7 @@ def test_vmc_energy(q, oracle_cls, n26, equilibrated):
 def test_dmc_energy(q, oracle_cls, n26, equilibrated):
     x = equilibrated
     tau, et = 0.01, -0.445
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     pop = o.population_init(x)
     o.dmc_philox(pop, 100, 1, tau, et, 2.0, 50, 0x3333, 0, 0)
     cpu = []
@@ -95,7 +95,7 @@ def test_reptation_energy(q, oracle_cls, n26, equilibrated):
     capi = importlib.import_module("2degas_b200._capi")
     ntau, nrep_cpu = 16, 8
     prm = capi.RmcParams(ntau, 2, 2, 0.01, -0.445, 1000, 1000)
-    o = oracle_cls(n26.ptr)
+    o = oracle_cls(n26)
     paths = [equilibrated[(r * ntau) % 64:(r * ntau) % 64 + ntau] for r in range(4)]
     reps = []
     for r in range(nrep_cpu):
