@@ -241,18 +241,65 @@ def whole_job_rate(world, walkers_per_rank, steps, seconds):
 
 
 # ------------------------------------------------------------------- arms
+def workload_desc(args, world):
+    """(metric, config) of the workload `args` selects; the same for the
+    device arm and the reference arm, computed without a GPU."""
+    tables = importlib.import_module("2degas_b200.tables")
+    common = {"l2": "flushed between timed steps (256 MiB write)",
+              "parallelism": f"independent populations x{world}"}
+    if args.workload == "vmc":
+        rs = tables.CONFIGS[VMC_CONFIG]["rs"]
+        nw = args.walkers if args.walkers != 4096 else 256
+        metric = f"walker-moves/sec (VMC, N=26 r_s={rs:g}, {nw} walkers)"
+        cfg = {"workload": VMC_CONFIG, "walkers_per_gpu": nw, "N": 26, "rs": rs,
+               "tau": 0.045 * rs * rs, "moves_per_step": nw * world}
+    elif args.workload == "rmc":
+        name = "rmc_n26_rs10" if args.rmc_n == 26 else RMC_CONFIG
+        rs = tables.CONFIGS[name]["rs"]
+        nw = args.walkers if args.walkers != 4096 else 512
+        metric = (f"walker-moves/sec (reptation, N={args.rmc_n} r_s={rs:g}, {nw} reptiles x "
+                  f"200 beads, one bead growth = one walker-move)")
+        cfg = {"workload": name, "walkers_per_gpu": nw, "N": args.rmc_n, "rs": rs,
+               "tau": 0.01 * rs * rs, "beads": 200, "mdelta": 1, "moves_per_step": nw * world}
+    else:
+        if args.shell is None:
+            metric, name, N, rs = METRIC, CONFIG, 58, 5.0
+        else:
+            rs = args.rs if args.rs is not None else 5.0
+            N = sum(args.shell)
+            name = f"dmc_bf_n{N}{'p' if args.shell[1] == 0 else ''}_rs{rs:g}"
+            metric = (f"walker-moves/sec (DMC with backflow, N={N}"
+                      f"{' polarised' if args.shell[1] == 0 else ''} r_s={rs:g}, "
+                      f"{args.walkers} walkers)")
+        cfg = {"workload": name, "walkers_per_gpu": args.walkers, "N": N, "rs": rs,
+               "precision": args.precision, "tau": 0.05 * rs * rs, "mmstep": 1,
+               "moves_per_step": args.walkers * world}
+    cfg.update(common)
+    return metric, cfg
+
+
 def reference_arm(args, rank, world):
+    """The reference's algorithm on the host cores (the oracle, which restates
+    it; the Fortran reference cannot be built here) for the same workload,
+    metric and config as the device arm."""
     if rank != 0:
         return 0
+    metric, config = workload_desc(args, world)
+    secs = max(4.0, min(20.0, 0.4 * (args.steps + args.warmup)))
     with tempfile.TemporaryDirectory() as tmp:
-        d, _, _ = make_config(tmp, 64, 1)
-        secs = max(4.0, min(20.0, 0.4 * (args.steps + args.warmup)))
-        rate, cores, sample = cpu_rate(d, secs)
+        if args.workload in ("vmc", "rmc"):
+            tables = importlib.import_module("2degas_b200.tables")
+            cfg = tables.CONFIGS[config["workload"]]
+            d = tables.make_run(os.path.join(tmp, "c"), "c", nconf=64, seed=1, **cfg)
+            rate, cores, sample = config_cpu_baseline(args.workload, d, cfg, secs)
+        else:
+            d, _, _ = make_config(tmp, 64, 1, args.shell, args.rs)
+            rate, cores, sample = cpu_rate(d, secs, rs=config["rs"])
     line = {
-        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
+        "impl": "reference", "metric": metric, "value": rate, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": CONFIG, "walkers": 4096, "N": 58, "rs": 5.0},
+        "config": config,
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -392,21 +439,16 @@ def b200_arm(args, rank, world, local_rank):
             rate, cores, sample = cpu_rate(d, args.cpu_seconds, rs=rs)
             cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
         launches = pair_n + move_n + br_n + ga_n
+        metric, config = workload_desc(args, world)
         line = {
-            "metric": METRIC if headline else
-            (f"walker-moves/sec (DMC with backflow, N={N}{' polarised' if len(ns) == 1 else ''}"
-             f" r_s={rs:g}, {nw} walkers)"),
+            "metric": metric,
             "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f64 (f32 u2 and v2 pair terms)",
             "data": "synthetic",
-            "config": {"workload": workload, "walkers_per_gpu": nw, "N": N, "rs": rs,
-                       "precision": args.precision,
-                       "pair_launch": {"groups": tuned[0], "stage_rows": tuned[1] == 0},
-                       "tau": delta, "mmstep": 1, "moves_per_step": nw * world,
-                       "l2": "flushed between timed steps (256 MiB write)",
-                       "parallelism": f"independent populations x{world}"},
+            "config": config,
+            "pair_launch": {"groups": tuned[0], "stage_rows": tuned[1] == 0},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
@@ -422,6 +464,262 @@ def b200_arm(args, rank, world, local_rank):
             "kernel_ms": {"pairs": pair_ms, "move": move_ms, "branch": br_ms, "gather": ga_ms},
             "wall_s": wall,
             "e_mixed": e_mean,
+            "clocks": clk.summary(),
+        }
+    if dist:
+        dist.barrier()
+    h.close()
+    if dist:
+        dist.destroy_process_group()
+    if line:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------ configs 0 and 2 (VMC, RQMC)
+VMC_CONFIG, RMC_CONFIG = "vmc_n26_rs1", "rmc_n58_rs10"
+
+
+def _vmc_cpu_worker(args):
+    """Oracle VMC steps on `nw` walkers for `seconds` (one host process)."""
+    d, nw, seed, seconds, delta = args
+    from oracle_lib import Oracle, OracleSystem
+
+    s = OracleSystem.read(d, "c")
+    o = Oracle(s)
+    pop = o.population_init(s.read_configs(d, ".0", 0, nw))
+    t0 = time.perf_counter()
+    moves, stp = 0, 0
+    while time.perf_counter() - t0 < seconds:
+        o.vmc_philox(pop, 1, delta, 10 ** 9, seed, stp)
+        moves += nw
+        stp += 1
+    return moves, time.perf_counter() - t0
+
+
+def _rmc_cpu_worker(args):
+    """Oracle reptation moves of one reptile for `seconds` (one host
+    process); the path set-up (ntau evaluations) is not timed."""
+    d, ntau, seed, seconds, delta, etrial, mage_r, rs = args
+    from oracle_lib import Oracle, OracleSystem, Reptile
+
+    capi = importlib.import_module("2degas_b200._capi")
+    s = OracleSystem.read(d, "c")
+    o = Oracle(s)
+    x = rmc_start_paths(s.read_configs(d, ".0", 0, 1), ntau, delta, rs, seed)
+    rep = Reptile(o, capi.RmcParams(ntau, 1, 1, delta, etrial, 10 ** 9, mage_r))
+    rep.init(x)
+    t0 = time.perf_counter()
+    moves = 0
+    while time.perf_counter() - t0 < seconds:
+        rep.run(seed, seed, moves, 1)
+        moves += 1
+    return moves, time.perf_counter() - t0
+
+
+def cpu_pool_rate(worker, argsets):
+    """Run `worker` on every host core (spawned processes); returns
+    (walker-moves/s, cores, total moves)."""
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(len(argsets)) as pool:
+        res = pool.map(worker, argsets)
+    moves = sum(r[0] for r in res)
+    return moves / max(r[1] for r in res), len(argsets), moves
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def rmc_start_paths(x0, ntau, delta, rs, seed):
+    """Reptiles as random walks of ntau beads from the configurations x0,
+    with the propagator's link variance 2 hbs2m delta = 2 delta / r_s^2."""
+    rng = np.random.default_rng(seed)
+    var = 2.0 * delta / rs ** 2
+    st = rng.normal(0.0, math.sqrt(var), size=(x0.shape[0], ntau, x0.shape[1]))
+    st[:, 0] = 0.0
+    return (x0[:, None, :] + np.cumsum(st, axis=1)).reshape(x0.shape[0] * ntau, -1)
+
+
+def config_cpu_baseline(kind, d, cfg, seconds):
+    """The oracle on every host core for a bounded sample of the workload."""
+    rs = cfg["rs"]
+    n = host_cores()
+    if kind == "vmc":
+        delta = 0.045 * rs * rs
+        rate, cores, moves = cpu_pool_rate(
+            _vmc_cpu_worker, [(d, 8, 300 + i, seconds, delta) for i in range(n)])
+        sample = (f"{cores} processes x 8 walkers, oracle VMC steps for {seconds:.0f} s each "
+                  f"({moves} walker-moves)")
+    else:
+        delta = 0.01 * rs * rs
+        rate, cores, moves = cpu_pool_rate(
+            _rmc_cpu_worker, [(d, 200, 500 + i, seconds, delta, -0.27, 50, rs)
+                              for i in range(n)])
+        sample = (f"{cores} processes x 1 reptile of 200 beads, oracle reptation moves "
+                  f"(mdelta 1) for {seconds:.0f} s each ({moves} bead growths)")
+    return rate, cores, sample
+
+
+def config_arm(args, rank, world, local_rank):
+    """BASELINE's configuration 0 (--workload vmc: plain VMC, N = 26 r_s = 1,
+    256 walkers, Gaussian step 0.3 r_s) or 2 (--workload rmc: reptation,
+    N = 58 r_s = 10 with u2 + u3 + backflow, 512 reptiles of 200 beads,
+    one-bead head moves, tau = 0.01 r_s^2; --rmc-n 26 for the N = 26 deck).
+    One step = one VMC step of every walker, or one reptation move of every
+    reptile (one bead growth each = one walker-move)."""
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    q = importlib.import_module("2degas_b200")
+    tables = importlib.import_module("2degas_b200.tables")
+    capi = q._capi
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    vmc = args.workload == "vmc"
+    name = VMC_CONFIG if vmc else ("rmc_n26_rs10" if args.rmc_n == 26 else RMC_CONFIG)
+    cfg = tables.CONFIGS[name]
+    rs = cfg["rs"]
+    nw = args.walkers if args.walkers != 4096 else (256 if vmc else 512)
+    ntau = 200
+    cfg_seed, walker_seed = rank_seeds(rank)
+    tmp = tempfile.mkdtemp(prefix="qmc2d_bench_")
+    d = tables.make_run(os.path.join(tmp, name), "c", nconf=nw, seed=cfg_seed, **cfg)
+    sysobj = q.System.read(d, "c")
+    N, nt, npr = sysobj.N, sysobj.ntypes, sysobj.nprops
+    ns = [sysobj.s.np[t] for t in range(nt)]
+    x0 = sysobj.read_configs(d, ".0", 0, nw)
+    if vmc:
+        delta = 0.045 * rs * rs
+        h = q.Handle(sysobj, capacity=nw, seed=walker_seed, device=local_rank)
+        h.population_set(x0)
+        h.vmc(args.equil, delta, 10 ** 9)
+        tuned = h.autotune()
+
+        def step():
+            h.vmc(1, delta, 10 ** 9)
+        kernels = (capi.KERNEL_PAIRS, capi.KERNEL_MOVE)
+    else:
+        delta, etrial, mage_r = 0.01 * rs * rs, -0.27, 50
+        h = q.Handle(sysobj, capacity=nw, seed=walker_seed, device=local_rank)
+        h.population_set(x0)
+        h.vmc(args.equil, 0.045 * rs * rs, 10 ** 9)  # seeded VMC start configurations
+        x1 = h.population_get()["x"]
+        h.rmc_init(nw, rmc_start_paths(x1, ntau, delta, rs, walker_seed & 0xFFFF), ntau, 1, 1,
+                   delta, etrial, 10 ** 9, mage_r)
+        tuned = None
+
+        def step():
+            h.rmc(1)
+        kernels = (capi.KERNEL_RMC,)
+    stream = torch.cuda.ExternalStream(h.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    h.profile(True)
+    h.block_reset()
+    dev_ms = 0.0
+    with Clocks(local_rank) as clk:
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (outside the events)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            dev_ms += e0.elapsed_time(e1)
+        torch.cuda.synchronize()
+    kms = {k: h.profile_get(k) for k in kernels}
+    h.profile(False)
+    blk, norm = h.block_get()
+    acc = h.counters()
+    t_max = max_over_ranks(dev_ms, dist, "cuda")
+    value = whole_job_rate(world, nw, args.steps, t_max * 1e-3)
+
+    # e2e through the public C-ABI with pinned host buffers every step
+    k2 = max(3, args.steps // 2)
+    if vmc:
+        pin = {k: torch.empty(n, dtype=torch.float64, pin_memory=True)
+               for k, n in (("x", nw * 2 * N), ("g", nw * 2 * N), ("h", nw * nt),
+                            ("p", nw * npr), ("s", nw), ("a", nw))}
+        ptr = {k: v.data_ptr() for k, v in pin.items()}
+        h.population_get_ptr(ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"], ptr["a"])
+        h2d = sum(v.numel() * 8 for v in pin.values())
+        d2h = h2d + npr * 8 + 8
+
+        def e2e_step():
+            h.population_load_ptr(nw, ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"], ptr["a"])
+            step()
+            h.population_get_ptr(ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"], ptr["a"])
+            h.block_get()
+    else:
+        # reptiles stay resident (the reference keeps its path in COMMON);
+        # each step the host reads the block sums back
+        h2d, d2h = 0, npr * 8 + 8
+
+        def e2e_step():
+            step()
+            h.block_get()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(k2):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+    e2e = whole_job_rate(world, nw, k2, e2e_s)
+
+    line = None
+    if rank == 0:
+        K = sysobj.s.nk
+        # config 0's deck carries an eta = 0 backflow table (the reference
+        # builds its determinant only in the backflow routine): counted as
+        # the plain Slater-Jastrow algorithm it is
+        fpm = flops_per_move(N, ns, K, 0 if vmc else 1, 0 if vmc else 1)
+        kern_ms = sum(kms[k][0] for k in kernels)
+        n_launch = max(kms[kernels[-1]][1], 1)
+        achieved = fpm * nw / (kern_ms / n_launch * 1e-3) / 1e12
+        peak = fp64_peak_tflops(torch)
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            rate, cores, sample = config_cpu_baseline(args.workload, d, cfg, args.cpu_seconds)
+            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        metric, config = workload_desc(args, world)
+        line = {
+            "metric": metric,
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config,
+            "pair_launch": ({"groups": tuned[0], "stage_rows": tuned[1] == 0}
+                            if tuned else None),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "kernel": "pairs_kernel + move_kernel" if vmc else "rmc_move_kernel",
+                         "flops_per_move": fpm,
+                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64)"},
+            "cpu_baseline": cpu,
+            "gpu_launches": sum(kms[k][1] for k in kernels),
+            "kernel_ms": {str(k): kms[k][0] for k in kernels},
+            "acceptance": acc["accepted"] / max(acc["proposed"], 1),
+            "e_mean": blk[0] / norm,
             "clocks": clk.summary(),
         }
     if dist:
@@ -596,9 +894,13 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="pair passes in FP64 (default), or u2 and real-space Ewald pair terms "
                          "in FP32 with compensated sums")
-    ap.add_argument("--workload", default="dmc", choices=["dmc", "serve", "batch"],
-                    help="dmc: the N=58 DMC generation (default); serve: the serving stream; "
-                         "batch: 64 uneven populations through one graph")
+    ap.add_argument("--workload", default="dmc", choices=["dmc", "vmc", "rmc", "serve", "batch"],
+                    help="dmc: the N=58 DMC generation (default); vmc: plain VMC N=26 r_s=1, "
+                         "256 walkers; rmc: reptation N=58 r_s=10, 512 reptiles x 200 beads; "
+                         "serve: the serving stream; batch: 64 uneven populations through "
+                         "one graph")
+    ap.add_argument("--rmc-n", type=int, default=58, choices=[26, 58],
+                    help="electrons of the reptation workload's deck")
     ap.add_argument("--shell", type=lambda v: tuple(int(t) for t in v.split(",")),
                     default=None, metavar="NU,ND",
                     help="dmc workload on another closed shell (electrons up, down)")
@@ -625,6 +927,8 @@ def main():
         return serve_arm(args, rank, world)
     if args.workload == "batch":
         return batch_arm(args, rank, world)
+    if args.workload in ("vmc", "rmc"):
+        return config_arm(args, rank, world, local_rank)
     return b200_arm(args, rank, world, local_rank)
 
 
