@@ -228,6 +228,17 @@ class Handle:
     def vmc(self, nstp, delta, mage):
         self._chk(self.lib.qmc2d_vmc(self.h, nstp, delta, mage))
 
+    def vmc_single(self, nsweep, delta, refresh=50):
+        """nsweep sweeps of single-electron moves (plain Slater-Jastrow decks);
+        the inverse is recomputed every `refresh` moves (0: at the start only)."""
+        self._chk(self.lib.qmc2d_vmc_single(self.h, nsweep, delta, refresh))
+
+    def single_drift(self):
+        """Largest |W D - I| before a recompute in the last vmc_single call."""
+        d = ctypes.c_double()
+        self._chk(self.lib.qmc2d_single_drift(self.h, ctypes.byref(d)))
+        return d.value
+
     def dmc(self, nstp, mmstep, delta, etrial, mmult, mage):
         self._chk(self.lib.qmc2d_dmc(self.h, nstp, mmstep, delta, etrial, mmult, mage))
 

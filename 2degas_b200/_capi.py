@@ -33,7 +33,8 @@ ERR_LIMIT = 10
 ERR_STACK = 11
 
 # kernels for qmc2d_profile_get
-KERNEL_MOVE, KERNEL_BRANCH, KERNEL_GATHER, KERNEL_EVAL, KERNEL_RMC, KERNEL_PAIRS = range(6)
+(KERNEL_MOVE, KERNEL_BRANCH, KERNEL_GATHER, KERNEL_EVAL, KERNEL_RMC, KERNEL_PAIRS,
+ KERNEL_SINGLE) = range(7)
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 
 # property indices (0-based; reptation.f:577-637)
@@ -187,6 +188,8 @@ SIGNATURES = {
     "qmc2d_compute_properties_noalloc": (c_int, [SYSP, c_int, c_void_p, c_void_p, c_void_p,
                                                  c_void_p, c_void_p, c_void_p]),
     "qmc2d_compute_properties_noalloc_status": (c_int, [c_int, c_void_p]),
+    "qmc2d_vmc_single": (c_int, [c_void_p, c_int, c_double, c_int]),
+    "qmc2d_single_drift": (c_int, [c_void_p, PD]),
     "qmc2d_compute_properties_dev_status": (c_int, [c_void_p, c_int, c_void_p]),
     "qmc2d_population_set": (c_int, [c_void_p, c_int, PD]),
     "qmc2d_population_size": (c_int, [c_void_p, POINTER(c_int)]),

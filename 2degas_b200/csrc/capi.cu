@@ -216,6 +216,7 @@ size_t handle_bytes(const qmc2d_system *sys, const q2d::DevSys &hs, size_t ncoef
   b += al(c, 8) * 2 + al(c, 4) * 4 + al(1, 4);                           // branch scratch
   b += al(c * 2 * N, 8) * 2 + al(c * nt, 8) + al(c * np, 8) + al(c, 8);  // staging
   b += al(c * q2d::move_scratch_doubles(hs), 8) + al(np + 1, 8);
+  b += al(c, 8);  // inverse drift of the single-electron sweeps
   // determinants beyond shared memory: qmc2d_create moves them to HBM when
   // the walker exceeds the device's opt-in shared memory per block; this
   // count is made without a device, at the B200's 227 KB
@@ -332,8 +333,22 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
       (e = dalloc(&h->d_p, (size_t)cap * np)) != cudaSuccess ||
       (e = dalloc(&h->d_s, (size_t)cap)) != cudaSuccess ||
       (e = dalloc(&h->d_mscr, (size_t)cap * q2d::move_scratch_doubles(h->hs))) != cudaSuccess ||
-      (e = dalloc(&h->d_blksum, (size_t)np + 1)) != cudaSuccess)
+      (e = dalloc(&h->d_blksum, (size_t)np + 1)) != cudaSuccess ||
+      (e = dalloc(&h->d_sdrift, (size_t)cap)) != cudaSuccess)
     return fail(cuda_fail(e, "cudaMalloc"));
+  // a backflow table of zeros only: the determinant of plain plane waves
+  h->bf_zero = 0;
+  if (h->hs.has_bf) {
+    bool zero = true;
+    for (int a = 0; a < sys->ntypes; a++)
+      for (int b = 0; b < sys->ntypes; b++) {
+        const int t = sys->iub[a][b];
+        if (t < 0) continue;
+        const qmc2d_table &tb = sys->tables[t];
+        for (size_t q = 0; q < 4 * (size_t)(tb.ngrid + 1) && zero; q++) zero = tb.ut[q] == 0.0;
+      }
+    h->bf_zero = zero ? 1 : 0;
+  }
   cudaMemset(h->d_blk, 0, sizeof(double) * cap * np);
   cudaMemset(h->d_norm, 0, sizeof(double) * cap);
   cudaMemset(h->d_cnt, 0, sizeof(double) * cap * 4);
@@ -451,7 +466,7 @@ extern "C" int qmc2d_destroy(qmc2d_handle *h) {
   void *bufs[] = {h->ds, h->d_coef, h->d_kvec, h->d_gvec, h->d_blk, h->d_norm, h->d_cnt,
                   h->d_wate, h->d_status, h->br.delt, h->br.csum, h->br.mult, h->br.src,
                   h->br.ecum, h->br.zrank, h->br.ncapped, h->d_x, h->d_g, h->d_h, h->d_p,
-                  h->d_s, h->d_mscr, h->d_blksum, h->hs.phase, h->d_gmat};
+                  h->d_s, h->d_mscr, h->d_blksum, h->hs.phase, h->d_gmat, h->d_sdrift};
   for (void *b : bufs) cudaFree(b);
   for (int k = 0; k < QMC2D_NKERNELS; k++)
     for (cudaEvent_t e : h->ev[k]) cudaEventDestroy(e);

@@ -31,6 +31,9 @@ struct qmc2d_handle {
   int device = 0;
   uint64_t seed = 0;
   uint32_t move_counter = 0, gen_counter = 0;
+  uint32_t sweep_counter = 0;  // Philox c2 of single-electron sweeps (qmc2d_vmc_single)
+  int bf_zero = 0;             // every backflow table identically zero (a plain determinant)
+  double *d_sdrift = nullptr;  // cap: inverse drift of the last qmc2d_vmc_single
   double dmc_ecut = 0.0;  // qmc2d_set_dmc_ecut (0: the reference's weights)
   q2d::RmcState rmc{};
   // per-kernel CUDA-event timing (qmc2d_profile)

@@ -63,6 +63,20 @@ def move_scratch_bytes(N, nk):
     return 8 * ((pair + 3 * N * N + 31) & ~31)
 
 
+def flops_per_sweep(N, ns, K):
+    """Algorithmic flops of one sweep of single-electron moves (N moves on a
+    plain Slater-Jastrow deck, then one measurement; transcendental = 1):
+    per move of an electron whose spin has n orbitals, the orbitals, ratio
+    and gradient at the old and new positions (2 x 13 n), the two-body
+    Jastrow at both (2 x 30 (N - 1)) and the Sherman-Morrison update (16 n^2);
+    the measurement's pair sums (60 per pair), rho_k (7 N K) and the
+    determinant drift and Laplacian (25 n^2 per spin)."""
+    f = 0
+    for n in ns:
+        f += n * (26 * n + 60 * (N - 1) + 16 * n * n) + 25 * n * n
+    return float(f + 60 * N * (N - 1) // 2 + 7 * N * K)
+
+
 def flops_per_move(N, ns, K, u3, backflow):
     """Algorithmic flops of one all-electron walker-move (proposal + evaluation
     + accept/reject) of the reference's algorithm, counted from its loop
@@ -250,9 +264,15 @@ def workload_desc(args, world):
     if args.workload == "vmc":
         rs = tables.CONFIGS[VMC_CONFIG]["rs"]
         nw = args.walkers if args.walkers != 4096 else 256
-        metric = f"walker-moves/sec (VMC, N=26 r_s={rs:g}, {nw} walkers)"
+        if args.single:
+            metric = (f"walker-moves/sec (VMC, N=26 r_s={rs:g}, {nw} walkers; single-electron "
+                      f"moves, one sweep of N moves = one walker-move)")
+        else:
+            metric = f"walker-moves/sec (VMC, N=26 r_s={rs:g}, {nw} walkers)"
         cfg = {"workload": VMC_CONFIG, "walkers_per_gpu": nw, "N": 26, "rs": rs,
-               "tau": 0.045 * rs * rs, "moves_per_step": nw * world}
+               "tau": 0.045 * rs * rs, "moves_per_step": nw * world,
+               "moves": "single-electron sweeps, inverse recomputed every 50 moves"
+               if args.single else "all-electron"}
     elif args.workload == "rmc":
         name = "rmc_n26_rs10" if args.rmc_n == 26 else RMC_CONFIG
         rs = tables.CONFIGS[name]["rs"]
@@ -598,7 +618,17 @@ def config_arm(args, rank, world, local_rank):
     N, nt, npr = sysobj.N, sysobj.ntypes, sysobj.nprops
     ns = [sysobj.s.np[t] for t in range(nt)]
     x0 = sysobj.read_configs(d, ".0", 0, nw)
-    if vmc:
+    if vmc and args.single:
+        delta = 0.045 * rs * rs
+        h = q.Handle(sysobj, capacity=nw, seed=walker_seed, device=local_rank)
+        h.population_set(x0)
+        h.vmc_single(args.equil, delta, 50)
+        tuned = None
+
+        def step():
+            h.vmc_single(1, delta, 50)
+        kernels = (capi.KERNEL_SINGLE,)
+    elif vmc:
         delta = 0.045 * rs * rs
         h = q.Handle(sysobj, capacity=nw, seed=walker_seed, device=local_rank)
         h.population_set(x0)
@@ -690,7 +720,8 @@ def config_arm(args, rank, world, local_rank):
         # config 0's deck carries an eta = 0 backflow table (the reference
         # builds its determinant only in the backflow routine): counted as
         # the plain Slater-Jastrow algorithm it is
-        fpm = flops_per_move(N, ns, K, 0 if vmc else 1, 0 if vmc else 1)
+        fpm = (flops_per_sweep(N, ns, K) if vmc and args.single else
+               flops_per_move(N, ns, K, 0 if vmc else 1, 0 if vmc else 1))
         kern_ms = sum(kms[k][0] for k in kernels)
         n_launch = max(kms[kernels[-1]][1], 1)
         achieved = fpm * nw / (kern_ms / n_launch * 1e-3) / 1e12
@@ -712,7 +743,8 @@ def config_arm(args, rank, world, local_rank):
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                         "kernel": "pairs_kernel + move_kernel" if vmc else "rmc_move_kernel",
+                         "kernel": ("single_kernel" if vmc and args.single else
+                                    "pairs_kernel + move_kernel" if vmc else "rmc_move_kernel"),
                          "flops_per_move": fpm,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64)"},
             "cpu_baseline": cpu,
@@ -899,6 +931,8 @@ def main():
                          "256 walkers; rmc: reptation N=58 r_s=10, 512 reptiles x 200 beads; "
                          "serve: the serving stream; batch: 64 uneven populations through "
                          "one graph")
+    ap.add_argument("--single", action="store_true",
+                    help="vmc workload with single-electron moves and Sherman-Morrison updates")
     ap.add_argument("--rmc-n", type=int, default=58, choices=[26, 58],
                     help="electrons of the reptation workload's deck")
     ap.add_argument("--shell", type=lambda v: tuple(int(t) for t in v.split(",")),

@@ -408,6 +408,35 @@ int qmc2d_vmc(qmc2d_handle *h, int nstp, double delta, int mage);
 int qmc2d_dmc(qmc2d_handle *h, int nstp, int mmstep, double delta, double etrial,
               double mmult, int mage);
 
+/* Single-electron moves. The reference moves all electrons at once (move,
+ * reptation.f:4617-4680); this is the same importance-sampled Metropolis
+ * step (drift from -grad ln|psi|, the Green's-function ratio and the
+ * acceptance of metropolis_test, :2622-2659) applied to one electron at a
+ * time, for decks whose wave function is a Slater determinant of plane
+ * waves times a two-body Jastrow: no u3, and backflow tables that are
+ * identically zero (the reference carries its determinant in the backflow
+ * routine, so a plain determinant is a zero eta table). Otherwise
+ * QMC2D_ERR_UNSUPPORTED.
+ * nsweep sweeps of every walker of the population: each sweep moves
+ * electrons 0..N-1 in turn; the determinant ratio comes from the inverse
+ * Slater matrices, which stay resident on the device for the whole call and
+ * are updated by Sherman-Morrison after every accepted move, and rebuilt
+ * from the positions and inverted from scratch (FP64) at the start and
+ * after every `refresh` single-electron moves (0: at the start only).
+ * After each sweep the walker's properties are measured and added to the
+ * block sums with weight 1, as qmc2d_vmc does per step, p(jacc) being the
+ * mean acceptance probability of the sweep's N moves. The counters count
+ * single-electron moves. Random draws: electron i, coordinate d of walker
+ * slot w in sweep t uses Philox (c0 = 2i+d, c1 = w, c2 = t, c3 = 0x5100)
+ * and its acceptance u[0] of (c0 = 0x80000000|i, c1 = w, c2 = t,
+ * c3 = 0x5100), t counting the handle's sweeps. */
+int qmc2d_vmc_single(qmc2d_handle *h, int nsweep, double delta, int refresh);
+/* The largest max_jm |sum_k W(j,k) D(k,m) - delta_jm| over the walkers of
+ * the last qmc2d_vmc_single call, measured on the updated inverse just
+ * before each recompute: the round-off drift of the Sherman-Morrison
+ * updates between refreshes (0 when no recompute happened within the call). */
+int qmc2d_single_drift(qmc2d_handle *h, double *max_err);
+
 /* ------------------------------------------------------------- reptation */
 typedef struct qmc2d_rmc_params {
   int ntau, ntauskip, mdelta;
@@ -495,7 +524,8 @@ enum qmc2d_kernel {
   QMC2D_KERNEL_EVAL = 3,    /* batched compute_properties */
   QMC2D_KERNEL_RMC = 4,     /* reptation moves */
   QMC2D_KERNEL_PAIRS = 5,   /* proposal + pair passes of a VMC/DMC move */
-  QMC2D_NKERNELS = 6
+  QMC2D_KERNEL_SINGLE = 6,  /* single-electron VMC sweeps (qmc2d_vmc_single) */
+  QMC2D_NKERNELS = 7
 };
 /* The handle's CUDA stream (a cudaStream_t) so callers can order work and
  * events after the library's launches. */

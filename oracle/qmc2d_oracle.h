@@ -133,6 +133,16 @@ int oracle_dmc_philox(const qmc2d_system *sys, int nw, int ngen, int mmstep, dou
                       long move0, double *x, double *g, double *hl, double *p, double *s,
                       double *age, double *blk, double *blk_norm, long *naccept);
 
+/* Single-electron VMC sweeps with the device's Philox streams
+ * (qmc2d_vmc_single; oracle_single.c): nsweep sweeps over electrons 0..N-1
+ * of each walker, every ratio and drift from a full evaluation. x holds the
+ * walkers on entry; x, g, hl, p, s, age the final records; blk accumulates
+ * the walker's properties after every sweep (p(jacc) = the sweep's mean
+ * acceptance probability); naccept counts accepted single-electron moves. */
+int oracle_vmc_single(const qmc2d_system *sys, int nw, int nsweep, double delta, uint64_t seed,
+                      long sweep0, double *x, double *g, double *hl, double *p, double *s,
+                      double *age, double *blk, long *naccept);
+
 /* ---- reptation (rmc, reptation.f:1286-2160) for one reptile with Philox
  * draws. Path beads are held in a ring of n_buffer = ntau + mdelta slots. */
 typedef struct oracle_reptile oracle_reptile;

@@ -118,6 +118,9 @@ class Oracle:
                                           PD, PD, PD, PD, PD, POINTER(c_long)]
         lib.oracle_philox_uniform2.argtypes = [c_uint64, c_uint32, c_uint32, c_uint32, c_uint32,
                                                PD]
+        lib.oracle_vmc_single.restype = c_int
+        lib.oracle_vmc_single.argtypes = [c_void_p, c_int, c_int, c_double, c_uint64, c_long,
+                                          PD, PD, PD, PD, PD, PD, PD, POINTER(c_long)]
         lib.oracle_reptile_new.restype = c_void_p
         lib.oracle_reptile_new.argtypes = [c_void_p, c_void_p]
         lib.oracle_reptile_free.argtypes = [c_void_p]
@@ -190,6 +193,20 @@ class Oracle:
         blk = np.zeros(self.nprops)
         nacc = c_long(0)
         st = self.lib.oracle_vmc_philox(self._s, nw, nstp, delta, mage, seed, step0,
+                                        _ptr(pop["x"]), _ptr(pop["g"]), _ptr(pop["h"]),
+                                        _ptr(pop["p"]), _ptr(pop["s"]), _ptr(pop["age"]),
+                                        _ptr(blk), ctypes.byref(nacc))
+        if st:
+            raise RuntimeError(f"oracle status {st}")
+        return blk, nacc.value
+
+    def vmc_single(self, pop, nsweep, delta, seed, sweep0=0):
+        """Single-electron sweeps (qmc2d_vmc_single's streams); pop["x"] in,
+        every record out; returns (block sums, accepted moves)."""
+        nw = pop["x"].shape[0]
+        blk = np.zeros(self.nprops)
+        nacc = c_long(0)
+        st = self.lib.oracle_vmc_single(self._s, nw, nsweep, delta, seed, sweep0,
                                         _ptr(pop["x"]), _ptr(pop["g"]), _ptr(pop["h"]),
                                         _ptr(pop["p"]), _ptr(pop["s"]), _ptr(pop["age"]),
                                         _ptr(blk), ctypes.byref(nacc))

@@ -21,10 +21,11 @@ def test_footprint_is_linear_in_walkers_and_counts_every_record(q, n26):
     per = (f[1024] - f[512]) / 512
     assert f[2048] - f[1024] == 1024 * per
     # two populations (x, g, h, p, s, age), block sums, norm, counters,
-    # weights, status, comb scratch, staging, and the move scratch
+    # weights, status, comb scratch, staging, the inverse drift record of
+    # the single-electron sweeps, and the move scratch
     lib = s.lib
     recs = 2 * (4 * N + nt + np_ + 2) * 8 + (np_ + 1 + 4 + 1) * 8 + 4 + 2 * 8 + 4 * 4 \
-        + (4 * N + nt + np_ + 1) * 8
+        + (4 * N + nt + np_ + 1) * 8 + 8  # + the single-electron sweeps' drift record
     # the move scratch: per-particle sums, rho_k and (backflow) 3 N^2 pair
     # values, rounded up to 256 bytes
     nk = s.s.nk
