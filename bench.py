@@ -764,6 +764,63 @@ def config_arm(args, rank, world, local_rank):
     return 0
 
 
+def _serve_cpu_worker(args):
+    """Oracle moves of one request's state point (VMC steps or DMC
+    generations of `nw` walkers) for `seconds`; returns (moves, seconds)."""
+    d, method, nw, seed, seconds, delta = args
+    from oracle_lib import Oracle, OracleSystem
+
+    s = OracleSystem.read(d, "s")
+    o = Oracle(s)
+    rng = np.random.default_rng(seed)
+    el = math.sqrt(s.N * math.pi)
+    pop = o.population_init(rng.uniform(-0.5 * el, 0.5 * el, size=(nw, 2 * s.N)))
+    t0 = time.perf_counter()
+    moves, k = 0, 0
+    while time.perf_counter() - t0 < seconds:
+        if method == "dmc":
+            o.dmc_philox(pop, 1, 1, delta, -0.3, 2.0, 50, seed, k, k)
+        else:
+            o.vmc_philox(pop, 1, delta, 50, seed, k)
+        moves += nw
+        k += 1
+    return moves, time.perf_counter() - t0
+
+
+def serve_cpu_baseline(reqs, results, seconds, max_requests=6):
+    """The reference's algorithm (the oracle) on every host core for the first
+    requests of the stream: each request's deck, its method, a bounded time.
+    The rate is the CPU time those requests' served walker-moves would take:
+    sum of moves / sum of (moves / per-request CPU rate)."""
+    import multiprocessing as mp
+
+    tables = importlib.import_module("2degas_b200.tables")
+    n = host_cores()
+    sample = [(r, res) for r, res in zip(reqs, results) if res.status != "rejected"]
+    sample = sample[:max_requests]
+    if not sample:
+        return None
+    per = max(2.0, seconds / len(sample))
+    tot_moves, tot_time, rows = 0.0, 0.0, []
+    with tempfile.TemporaryDirectory() as tmp, mp.get_context("spawn").Pool(n) as pool:
+        for r, res in sample:
+            d = os.path.join(tmp, f"req{r.rid}")
+            bf = (0.2, 1.0 * r.rs, 0.6 * r.rs) if r.backflow else None
+            tables.make_run(d, "s", r.n_up, r.n_down, r.rs, backflow=bf, ewald="fitpn")
+            out = pool.map(_serve_cpu_worker, [(d, r.method, 2, 900 + i, per, 0.05 * r.rs ** 2)
+                                               for i in range(n)])
+            rate = sum(o[0] for o in out) / max(o[1] for o in out)
+            m = max(res.moves, 1)
+            tot_moves += m
+            tot_time += m / rate
+            rows.append({"rid": r.rid, "N": r.N, "method": r.method, "cpu_moves_per_s": rate})
+    return {"value": tot_moves / tot_time, "unit": UNIT, "cores": n, "kind": "port",
+            "sample": (f"first {len(sample)} requests of the stream, oracle "
+                       f"VMC/DMC on {n} processes x 2 walkers for {per:.0f} s each, weighted by "
+                       f"each request's served walker-moves"),
+            "per_request": rows}
+
+
 def serve_arm(args, rank, world):
     """The serving stream: Poisson arrivals (20 requests/s, seeded) of
     state points on the closed shells 26..162 that the kernels hold, r_s
@@ -818,6 +875,8 @@ def serve_arm(args, rank, world):
                                          energy=r.energy, error=r.error, blocks=r.blocks,
                                          moves=r.moves, message=r.message[:80]) for r in res]},
         "one_at_a_time_fp64": seq,
+        "cpu_baseline": (serve_cpu_baseline(stream(), res, args.cpu_seconds)
+                         if not args.no_cpu else None),
         "clocks": clk.summary(),
     }
     for d, r in zip(line["serving"]["per_request"], stream()):
