@@ -228,6 +228,31 @@ class Handle:
     def vmc(self, nstp, delta, mage):
         self._chk(self.lib.qmc2d_vmc(self.h, nstp, delta, mage))
 
+    def dmc_weights(self, mmstep, delta, etrial, mmult, mage):
+        """One DMC generation's moves and weights, without the comb."""
+        w = np.zeros(self.population_size())
+        self._chk(self.lib.qmc2d_dmc_weights(self.h, mmstep, delta, etrial, mmult, mage, _pd(w)))
+        return w
+
+    def record_len(self):
+        n = ctypes.c_int()
+        self._chk(self.lib.qmc2d_record_len(self.h, ctypes.byref(n)))
+        return n.value
+
+    def records_pack(self, slots, buf_ptr, stream=None):
+        sl = np.ascontiguousarray(slots, dtype=np.int32)
+        self._chk(self.lib.qmc2d_records_pack(self.h, len(sl), sl.ctypes.data_as(_capi.PI),
+                                              buf_ptr, stream))
+
+    def records_unpack(self, slots, buf_ptr, stream=None):
+        sl = np.ascontiguousarray(slots, dtype=np.int32)
+        self._chk(self.lib.qmc2d_records_unpack(self.h, len(sl), sl.ctypes.data_as(_capi.PI),
+                                                buf_ptr, stream))
+
+    def population_resample(self, src):
+        s = np.ascontiguousarray(src, dtype=np.int32)
+        self._chk(self.lib.qmc2d_population_resample(self.h, s.ctypes.data_as(_capi.PI)))
+
     def vmc_single(self, nsweep, delta, refresh=50):
         """nsweep sweeps of single-electron moves (plain Slater-Jastrow decks);
         the inverse is recomputed every `refresh` moves (0: at the start only)."""

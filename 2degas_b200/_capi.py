@@ -169,6 +169,7 @@ class RmcParams(ctypes.Structure):
 
 
 PD = POINTER(c_double)
+PI = POINTER(c_int)
 SYSP = POINTER(System)
 
 # name -> (restype, argtypes); every symbol include/qmc2d.h declares.
@@ -189,6 +190,13 @@ SIGNATURES = {
                                                  c_void_p, c_void_p, c_void_p]),
     "qmc2d_compute_properties_noalloc_status": (c_int, [c_int, c_void_p]),
     "qmc2d_vmc_single": (c_int, [c_void_p, c_int, c_double, c_int]),
+    "qmc2d_dmc_weights": (c_int, [c_void_p, c_int, c_double, c_double, c_double, c_int, PD]),
+    "qmc2d_comb_plan": (c_int, [c_int, c_int, PD, c_uint64, ctypes.c_uint32, c_int, PI, PI, PI,
+                                PI, PI, PI, PI, PI]),
+    "qmc2d_record_len": (c_int, [c_void_p, PI]),
+    "qmc2d_records_pack": (c_int, [c_void_p, c_int, PI, c_void_p, c_void_p]),
+    "qmc2d_records_unpack": (c_int, [c_void_p, c_int, PI, c_void_p, c_void_p]),
+    "qmc2d_population_resample": (c_int, [c_void_p, PI]),
     "qmc2d_single_drift": (c_int, [c_void_p, PD]),
     "qmc2d_compute_properties_dev_status": (c_int, [c_void_p, c_int, c_void_p]),
     "qmc2d_population_set": (c_int, [c_void_p, c_int, PD]),

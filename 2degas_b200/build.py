@@ -16,7 +16,7 @@ LIBDIR = os.path.join(HERE, "lib")
 OUT = os.path.join(LIBDIR, "libqmc2d.so")
 
 SOURCES = ["input.cpp", "system.cpp", "io.cpp", "kernels.cu", "capi.cu", "rmc.cu", "noalloc.cu",
-           "batch.cu", "estimators.cpp", "single.cu"]
+           "batch.cu", "estimators.cpp", "single.cu", "comb.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -771,3 +771,75 @@ extern "C" int qmc2d_dmc(qmc2d_handle *h, int nstp, int mmstep, double delta, do
   }
   return sync_status(h, h->nw);
 }
+
+// ------------------------------------------- DMC across ranks (branch2)
+extern "C" int qmc2d_dmc_weights(qmc2d_handle *h, int mmstep, double delta, double etrial,
+                                 double mmult, int mage, double *wate) {
+  if (!h || mmstep <= 0 || !(delta > 0.0) || !wate) return QMC2D_ERR_ARG;
+  if (h->nw <= 0) {
+    q2d::set_error("qmc2d_dmc_weights: empty population");
+    return QMC2D_ERR_STACK;
+  }
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * h->nw, h->stream));
+  int st = run_moves(h, mmstep, 1, delta, etrial, mmult, mage);
+  if (st) return st;
+  CK(cudaMemcpyAsync(wate, h->d_wate, sizeof(double) * h->nw, cudaMemcpyDeviceToHost,
+                     h->stream));
+  return sync_status(h, h->nw);
+}
+
+extern "C" int qmc2d_population_resample(qmc2d_handle *h, const int *src) {
+  if (!h || !src) return QMC2D_ERR_ARG;
+  for (int j = 0; j < h->nw; j++)
+    if (src[j] < 0 || src[j] >= h->nw) {
+      q2d::set_error("qmc2d_population_resample: source slot out of range");
+      return QMC2D_ERR_ARG;
+    }
+  CK(cudaSetDevice(h->device));
+  CK(cudaMemcpyAsync(h->br.src, src, sizeof(int) * h->nw, cudaMemcpyHostToDevice, h->stream));
+  const int nxt = 1 - h->cur;
+  {
+    ProfScope ps(h, QMC2D_KERNEL_GATHER, h->stream);
+    CK(q2d::launch_gather(h->hs, h->pop[h->cur], h->pop[nxt], h->br.src, h->nw, h->stream));
+  }
+  h->cur = nxt;
+  h->gen_counter++;
+  CK(cudaStreamSynchronize(h->stream));
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_record_len(qmc2d_handle *h, int *len) {
+  if (!h || !len) return QMC2D_ERR_ARG;
+  *len = 4 * h->N + h->nt + h->nprops + 2;
+  return QMC2D_OK;
+}
+
+static int records(qmc2d_handle *h, int n, const int *slots, double *buf_dev, void *stream,
+                   int unpack) {
+  if (!h || n < 0 || n > h->cap || (n > 0 && (!slots || !buf_dev))) return QMC2D_ERR_ARG;
+  for (int k = 0; k < n; k++)
+    if (slots[k] < 0 || slots[k] >= h->cap) {
+      q2d::set_error("qmc2d_records_pack/unpack: slot out of range");
+      return QMC2D_ERR_ARG;
+    }
+  if (n == 0) return QMC2D_OK;
+  CK(cudaSetDevice(h->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  // the slot list goes through the comb's rank scratch (cap ints), which no
+  // other call uses between a generation's weights and its resample
+  CK(cudaMemcpyAsync(h->br.zrank, slots, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+  CK(q2d::launch_records(h->hs, h->pop[h->cur], h->br.zrank, buf_dev, n, unpack, st));
+  CK(cudaStreamSynchronize(st));
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_records_pack(qmc2d_handle *h, int n, const int *slots, double *buf_dev,
+                                  void *stream) {
+  return records(h, n, slots, buf_dev, stream, 0);
+}
+
+extern "C" int qmc2d_records_unpack(qmc2d_handle *h, int n, const int *slots,
+                                    const double *buf_dev, void *stream) {
+  return records(h, n, slots, const_cast<double *>(buf_dev), stream, 1);
+}

@@ -517,6 +517,26 @@ __global__ void gather_kernel(DevPop from, DevPop to, const int *src, int N2, in
   }
 }
 
+// Walker records [x(2N), g(2N), h(nt), p(np), s, age] of slots[k] to or
+// from row k of a contiguous buffer (one CTA per record).
+__global__ void records_kernel(DevPop pop, const int *slots, double *buf, int N2, int nt, int np,
+                               int unpack) {
+  const int k = blockIdx.x, j = slots[k];
+  const size_t len = 2 * (size_t)N2 + nt + np + 2;
+  double *r = buf + (size_t)k * len;
+  double *f[6] = {pop.x + (size_t)j * N2, pop.g + (size_t)j * N2, pop.h + (size_t)j * nt,
+                  pop.p + (size_t)j * np, pop.s + j, pop.age + j};
+  const int n[6] = {N2, N2, nt, np, 1, 1};
+  size_t off = 0;
+  for (int q = 0; q < 6; q++) {
+    for (int e = threadIdx.x; e < n[q]; e += blockDim.x) {
+      if (unpack) f[q][e] = r[off + e];
+      else r[off + e] = f[q][e];
+    }
+    off += n[q];
+  }
+}
+
 __global__ void philox_probe_kernel(uint64_t seed, const uint32_t *ctr, uint32_t *out, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -663,6 +683,13 @@ __global__ void counters_add_kernel(uint32_t *ctr, uint32_t steps, uint32_t gens
 
 cudaError_t launch_counters_add(uint32_t *ctr, uint32_t steps, uint32_t gens, cudaStream_t st) {
   counters_add_kernel<<<1, 1, 0, st>>>(ctr, steps, gens);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_records(const DevSys &hs, DevPop pop, const int *slots, double *buf, int n,
+                           int unpack, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  records_kernel<<<n, 128, 0, st>>>(pop, slots, buf, 2 * hs.N, hs.nt, hs.nprops, unpack);
   return cudaGetLastError();
 }
 

@@ -69,6 +69,11 @@ cudaError_t launch_counters_add(uint32_t *ctr, uint32_t steps, uint32_t gens, cu
 cudaError_t launch_gather(const DevSys &hs, DevPop from, DevPop to, const int *src, int nw,
                           cudaStream_t st);
 
+// Walker records [x(2N), g(2N), h(nt), p(np), s, age] of slots[0..n) into
+// rows of buf (unpack = 0) or from them (unpack = 1); slots in device memory.
+cudaError_t launch_records(const DevSys &hs, DevPop pop, const int *slots, double *buf, int n,
+                           int unpack, cudaStream_t st);
+
 // Device Philox4x32-10 check: out[4*i..] = philox(ctr_i, key) for testing.
 cudaError_t launch_philox_probe(uint64_t seed, const uint32_t *ctr, uint32_t *out, int n,
                                 cudaStream_t st);

@@ -437,6 +437,48 @@ int qmc2d_vmc_single(qmc2d_handle *h, int nsweep, double delta, int refresh);
  * updates between refreshes (0 when no recompute happened within the call). */
 int qmc2d_single_drift(qmc2d_handle *h, double *max_err);
 
+/* ------------------------------------------------- DMC across ranks
+ * branch2 (reptation.f:2162-2273) over the walkers of several ranks, one
+ * population (handle) per rank and GPU: each rank advances its walkers and
+ * weights (qmc2d_dmc_weights), the weights are all-gathered by the caller
+ * (MPI_ALLGATHER in the reference, :2185), every rank computes the same
+ * plan (qmc2d_comb_plan), ships the records it sends (qmc2d_records_pack
+ * into a device buffer, then the caller's send; the reference's
+ * send/receive, :2275-2318) and places the ones it receives
+ * (qmc2d_records_unpack), and finally copies walkers within the rank
+ * (qmc2d_population_resample; prov_dest, :2320). With one rank this is the
+ * comb of qmc2d_dmc. */
+/* One DMC generation's moves and weights without the comb: mmstep moves of
+ * every walker, the weight the product of min(mmult, exp(-npnorm (E_L -
+ * etrial) delta)) over them (dmc, reptation.f:894-906); wate[nw] receives
+ * the weights (host). */
+int qmc2d_dmc_weights(qmc2d_handle *h, int mmstep, double delta, double etrial, double mmult,
+                      int mage, double *wate);
+/* The comb of nproc ranks of nconf walkers each, from the weights of all
+ * ranks (wate_all[p * nconf + i], as all-gathered), for `rank`: the same on
+ * every rank. Weights are capped at 10 (wmult, :2174); the comb's uniforms
+ * are Philox u[0] of (c0 = tooth, c1 = 0xFFFFFFFF, c2 = gen, c3 = 1) keyed
+ * by `seed`, which all ranks share (the reference's rannyu2 stream). Out:
+ * sends (send_rank[k], send_slot[k]) and receives (recv_rank[k],
+ * recv_slot[k]) in exchange order (each list has room for nconf entries),
+ * then src[nconf]: after the exchange, new slot j copies slot src[j].
+ * ncapped: this rank's weights that were capped. Host only. */
+int qmc2d_comb_plan(int nproc, int nconf, const double *wate_all, uint64_t seed, uint32_t gen,
+                    int rank, int *src, int *nsend, int *send_rank, int *send_slot, int *nrecv,
+                    int *recv_rank, int *recv_slot, int *ncapped);
+/* Doubles of one walker record: x (2N), g (2N), h (ntypes), props
+ * (n_props), sign, age. */
+int qmc2d_record_len(qmc2d_handle *h, int *len);
+/* Records of the n slots[] (host) of the current population to or from
+ * rows of buf_dev (device, n * record_len doubles); synchronous on
+ * `stream` (NULL: the handle's stream). */
+int qmc2d_records_pack(qmc2d_handle *h, int n, const int *slots, double *buf_dev, void *stream);
+int qmc2d_records_unpack(qmc2d_handle *h, int n, const int *slots, const double *buf_dev,
+                         void *stream);
+/* new[j] = old[src[j]] for every walker slot (src host, nw entries); the
+ * comb's generation counter advances as qmc2d_dmc's does. */
+int qmc2d_population_resample(qmc2d_handle *h, const int *src);
+
 /* ------------------------------------------------------------- reptation */
 typedef struct qmc2d_rmc_params {
   int ntau, ntauskip, mdelta;
