@@ -294,6 +294,8 @@ def workload_desc(args, world):
         cfg = {"workload": name, "walkers_per_gpu": args.walkers, "N": N, "rs": rs,
                "precision": args.precision, "tau": 0.05 * rs * rs, "mmstep": 1,
                "moves_per_step": args.walkers * world}
+        if args.global_comb:
+            common["parallelism"] = f"one population over {world} ranks (global comb)"
     cfg.update(common)
     return metric, cfg
 
@@ -365,8 +367,20 @@ def b200_arm(args, rank, world, local_rank):
     stream = torch.cuda.ExternalStream(h.stream())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def step():
-        h.dmc(1, 1, delta, etrial, mmult, mage)
+    if args.global_comb:
+        # one population over all ranks: branch2's comb and walker exchange
+        # every generation (2degas_b200/multirank.py)
+        mr = importlib.import_module("2degas_b200.multirank")
+        pop = mr.HandleRecords(h, torch.device("cuda", local_rank))
+        gen = [0]
+
+        def step():
+            mr.dmc_generations(pop, dist, 1, 1, delta, etrial, mmult, mage, 0x5EEDC0B1,
+                               gen0=gen[0], device=f"cuda:{local_rank}")
+            gen[0] += 1
+    else:
+        def step():
+            h.dmc(1, 1, delta, etrial, mmult, mage)
 
     if args.phases:
         # SM cycles per walker-move of each phase of the move kernel (clock64
@@ -821,6 +835,100 @@ def serve_cpu_baseline(reqs, results, seconds, max_requests=6):
             "per_request": rows}
 
 
+def precision_arm(args, rank, world, local_rank):
+    """The plain FP64 path and the mixed-precision form on the headline DMC
+    state point (N = 58, r_s = 5, 4096 walkers), same box, same start:
+    walker-moves/s of each and their ratio (at fixed E_L error the ratio of
+    walker-moves/s is the ratio of cost, as long as the mixed form samples
+    the same distribution), the per-configuration |Delta E_L| against the
+    FP64 path on 512 configurations, each run's mean energy with its error
+    bar, and the acceptance ratio."""
+    import torch
+
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local_rank)
+    q = importlib.import_module("2degas_b200")
+    tmp = tempfile.mkdtemp(prefix="qmc2d_prec_")
+    nw = args.walkers
+    d, cfg, workload = make_config(tmp, nw, 1)
+    sysobj = q.System.read(d, "c")
+    rs = cfg["rs"]
+    delta, mmult, mage = 0.05 * rs * rs, 2.0, 50
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    with q.Handle(sysobj, capacity=nw, seed=7) as h0:
+        h0.population_set(sysobj.read_configs(d, ".0", 0, nw))
+        h0.vmc(args.equil, delta, 10 ** 9)
+        h0.block_reset()
+        h0.vmc(10, delta, 10 ** 9)
+        blk, norm = h0.block_get()
+        etrial = blk[0] / norm
+        start = h0.population_get()
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with q.Handle(sysobj, capacity=nw, seed=11) as h:
+            h.set_precision(prec)
+            h.population_set(start["x"])
+            h.autotune()
+            stream = torch.cuda.ExternalStream(h.stream())
+            for _ in range(args.warmup):
+                h.dmc(1, 1, delta, etrial, mmult, mage)
+            c0 = h.counters()
+            dev_ms, means = 0.0, []
+            nb = max(10, args.steps // 10)
+            per = max(1, args.steps // nb)
+            for b in range(nb):
+                h.block_reset()
+                for _ in range(per):
+                    flush.zero_()
+                    torch.cuda.synchronize()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    h.dmc(1, 1, delta, etrial, mmult, mage)
+                    e1.record(stream)
+                    e1.synchronize()
+                    dev_ms += e0.elapsed_time(e1)
+                blk, norm = h.block_get()
+                means.append(blk[0] / norm)
+            c1 = h.counters()
+            means = np.array(means)
+            out[prec] = {"walker_moves_per_s": nw * nb * per / (dev_ms * 1e-3),
+                         "ms_per_step": dev_ms / (nb * per),
+                         "e_mean": float(means.mean()),
+                         "e_err": float(means.std(ddof=1) / math.sqrt(len(means))),
+                         "acceptance": (c1["accepted"] - c0["accepted"]) /
+                                       max(c1["proposed"] - c0["proposed"], 1)}
+    # per-configuration error of the mixed form against the FP64 path
+    x = start["x"][:512]
+    res = {}
+    for prec in ("fp64", "mixed"):
+        with q.Handle(sysobj, capacity=len(x), seed=1) as h:
+            h.set_precision(prec)
+            res[prec] = h.compute_properties(x)
+    de = np.abs(res["mixed"][2][:, 0] - res["fp64"][2][:, 0])
+    dl = np.abs(res["mixed"][2][:, 1] - res["fp64"][2][:, 1])
+    ratio = out["mixed"]["walker_moves_per_s"] / out["fp64"]["walker_moves_per_s"]
+    comb = math.hypot(out["mixed"]["e_err"], out["fp64"]["e_err"])
+    line = {
+        "metric": ("walker-moves/sec ratio, mixed precision over plain FP64 (DMC with "
+                   f"backflow, N=58 r_s={rs:g}, {nw} walkers, same E_L error)"),
+        "value": ratio, "unit": "x", "n_gpus": 1, "steps": nb * per, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 / f64 with f32 u2 and v2 pair terms", "data": "synthetic",
+        "config": {"workload": workload, "walkers_per_gpu": nw, "N": 58, "rs": rs,
+                   "tau": delta, "l2": "flushed between timed steps (256 MiB write)"},
+        "fp64": out["fp64"], "mixed": out["mixed"],
+        "per_configuration_vs_fp64": {"configs": len(x), "max_abs_dE_L_ry_per_el": float(de.max()),
+                                      "rms_dE_L_ry_per_el": float(np.sqrt((de ** 2).mean())),
+                                      "max_abs_d_minus_ln_psi": float(dl.max())},
+        "mean_energy_difference_in_combined_errors":
+            (out["mixed"]["e_mean"] - out["fp64"]["e_mean"]) / max(comb, 1e-300),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def serve_arm(args, rank, world):
     """The serving stream: Poisson arrivals (20 requests/s, seeded) of
     state points on the closed shells 26..162 that the kernels hold, r_s
@@ -985,11 +1093,16 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="pair passes in FP64 (default), or u2 and real-space Ewald pair terms "
                          "in FP32 with compensated sums")
-    ap.add_argument("--workload", default="dmc", choices=["dmc", "vmc", "rmc", "serve", "batch"],
+    ap.add_argument("--workload", default="dmc",
+                    choices=["dmc", "vmc", "rmc", "serve", "batch", "precision"],
                     help="dmc: the N=58 DMC generation (default); vmc: plain VMC N=26 r_s=1, "
                          "256 walkers; rmc: reptation N=58 r_s=10, 512 reptiles x 200 beads; "
                          "serve: the serving stream; batch: 64 uneven populations through "
                          "one graph")
+    ap.add_argument("--global-comb", action="store_true",
+                    help="dmc workload over N ranks as one population: branch2's comb over "
+                         "all ranks' walkers and the walker exchange every generation "
+                         "(default: independent populations per rank)")
     ap.add_argument("--single", action="store_true",
                     help="vmc workload with single-electron moves and Sherman-Morrison updates")
     ap.add_argument("--rmc-n", type=int, default=58, choices=[26, 58],
@@ -1022,6 +1135,8 @@ def main():
         return batch_arm(args, rank, world)
     if args.workload in ("vmc", "rmc"):
         return config_arm(args, rank, world, local_rank)
+    if args.workload == "precision":
+        return precision_arm(args, rank, world, local_rank)
     return b200_arm(args, rank, world, local_rank)
 
 
