@@ -305,6 +305,11 @@ class Handle:
         and pair-row staging (0 when it fits, 1 never)."""
         self._chk(self.lib.qmc2d_set_launch(self.h, groups, stage))
 
+    def set_inversion(self, layout):
+        """0: register-resident Gauss-Jordan over every warp (default); 1: one
+        warp per spin in shared memory."""
+        self._chk(self.lib.qmc2d_set_inversion(self.h, layout))
+
     def autotune(self):
         """Time the pair kernel's launch choices on the current population,
         keep the fastest; returns (groups, stage, ms per launch)."""

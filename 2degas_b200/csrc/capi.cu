@@ -390,6 +390,18 @@ extern "C" int qmc2d_set_launch(qmc2d_handle *h, int groups, int stage) {
   return QMC2D_OK;
 }
 
+extern "C" int qmc2d_set_inversion(qmc2d_handle *h, int layout) {
+  if (!h || layout < 0 || layout > 1) {
+    q2d::set_error("qmc2d_set_inversion: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  h->hs.tune_inv = layout;
+  CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return QMC2D_OK;
+}
+
 extern "C" int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *ms) {
   if (!h) return QMC2D_ERR_ARG;
   if (h->nw <= 0) {

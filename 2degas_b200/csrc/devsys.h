@@ -53,6 +53,11 @@ struct DevSys {
   // groups per CTA (0: the default, 2) and the staging of the pair rows in
   // shared memory (0: when they fit, 1: never).
   int tune_groups, tune_stage;
+  // Inversion layout of the determinant section (qmc2d_set_inversion):
+  // 0 the register-resident Gauss-Jordan over every warp (4 warps per
+  // spin, one CTA barrier per pivot step); 1 one warp per spin in shared
+  // memory (warp-synchronous steps) with rho_k on the other warps.
+  int tune_inv;
   // Determinants too large for one CTA's shared memory (gmat = 1): the
   // orbital, inversion, F and cross-term matrices of walker (CTA) b live at
   // gmat_base + b * gmat_stride (doubles) in global memory; everything

@@ -1279,9 +1279,21 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
     // with rho_k on the other warps
     // (determinants in HBM: every warp, coalesced rows, then rho_k)
     const int Gr = gj_reg_warps(nt);
-    bool reg_path = !kGmat;
+    bool reg_path = !kGmat && S.tune_inv == 0;
     for (int sp = 0; sp < nt; sp++) reg_path = reg_path && gj_reg_lanes(S.np[sp], 32 * Gr) > 0;
-    if (reg_path) {
+    if (!kGmat && S.tune_inv == 1) {
+      // one warp per spin, warp-synchronous pivot steps; rho_k on the rest
+      const int w = tid >> 5;
+      if (w < nt) {
+        const int ns = S.np[w];
+        gj_invert(w ? m.W[1] : m.W[0], ws_ld(ns), ns, w ? m.perm[1] : m.perm[0],
+                  w ? m.dk[1] : m.dk[0], w ? m.used[1] : m.used[0], &m.iscal[w], tid & 31, 1,
+                  1 + w, m.gval + 8 * w, m.gidx + 8 * w);
+      } else {
+        rhok(tid - 32 * nt, kThreads - 32 * nt);
+      }
+      __syncthreads();
+    } else if (reg_path) {
       const int sp = nt > 1 ? (tid >> 5) / Gr : 0, gt = tid - sp * 32 * Gr;
       gj_invert_reg(sp ? m.W[1] : m.W[0], ws_ld(S.np[sp]), S.np[sp], sp ? m.perm[1] : m.perm[0],
                     sp ? m.dk[1] : m.dk[0], &m.iscal[sp], gt, Gr, 1 + sp,

@@ -356,6 +356,8 @@ def b200_arm(args, rank, world, local_rank):
     x0 = sysobj.read_configs(d, ".0", 0, nw)
     h = q.Handle(sysobj, capacity=nw, seed=walker_seed, device=local_rank)
     h.set_precision(args.precision)
+    if args.inversion is not None:
+        h.set_inversion(args.inversion)
     h.population_set(x0)
     h.vmc(args.equil, delta, 10 ** 9)  # seeded VMC equilibration
     tuned = h.autotune()  # pair-kernel launch choice, timed on this population
@@ -1103,6 +1105,8 @@ def main():
                     help="dmc workload over N ranks as one population: branch2's comb over "
                          "all ranks' walkers and the walker exchange every generation "
                          "(default: independent populations per rank)")
+    ap.add_argument("--inversion", type=int, default=None, choices=[0, 1],
+                    help="determinant inversion layout (qmc2d_set_inversion)")
     ap.add_argument("--single", action="store_true",
                     help="vmc workload with single-electron moves and Sherman-Morrison updates")
     ap.add_argument("--rmc-n", type=int, default=58, choices=[26, 58],

@@ -227,6 +227,14 @@ int qmc2d_set_dmc_ecut(qmc2d_handle *h, double ecut);
  * keeps the fastest and returns it with its time per launch. The reference
  * has no counterpart. */
 int qmc2d_set_launch(qmc2d_handle *h, int groups, int stage);
+/* Inversion layout of the determinant section (compute_properties, VMC,
+ * DMC, reptation) for determinants held in shared memory: 0 (the default)
+ * the register-resident Gauss-Jordan over every warp of the CTA, 1 one warp
+ * per spin in shared memory with rho_k on the other warps. Both pivot as
+ * zgefa does (the unused row of largest |re|+|im|, reptation.f:9079-9227)
+ * and give the same values up to round-off. The reference has no
+ * counterpart. */
+int qmc2d_set_inversion(qmc2d_handle *h, int layout);
 int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *ms);
 
 /* Batches: many independent populations (handles of different systems, on
