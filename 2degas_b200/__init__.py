@@ -194,7 +194,7 @@ class Handle:
         self._chk(self.lib.qmc2d_profile(self.h, 1 if enable else 0))
 
     PHASES = ("propose", "pairs", "rhok", "u3", "orbitals", "invert", "fmat", "drift",
-              "mbuild", "cross", "assemble", "accept")
+              "mbuild", "cross", "assemble", "accept", "path")
 
     def phase_timers(self, enable=True):
         """Start (enable) or stop and return {phase: SM cycles summed over CTAs}."""

@@ -349,6 +349,8 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
       }
     h->bf_zero = zero ? 1 : 0;
   }
+  h->hs.bf_zero = h->bf_zero;
+  cudaMemcpy(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice);
   cudaMemset(h->d_blk, 0, sizeof(double) * cap * np);
   cudaMemset(h->d_norm, 0, sizeof(double) * cap);
   cudaMemset(h->d_cnt, 0, sizeof(double) * cap * 4);

@@ -58,6 +58,11 @@ struct DevSys {
   // spin, one CTA barrier per pivot step); 1 one warp per spin in shared
   // memory (warp-synchronous steps) with rho_k on the other warps.
   int tune_inv;
+  // Every backflow table identically zero (set by the handle): q = x and the
+  // backflow Jacobian is the identity, so the pair passes skip the backflow
+  // terms and the determinant's drift and Laplacian come from the diagonals
+  // of F and D2 without the cross-term GEMM.
+  int bf_zero;
   // Determinants too large for one CTA's shared memory (gmat = 1): the
   // orbital, inversion, F and cross-term matrices of walker (CTA) b live at
   // gmat_base + b * gmat_stride (doubles) in global memory; everything
@@ -75,6 +80,7 @@ struct DevSys {
 enum : int {
   PH_PROPOSE = 0, PH_PAIRS = 1, PH_RHOK = 2, PH_U3 = 3, PH_ORBITALS = 4, PH_INVERT = 5,
   PH_FMAT = 6, PH_DRIFT = 7, PH_MBUILD = 8, PH_CROSS = 9, PH_ASSEMBLE = 10, PH_ACCEPT = 11,
+  PH_PATH = 12,  // reptation: path_props rescan, action deltas and the global accept
   PH_COUNT = 16
 };
 

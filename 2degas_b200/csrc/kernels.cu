@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
   const int N = S.N, N2 = 2 * N, np = S.nprops, nt = S.nt;
   const MoveScratch L = move_scratch(S);
   const double *o = a.scr + (size_t)w * L.stride;
-  if (S.has_bf) {
+  if (S.has_bf && !S.bf_zero) {
     // the pair values are read by the Jacobian build long after this point;
     // by now the pair kernel's writes for this walker have left L2, so bring
     // them back (bulk L2 prefetch, 32 KB per request; the block is 256-byte

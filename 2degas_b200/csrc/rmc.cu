@@ -255,6 +255,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
       int j = (jstart + idir * (idelta - 1) + nb) % nb;
       int jn = (jstart + idir * idelta + nb) % nb;
       uint32_t c3 = 3u + (uint32_t)(idelta - 1);
+      long long tph = clock64();
       Bead bj = bead(S, a, r, j), bn = bead(S, a, r, jn);
       double ww = 0, wg = 0, dd = 0;
       for (int k = tid; k < N2; k += blockDim.x) {
@@ -270,7 +271,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
       }
       double wold = block_sum(ww, m.red), dold = block_sum(dd, m.red);
       double lng = block_sum(wg, m.red);
-      long long tph = clock64();
+      phase_mark(S, PH_PROPOSE, tph);
       status |= eval_walker(S, m, hn, pn, sc, tph);
       double sn = sc[0];
       double wn = 0.0;
@@ -343,7 +344,9 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
       __syncthreads();
       if (tid == 0) bn.p[QMC2D_JACC] = p;
       __syncthreads();
+      phase_mark(S, PH_ACCEPT, tph);
     }
+    long long tpp = clock64();
     int kfirst = (jfirst + idir * ndelta + nb) % nb;
     int klast = (jlast + idir * ndelta + nb) % nb;
     path_props(S, a, r, kfirst, klast, pp);
@@ -403,6 +406,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
     for (int ip = tid; ip < S.nprops; ip += blockDim.x) blk[ip] += ppo[ip];
     norm += 1.0;
     __syncthreads();
+    phase_mark(S, PH_PATH, tpp);
   }
   for (int ip = tid; ip < S.nprops; ip += blockDim.x) {
     a.pp_old[(size_t)r * S.nprops + ip] = ppo[ip];

@@ -1099,7 +1099,7 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
             lap3.add(d3 + c3);
           }
         }
-        if (S.has_bf) {
+        if (S.has_bf && !S.bf_zero) {
           double t, dt, ddt;
           spline3<kSh>(Knots<double>(S), reinterpret_cast<const double *>(row + Lay::bf), remd, t,
                        dt, ddt);
@@ -1413,6 +1413,25 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
       }
       __syncthreads();
       phase_mark(S, PH_FMAT, tph);
+      if (S.bf_zero) {
+        // eta = 0: q = x and every Jacobian block is the identity, so only
+        // this spin's electrons see this determinant, the drift and phase
+        // gradient are the diagonals of F, and the Laplacian terms of the
+        // Jacobian build and of the cross term reduce to -tr D2(i) and
+        // sum_a Re F_a(i,i)^2 (no M, no GEMM)
+        for (int jl = tid; jl < ns; jl += kThreads) {
+          const int i = f0 + jl;
+          const double2 fx = m.F0[jl + jl * ns], fy = m.F1[jl + jl * ns];
+          m.gd[2 * i] -= fx.x;
+          m.gd[2 * i + 1] -= fy.x;
+          m.ph2d[i] += fx.y * fx.y + fy.y * fy.y;
+          m.lapd[i] += -(m.D2[3 * jl] + m.D2[3 * jl + 2]) +
+                       ((fx.x * fx.x - fx.y * fx.y) + (fy.x * fy.x - fy.y * fy.y));
+        }
+        __syncthreads();  // the next spin's F overwrites F0/F1
+        phase_mark(S, PH_CROSS, tph);
+        continue;
+      }
       // cross term: M (2n x 2n, row stride ldM, over A[sp], W[sp]; the
       // padding columns zero), then per chunk of 16 electrons Y = M U on
       // the FP64 tensor cores and the quadratic forms sum_p U(p,c) Y(p,c)

@@ -672,6 +672,19 @@ def config_arm(args, rank, world, local_rank):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    if args.phases:
+        # SM cycles per walker-move of each phase (thread 0 of every CTA)
+        h.phase_timers(True)
+        for _ in range(args.steps):
+            step()
+        ph = h.phase_timers(False)
+        tot = sum(ph.values())
+        print(json.dumps({"phases_cycles_per_move": {k: v / (nw * args.steps)
+                                                     for k, v in ph.items() if v},
+                          "share": {k: v / tot for k, v in ph.items() if v},
+                          "workload": name, "walkers": nw, "steps": args.steps}), flush=True)
+        h.close()
+        return 0
     if dist:
         dist.barrier()
     h.profile(True)
