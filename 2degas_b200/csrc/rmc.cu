@@ -49,6 +49,7 @@ struct RmcArgs {
   int ecut, rejection, wpiu, gstorto, nodalaction;
   double value_ecut;
   double *x, *g, *p, *h, *s, *age_stack, *w, *pp_old, *age;
+  double *psum;  // nrep * nprops: raw window sums of the accepted paths
   int *ends;
   double *blk, *blk_norm, *cnt;
   int *status;
@@ -84,21 +85,53 @@ __device__ __forceinline__ Bead bead(const DevSys &S, const RmcArgs &a, int r, i
 }
 
 // path_props scalar part: mean over beads 1+ntauskip..ntau-ntauskip from
-// kfirst; E_L is the mixed estimator of the two ends.
+// kfirst; E_L is the mixed estimator of the two ends. raw (when given)
+// receives the window sums before the division.
 __device__ void path_props(const DevSys &S, const RmcArgs &a, int r, int kfirst, int klast,
-                           double *pp) {
+                           double *pp, double *raw = nullptr) {
   for (int ip = threadIdx.x; ip < S.nprops; ip += blockDim.x) {
     double t = 0.0;
     for (int i = 1 + a.ntauskip; i <= a.ntau - a.ntauskip; i++) {
       int j = (kfirst + i - 1) % a.nbuf;
       t += bead(S, a, r, j).p[ip];
     }
+    if (raw) raw[ip] = t;
     pp[ip] = t / (a.ntau - 2 * a.ntauskip);
   }
   __syncthreads();
   if (threadIdx.x == 0)
     pp[QMC2D_JETOT] =
         0.5 * (bead(S, a, r, klast).p[QMC2D_JETOT] + bead(S, a, r, kfirst).p[QMC2D_JETOT]);
+  __syncthreads();
+}
+
+// The proposed path's window sums (the sums of path_props) from the
+// accepted path's, psum: the window of beads ntauskip .. ntau-ntauskip-1
+// after the first shifts by d = idir * ndelta ring slots, so |d| beads leave
+// at one end and |d| enter at the other; every bead of the old window is
+// still in its slot (the grown beads go to the spare slots beyond the ends).
+// A full rescan when the windows do not overlap or `full` (every 256th
+// step, so round-off of the running sums cannot build up).
+__device__ void path_sums(const DevSys &S, const RmcArgs &a, int r, int jfirst, int d,
+                          const double *psum, double *out, bool full) {
+  const int cnt = a.ntau - 2 * a.ntauskip, nb = a.nbuf;
+  const int e = d < 0 ? -d : d;
+  const int kf = (jfirst + d + nb) % nb;
+  for (int ip = threadIdx.x; ip < S.nprops; ip += blockDim.x) {
+    double t;
+    if (full || e >= cnt) {
+      t = 0.0;
+      for (int i = 0; i < cnt; i++) t += bead(S, a, r, (kf + a.ntauskip + i) % nb).p[ip];
+    } else {
+      t = psum[ip];
+      for (int q = 0; q < e; q++) {
+        const int out_slot = d > 0 ? jfirst + a.ntauskip + q : jfirst + a.ntauskip + cnt - 1 - q;
+        const int in_slot = d > 0 ? jfirst + a.ntauskip + cnt + q : kf + a.ntauskip + q;
+        t += bead(S, a, r, in_slot % nb).p[ip] - bead(S, a, r, out_slot % nb).p[ip];
+      }
+    }
+    out[ip] = t;
+  }
   __syncthreads();
 }
 
@@ -159,7 +192,7 @@ __global__ void rmc_init_kernel(const DevSys *sp, RmcArgs a) {
     }
   }
   __syncthreads();
-  path_props(S, a, r, 0, a.ntau - 1, pp);
+  path_props(S, a, r, 0, a.ntau - 1, pp, a.psum + (size_t)r * S.nprops);
   for (int i = 1; i <= a.ntau - 1; i++) {
     int j = i - 1, jn = i;
     double wnew, wold;
@@ -221,7 +254,8 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
   double *pp = pn + S.nprops;   // p_p_new
   double *ppo = pp + S.nprops;  // p_p_old
   double *blk = ppo + S.nprops;
-  double *hn = blk + S.nprops;
+  double *psum = blk + S.nprops;  // window sums of the accepted path
+  double *hn = psum + S.nprops;
   double *sc = hn + 2;
   const int r = blockIdx.x, tid = threadIdx.x;
   if (r >= a.nrep) return;
@@ -229,6 +263,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
   for (int ip = tid; ip < S.nprops; ip += blockDim.x) {
     ppo[ip] = a.pp_old[(size_t)r * S.nprops + ip];
     blk[ip] = a.blk[(size_t)r * S.nprops + ip];
+    psum[ip] = a.psum[(size_t)r * S.nprops + ip];
   }
   int jfirst = a.ends[2 * r], jlast = a.ends[2 * r + 1];
   double age = a.age[r];
@@ -349,7 +384,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
     long long tpp = clock64();
     int kfirst = (jfirst + idir * ndelta + nb) % nb;
     int klast = (jlast + idir * ndelta + nb) % nb;
-    path_props(S, a, r, kfirst, klast, pp);
+    path_sums(S, a, r, jfirst, idir * ndelta, psum, pp, (t & 255u) == 0u);
     double wnew = 0.0;
     if (tid == 0) {
       auto P = [&](int j) { return bead(S, a, r, j); };
@@ -394,9 +429,15 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
     double p = (age == a.mage_r) ? 1.0 : exp(fmin(0.0, fmax(-50.0, wnew)));
     double ua = u2(a.seed, 0xFFFFFFFDu, (uint32_t)r, t, 2u).x;
     if (p >= ua) {
+      const double rc = 1.0 / (a.ntau - 2 * a.ntauskip);
+      const double emix =
+          0.5 * (bead(S, a, r, klast).p[QMC2D_JETOT] + bead(S, a, r, kfirst).p[QMC2D_JETOT]);
       jfirst = kfirst;
       jlast = klast;
-      for (int ip = tid; ip < S.nprops; ip += blockDim.x) ppo[ip] = pp[ip];
+      for (int ip = tid; ip < S.nprops; ip += blockDim.x) {
+        psum[ip] = pp[ip];
+        ppo[ip] = ip == QMC2D_JETOT ? emix : pp[ip] * rc;
+      }
       age = 0.0;
       nacc += 1.0;
     } else {
@@ -411,6 +452,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
   for (int ip = tid; ip < S.nprops; ip += blockDim.x) {
     a.pp_old[(size_t)r * S.nprops + ip] = ppo[ip];
     a.blk[(size_t)r * S.nprops + ip] = blk[ip];
+    a.psum[(size_t)r * S.nprops + ip] = psum[ip];
   }
   if (tid == 0) {
     a.ends[2 * r] = jfirst;
@@ -552,8 +594,8 @@ __global__ void rmc_estimators_mean_kernel(const double *rows, int nrep, int nv,
 }  // namespace
 
 void rmc_free(RmcState *r) {
-  void *b[] = {r->x, r->g, r->p, r->h, r->s, r->age_stack, r->w, r->ends, r->pp_old, r->age,
-               r->est};
+  void *b[] = {r->x,    r->g,      r->p,    r->h,   r->s,   r->age_stack, r->w,
+               r->ends, r->pp_old, r->psum, r->age, r->est};
   for (void *p : b) cudaFree(p);
   *r = RmcState{};
 }
@@ -608,6 +650,7 @@ q2d::RmcArgs rmc_args(qmc2d_handle *h, int nstp) {
   a.age_stack = r.age_stack;
   a.w = r.w;
   a.pp_old = r.pp_old;
+  a.psum = r.psum;
   a.age = r.age;
   a.ends = r.ends;
   a.blk = h->d_blk;
@@ -618,7 +661,7 @@ q2d::RmcArgs rmc_args(qmc2d_handle *h, int nstp) {
 }
 
 size_t rmc_move_smem(const q2d::DevSys &s) {
-  return q2d::eval_carve(s, nullptr, nullptr) + sizeof(double) * (4 * (size_t)s.nprops + 16);
+  return q2d::eval_carve(s, nullptr, nullptr) + sizeof(double) * (5 * (size_t)s.nprops + 16);
 }
 
 }  // namespace
@@ -660,6 +703,7 @@ extern "C" int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params 
   RCK(cudaMalloc(&r.w, sizeof(double) * nb * 5));
   RCK(cudaMalloc(&r.ends, sizeof(int) * 2 * nrep));
   RCK(cudaMalloc(&r.pp_old, sizeof(double) * nrep * np));
+  RCK(cudaMalloc(&r.psum, sizeof(double) * nrep * np));
   RCK(cudaMalloc(&r.age, sizeof(double) * nrep));
   RCK(cudaMemsetAsync(r.w, 0, sizeof(double) * nb * 5, h->stream));
   RCK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * h->cap, h->stream));

@@ -20,6 +20,7 @@ struct RmcState {
   double *age_stack = nullptr, *w = nullptr;
   int *ends = nullptr;        // nrep * 2: jfirst, jlast
   double *pp_old = nullptr;   // nrep * nprops
+  double *psum = nullptr;     // nrep * nprops: the accepted path's window sums (path_props)
   double *age = nullptr;      // nrep
   uint32_t step = 0;
   double *est = nullptr;  // path estimators: nrep rows and their mean (qmc2d_rmc_estimators)
