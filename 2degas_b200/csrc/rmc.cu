@@ -192,7 +192,7 @@ __global__ void rmc_init_kernel(const DevSys *sp, RmcArgs a) {
     }
   }
   __syncthreads();
-  path_props(S, a, r, 0, a.ntau - 1, pp, a.psum + (size_t)r * S.nprops);
+  path_props(S, a, r, 0, a.ntau - 1, pp);
   for (int i = 1; i <= a.ntau - 1; i++) {
     int j = i - 1, jn = i;
     double wnew, wold;
@@ -207,6 +207,8 @@ __global__ void rmc_init_kernel(const DevSys *sp, RmcArgs a) {
   }
   for (int ip = threadIdx.x; ip < S.nprops; ip += blockDim.x)
     a.pp_old[(size_t)r * S.nprops + ip] = pp[ip];
+  // the window sums the moves update, with the bead acceptances just set
+  path_sums(S, a, r, 0, 0, nullptr, a.psum + (size_t)r * S.nprops, true);
   if (threadIdx.x == 0) {
     a.ends[2 * r] = 0;
     a.ends[2 * r + 1] = a.ntau - 1;
