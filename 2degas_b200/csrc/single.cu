@@ -91,6 +91,7 @@ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
 struct Sweep {
   double *x;        // 2N positions
   double2 *W[2];    // per spin n_s x n_s, W[j * n + k]
+  double2 *Dc[2];   // per spin n_s x n_s, Dc[j * n + k] = phi_k(r_j): the current orbitals
   double2 *Dsc;     // nmax x nmax: D of a refresh
   double2 *v, *t;   // nmax: new orbitals, W v (also the pivot column)
   int *perm;        // nmax row interchanges of a refresh
@@ -104,7 +105,7 @@ __host__ __device__ inline size_t al2(size_t n) { return (n + 1) & ~size_t(1); }
 __host__ __device__ inline size_t sweep_doubles(const DevSys &s) {
   const size_t N = s.N, nm = s.nmax;
   size_t d = al2(2 * N);
-  for (int t = 0; t < s.nt; t++) d += 2 * (size_t)s.np[t] * s.np[t];
+  for (int t = 0; t < s.nt; t++) d += 4 * (size_t)s.np[t] * s.np[t];
   d += 2 * nm * nm + 4 * nm + al2((nm + 1) / 2);
   d += al2(2 * N) + 4 * al2(N) + al2(4 * (size_t)s.nk) + al2(s.nprops);
   return d;
@@ -117,6 +118,10 @@ __device__ inline Sweep sweep_carve(const DevSys &s, double *p) {
   p += al2(2 * N);
   for (int t = 0; t < 2; t++) {
     m.W[t] = reinterpret_cast<double2 *>(p);
+    if (t < s.nt) p += 2 * (size_t)s.np[t] * s.np[t];
+  }
+  for (int t = 0; t < 2; t++) {
+    m.Dc[t] = reinterpret_cast<double2 *>(p);
     if (t < s.nt) p += 2 * (size_t)s.np[t] * s.np[t];
   }
   m.Dsc = reinterpret_cast<double2 *>(p);
@@ -237,6 +242,7 @@ __device__ double refresh_spin(const DevSys &S, const Sweep &m, int s, bool meas
     double sv, cv;
     sincos(g.x * m.x[2 * (f + j)] + g.y * m.x[2 * (f + j) + 1], &sv, &cv);
     m.Dsc[e] = make_double2(cv, sv);
+    m.Dc[s][j * n + k] = make_double2(cv, sv);
   }
   __syncwarp();
   double2 *W = m.W[s];
@@ -260,34 +266,6 @@ __device__ double refresh_spin(const DevSys &S, const Sweep &m, int s, bool meas
   return warp_invert(W, n, m.t, m.perm, lane, sing);
 }
 
-// -grad_i of the two-body Jastrow at position (px, py) of electron i (all
-// partners m != i), and sum_m u(r_im) when usum is given.
-__device__ __forceinline__ void jastrow_at(const DevSys &S, const Sweep &m, int i, double px,
-                                           double py, int lane, double &gx, double &gy,
-                                           double *usum) {
-  const int ti = type_of(S, i);
-  double ax = 0.0, ay = 0.0, u = 0.0;
-  if (S.has_u2)
-    for (int j = lane; j < S.N; j += 32) {
-      if (j == i) continue;
-      double rx = px - m.x[2 * j], ry = py - m.x[2 * j + 1];
-      rx = rx - S.el[0] * round(S.eli[0] * rx);
-      ry = ry - S.el[1] * round(S.eli[1] * ry);
-      const double r = sqrt(rx * rx + ry * ry);
-      const int ind = (int)(r * S.drti);
-      const double rem = r - ind * S.drt;
-      double f, df, ddf;
-      spline3(S, pair_row(S, ti, type_of(S, j), ind) + PR_U2, rem, f, df, ddf);
-      const double dtr = df / r;
-      ax += dtr * rx;
-      ay += dtr * ry;
-      u += f;
-    }
-  gx = wsum(ax);
-  gy = wsum(ay);
-  if (usum) *usum = wsum(u);
-}
-
 // The drift cutoff of kinetic (reptation.f:2748-2763) on one electron's g.
 __device__ __forceinline__ void cutoff(const DevSys &S, int ti, double &gx, double &gy) {
   if (S.adrift == 0.0) return;
@@ -297,35 +275,6 @@ __device__ __forceinline__ void cutoff(const DevSys &S, int ti, double &gx, doub
   gg = (-1.0 + sqrt(1.0 + 2.0 * gg)) / gg;
   gx *= gg;
   gy *= gg;
-}
-
-// grad ln D of column c of spin s at position (px, py): sum_k W(c,k) i g_k
-// phi_k; with vout, phi_k(p) is kept and R = sum_k W(c,k) phi_k returned.
-__device__ __forceinline__ double2 det_at(const DevSys &S, const Sweep &m, int s, int c,
-                                          double px, double py, int lane, double2 &Gx,
-                                          double2 &Gy, double2 *vout) {
-  const int n = S.np[s];
-  const double2 *W = m.W[s];
-  double a[6] = {0, 0, 0, 0, 0, 0};
-  for (int k = lane; k < n; k += 32) {
-    const double2 g = gv(S, k);
-    double sv, cv;
-    sincos(g.x * px + g.y * py, &sv, &cv);
-    const double2 phi = make_double2(cv, sv);
-    if (vout) vout[k] = phi;
-    const double2 wp = cmul(W[c * n + k], phi);
-    a[0] += wp.x;
-    a[1] += wp.y;
-    a[2] -= g.x * wp.y;  // i g_x (W phi)
-    a[3] += g.x * wp.x;
-    a[4] -= g.y * wp.y;
-    a[5] += g.y * wp.x;
-  }
-#pragma unroll
-  for (int q = 0; q < 6; q++) a[q] = wsum(a[q]);
-  Gx = make_double2(a[2], a[3]);
-  Gy = make_double2(a[4], a[5]);
-  return make_double2(a[0], a[1]);
 }
 
 // The properties of the walker's current configuration from W (the
@@ -395,11 +344,10 @@ __device__ int measure(const DevSys &S, const Sweep &m, const double logdet[2], 
     if (S.has_bf && !underflow) {
       const double2 *W = m.W[s];
       double2 Gx = make_double2(0, 0), Gy = Gx, L = Gx;
+      const double2 *Dc = m.Dc[s];
       for (int k = 0; k < n; k++) {
         const double2 g = gv(S, k);
-        double sv, cv;
-        sincos(g.x * m.x[2 * i] + g.y * m.x[2 * i + 1], &sv, &cv);
-        const double2 wp = cmul(W[c * n + k], make_double2(cv, sv));
+        const double2 wp = cmul(W[c * n + k], Dc[c * n + k]);
         Gx.x -= g.x * wp.y;
         Gx.y += g.x * wp.x;
         Gy.x -= g.y * wp.y;
@@ -425,11 +373,15 @@ __device__ int measure(const DevSys &S, const Sweep &m, const double logdet[2], 
     }
     m.g[2 * i] = gx;
     m.g[2 * i + 1] = gy;
-    const int o = s == 1 ? 4 : 0;
-    sums[o] += lp;
-    sums[o + 1] += x2;
-    sums[o + 2] += m.vp[i];
-    sums[o + 3] += ph;
+    const bool t1 = s == 1;  // compile-time indices: the sums stay in registers
+    sums[0] += t1 ? 0.0 : lp;
+    sums[1] += t1 ? 0.0 : x2;
+    sums[2] += t1 ? 0.0 : m.vp[i];
+    sums[3] += t1 ? 0.0 : ph;
+    sums[4] += t1 ? lp : 0.0;
+    sums[5] += t1 ? x2 : 0.0;
+    sums[6] += t1 ? m.vp[i] : 0.0;
+    sums[7] += t1 ? ph : 0.0;
   }
 #pragma unroll
   for (int q = 0; q < 9; q++) sums[q] = wsum(sums[q]);
@@ -512,7 +464,7 @@ __device__ int measure(const DevSys &S, const Sweep &m, const double logdet[2], 
   return status;
 }
 
-__global__ void __launch_bounds__(128) single_kernel(const DevSys *sp, SingleArgs a,
+__global__ void __launch_bounds__(128, 1) single_kernel(const DevSys *sp, SingleArgs a,
                                                      size_t per_warp) {
   __shared__ DevSys S;
   extern __shared__ __align__(16) double sm_single[];
@@ -544,28 +496,86 @@ __global__ void __launch_bounds__(128) single_kernel(const DevSys *sp, SingleArg
       spin_of(S, i, s, c, n);
       const double var = 2.0 * S.hbs2m[s] * a.delta, vari = 1.0 / var;
       const double xi = m.x[2 * i], yi = m.x[2 * i + 1];
-      // -grad_i ln|psi| at the old position
-      double jx, jy, uold;
-      jastrow_at(S, m, i, xi, yi, lane, jx, jy, &uold);
-      double2 Gx, Gy;
-      det_at(S, m, s, c, xi, yi, lane, Gx, Gy, nullptr);
-      double gx = jx - Gx.x, gy = jy - Gy.x;
-      cutoff(S, s, gx, gy);
-      // the proposal (move, reptation.f:4631-4646, for one electron)
+      // the draws first: they depend on nothing else
       const double2 u0 = uni2(a.seed, (uint32_t)(2 * i), (uint32_t)w, t, kTagSingle);
       const double2 u1 = uni2(a.seed, (uint32_t)(2 * i + 1), (uint32_t)w, t, kTagSingle);
+      const double ua = uni2(a.seed, 0x80000000u | (uint32_t)i, (uint32_t)w, t, kTagSingle).x;
+      const double2 *Wc = m.W[s] + c * n;
+      const double2 *Dcc = m.Dc[s] + c * n;
+      const int ti = s;
+      // -grad_i ln|psi| at the old position and sum_m u(r_im): the orbitals
+      // from the cache, the partners' splines, one butterfly for both
+      double o[5] = {0, 0, 0, 0, 0};  // Re G_x, Re G_y, J_x, J_y, u
+      for (int q = lane; q < (n > N ? n : N); q += 32) {
+        if (q < n) {
+          const double2 g = gv(S, q), wp = cmul(Wc[q], Dcc[q]);
+          o[0] -= g.x * wp.y;
+          o[1] -= g.y * wp.y;
+        }
+        if (q < N && q != i && S.has_u2) {
+          double rx = xi - m.x[2 * q], ry = yi - m.x[2 * q + 1];
+          rx = rx - S.el[0] * round(S.eli[0] * rx);
+          ry = ry - S.el[1] * round(S.eli[1] * ry);
+          const double r = sqrt(rx * rx + ry * ry);
+          const int ind = (int)(r * S.drti);
+          const double rem = r - ind * S.drt;
+          double f, df, ddf;
+          spline3(S, pair_row(S, ti, type_of(S, q), ind) + PR_U2, rem, f, df, ddf);
+          const double dtr = df / r;
+          o[2] += dtr * rx;
+          o[3] += dtr * ry;
+          o[4] += f;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 5; q++) o[q] = wsum(o[q]);
+      double gx = o[2] - o[0], gy = o[3] - o[1];
+      const double uold = o[4];
+      cutoff(S, s, gx, gy);
+      // the proposal (move, reptation.f:4631-4646, for one electron)
       const double pi = 3.141592653589793;
       const double cx = cos(pi * u0.x) * sqrt(-2.0 * var * log(u0.y));
       const double cy = cos(pi * u1.x) * sqrt(-2.0 * var * log(u1.y));
       const double nx = xi - var * gx + cx, ny = yi - var * gy + cy;
       const double wold = -(cx * cx + cy * cy) * vari;
-      // ratio and gradient at the new position
-      double2 Nx, Ny;
-      const double2 R = det_at(S, m, s, c, nx, ny, lane, Nx, Ny, m.v);
-      double ux, uy, unew;
-      jastrow_at(S, m, i, nx, ny, lane, ux, uy, &unew);
-      const double2 dgx = cdiv(Nx, R), dgy = cdiv(Ny, R);
-      double hx = ux - dgx.x, hy = uy - dgy.x;
+      // the ratio, grad ln D and the Jastrow at the new position
+      double e9[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // R, N_x, N_y (complex), J_x, J_y, u
+      for (int q = lane; q < (n > N ? n : N); q += 32) {
+        if (q < n) {
+          const double2 g = gv(S, q);
+          double sv, cv;
+          sincos(g.x * nx + g.y * ny, &sv, &cv);
+          m.v[q] = make_double2(cv, sv);
+          const double2 wp = cmul(Wc[q], make_double2(cv, sv));
+          e9[0] += wp.x;
+          e9[1] += wp.y;
+          e9[2] -= g.x * wp.y;
+          e9[3] += g.x * wp.x;
+          e9[4] -= g.y * wp.y;
+          e9[5] += g.y * wp.x;
+        }
+        if (q < N && q != i && S.has_u2) {
+          double rx = nx - m.x[2 * q], ry = ny - m.x[2 * q + 1];
+          rx = rx - S.el[0] * round(S.eli[0] * rx);
+          ry = ry - S.el[1] * round(S.eli[1] * ry);
+          const double r = sqrt(rx * rx + ry * ry);
+          const int ind = (int)(r * S.drti);
+          const double rem = r - ind * S.drt;
+          double f, df, ddf;
+          spline3(S, pair_row(S, ti, type_of(S, q), ind) + PR_U2, rem, f, df, ddf);
+          const double dtr = df / r;
+          e9[6] += dtr * rx;
+          e9[7] += dtr * ry;
+          e9[8] += f;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 9; q++) e9[q] = wsum(e9[q]);
+      const double2 R = make_double2(e9[0], e9[1]);
+      const double2 dgx = cdiv(make_double2(e9[2], e9[3]), R);
+      const double2 dgy = cdiv(make_double2(e9[4], e9[5]), R);
+      const double unew = e9[8];
+      double hx = e9[6] - dgx.x, hy = e9[7] - dgy.x;
       cutoff(S, s, hx, hy);
       const double bx = xi - nx + var * hx, by = yi - ny + var * hy;
       const double wnew = -(bx * bx + by * by) * vari;
@@ -573,23 +583,36 @@ __global__ void __launch_bounds__(128) single_kernel(const DevSys *sp, SingleArg
       double p = 2.0 * lnr + 0.5 * (wnew - wold);
       p = exp(fmin(0.0, fmax(-50.0, p)));
       if (!(R.x * R.x + R.y * R.y > 0.0)) p = 0.0;
-      const double ua = uni2(a.seed, 0x80000000u | (uint32_t)i, (uint32_t)w, t, kTagSingle).x;
       psum += p;
       if (p >= ua) {
         // Sherman-Morrison: column c of D becomes v
         double2 *W = m.W[s];
         for (int j = lane; j < n; j += 32) {
-          double re = 0.0, im = 0.0;
-          for (int k = 0; k < n; k++) {
-            const double2 wv = cmul(W[j * n + k], m.v[k]);
-            re += wv.x;
-            im += wv.y;
+          double re0 = 0.0, im0 = 0.0, re1 = 0.0, im1 = 0.0;
+          int k = 0;
+          for (; k + 1 < n; k += 2) {
+            const double2 a0 = W[j * n + k], b0 = m.v[k];
+            const double2 a1 = W[j * n + k + 1], b1 = m.v[k + 1];
+            re0 += a0.x * b0.x - a0.y * b0.y;
+            im0 += a0.x * b0.y + a0.y * b0.x;
+            re1 += a1.x * b1.x - a1.y * b1.y;
+            im1 += a1.x * b1.y + a1.y * b1.x;
           }
-          m.t[j] = make_double2(re, im);
+          if (k < n) {
+            const double2 a0 = W[j * n + k], b0 = m.v[k];
+            re0 += a0.x * b0.x - a0.y * b0.y;
+            im0 += a0.x * b0.y + a0.y * b0.x;
+          }
+          m.t[j] = make_double2(re0 + re1, im0 + im1);
         }
         __syncwarp();
         const double2 Rc = m.t[c];
-        for (int k = lane; k < n; k += 32) W[c * n + k] = cdiv(W[c * n + k], Rc);
+        const double rd = 1.0 / (Rc.x * Rc.x + Rc.y * Rc.y);
+        const double2 rinv = make_double2(Rc.x * rd, -Rc.y * rd);
+        for (int k = lane; k < n; k += 32) {
+          W[c * n + k] = cmul(W[c * n + k], rinv);
+          m.Dc[s][c * n + k] = m.v[k];
+        }
         __syncwarp();
         for (int e = lane; e < n * n; e += 32) {
           const int j = e / n, k = e - j * n;
@@ -651,7 +674,12 @@ cudaError_t launch_single(const DevSys &hs, const DevSys *ds, const SingleArgs &
     return e;
   const size_t per = sweep_doubles(hs);
   const size_t room = (size_t)optin - sizeof(DevSys) - 64;
-  int wpb = 4;
+  int nsm = 0;
+  if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+    return e;
+  // spread small populations over the SMs (one walker per CTA), pack up to
+  // four per CTA when there are walkers enough to fill them
+  int wpb = a.nw >= 4 * 2 * nsm ? 4 : (a.nw >= 2 * 2 * nsm ? 2 : 1);
   while (wpb > 1 && wpb * per * sizeof(double) > room) wpb--;
   if (per * sizeof(double) > room) return cudaErrorInvalidConfiguration;
   const size_t sm = wpb * per * sizeof(double);
