@@ -491,6 +491,8 @@ __global__ void __launch_bounds__(128, 1) single_kernel(const DevSys *sp, Single
   for (int sw = 0; sw < a.nsweep; sw++) {
     const uint32_t t = a.sweep0 + (uint32_t)sw;
     double psum = 0.0;
+    long long tph = clock64();
+    const bool lead = lane == 0;
     for (int i = 0; i < N; i++) {
       int s, c, n;
       spin_of(S, i, s, c, n);
@@ -503,6 +505,11 @@ __global__ void __launch_bounds__(128, 1) single_kernel(const DevSys *sp, Single
       const double2 *Wc = m.W[s] + c * n;
       const double2 *Dcc = m.Dc[s] + c * n;
       const int ti = s;
+      // the Gaussian step (move, reptation.f:4633) is issued before the old
+      // position's sums, so its transcendental latency overlaps them
+      const double pi = 3.141592653589793;
+      const double cx = cos(pi * u0.x) * sqrt(-2.0 * var * log(u0.y));
+      const double cy = cos(pi * u1.x) * sqrt(-2.0 * var * log(u1.y));
       // -grad_i ln|psi| at the old position and sum_m u(r_im): the orbitals
       // from the cache, the partners' splines, one butterfly for both
       double o[5] = {0, 0, 0, 0, 0};  // Re G_x, Re G_y, J_x, J_y, u
@@ -516,12 +523,12 @@ __global__ void __launch_bounds__(128, 1) single_kernel(const DevSys *sp, Single
           double rx = xi - m.x[2 * q], ry = yi - m.x[2 * q + 1];
           rx = rx - S.el[0] * round(S.eli[0] * rx);
           ry = ry - S.el[1] * round(S.eli[1] * ry);
-          const double r = sqrt(rx * rx + ry * ry);
+          const double r2 = rx * rx + ry * ry, byr = rsqrt(r2), r = r2 * byr;
           const int ind = (int)(r * S.drti);
           const double rem = r - ind * S.drt;
           double f, df, ddf;
           spline3(S, pair_row(S, ti, type_of(S, q), ind) + PR_U2, rem, f, df, ddf);
-          const double dtr = df / r;
+          const double dtr = df * byr;
           o[2] += dtr * rx;
           o[3] += dtr * ry;
           o[4] += f;
@@ -533,11 +540,9 @@ __global__ void __launch_bounds__(128, 1) single_kernel(const DevSys *sp, Single
       const double uold = o[4];
       cutoff(S, s, gx, gy);
       // the proposal (move, reptation.f:4631-4646, for one electron)
-      const double pi = 3.141592653589793;
-      const double cx = cos(pi * u0.x) * sqrt(-2.0 * var * log(u0.y));
-      const double cy = cos(pi * u1.x) * sqrt(-2.0 * var * log(u1.y));
       const double nx = xi - var * gx + cx, ny = yi - var * gy + cy;
       const double wold = -(cx * cx + cy * cy) * vari;
+      phase_mark(S, PH_PROPOSE, tph, lead);
       // the ratio, grad ln D and the Jastrow at the new position
       double e9[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // R, N_x, N_y (complex), J_x, J_y, u
       for (int q = lane; q < (n > N ? n : N); q += 32) {
@@ -558,12 +563,12 @@ __global__ void __launch_bounds__(128, 1) single_kernel(const DevSys *sp, Single
           double rx = nx - m.x[2 * q], ry = ny - m.x[2 * q + 1];
           rx = rx - S.el[0] * round(S.eli[0] * rx);
           ry = ry - S.el[1] * round(S.eli[1] * ry);
-          const double r = sqrt(rx * rx + ry * ry);
+          const double r2 = rx * rx + ry * ry, byr = rsqrt(r2), r = r2 * byr;
           const int ind = (int)(r * S.drti);
           const double rem = r - ind * S.drt;
           double f, df, ddf;
           spline3(S, pair_row(S, ti, type_of(S, q), ind) + PR_U2, rem, f, df, ddf);
-          const double dtr = df / r;
+          const double dtr = df * byr;
           e9[6] += dtr * rx;
           e9[7] += dtr * ry;
           e9[8] += f;
@@ -584,6 +589,7 @@ __global__ void __launch_bounds__(128, 1) single_kernel(const DevSys *sp, Single
       p = exp(fmin(0.0, fmax(-50.0, p)));
       if (!(R.x * R.x + R.y * R.y > 0.0)) p = 0.0;
       psum += p;
+      phase_mark(S, PH_PAIRS, tph, lead);
       if (p >= ua) {
         // Sherman-Morrison: column c of D becomes v
         double2 *W = m.W[s];
@@ -628,12 +634,15 @@ __global__ void __launch_bounds__(128, 1) single_kernel(const DevSys *sp, Single
         logdet[s] += 0.5 * log(Rc.x * Rc.x + Rc.y * Rc.y);
         nacc += 1.0;
       }
+      phase_mark(S, PH_ACCEPT, tph, lead);
       if (a.refresh > 0 && ++since >= a.refresh) {
         for (int q = 0; q < S.nt; q++) logdet[q] = refresh_spin(S, m, q, true, &drift, lane, &sing);
         since = 0;
+        phase_mark(S, PH_INVERT, tph, lead);
       }
     }
     status |= measure(S, m, logdet, lane, hl);
+    phase_mark(S, PH_ASSEMBLE, tph, lead);
     if (lane == 0) m.props[QMC2D_JACC] = psum / N;
     __syncwarp();
     for (int ip = lane; ip < S.nprops; ip += 32) blk[ip] += m.props[ip];

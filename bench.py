@@ -266,11 +266,13 @@ def workload_desc(args, world):
         nw = args.walkers if args.walkers != 4096 else 256
         if args.single:
             metric = (f"walker-moves/sec (VMC, N=26 r_s={rs:g}, {nw} walkers; single-electron "
-                      f"moves, one sweep of N moves = one walker-move)")
+                      f"moves, one sweep of N moves = one walker-move, {SINGLE_SWEEPS} sweeps "
+                      f"per step)")
         else:
             metric = f"walker-moves/sec (VMC, N=26 r_s={rs:g}, {nw} walkers)"
         cfg = {"workload": VMC_CONFIG, "walkers_per_gpu": nw, "N": 26, "rs": rs,
-               "tau": 0.045 * rs * rs, "moves_per_step": nw * world,
+               "tau": 0.045 * rs * rs,
+               "moves_per_step": nw * world * (SINGLE_SWEEPS if args.single else 1),
                "moves": "single-electron sweeps, inverse recomputed every 50 moves"
                if args.single else "all-electron"}
     elif args.workload == "rmc":
@@ -514,6 +516,9 @@ def b200_arm(args, rank, world, local_rank):
 
 # ------------------------------------------------ configs 0 and 2 (VMC, RQMC)
 VMC_CONFIG, RMC_CONFIG = "vmc_n26_rs1", "rmc_n58_rs10"
+# sweeps per call of the single-electron workload: the inverse stays resident
+# within a call, and each call starts from a fresh one
+SINGLE_SWEEPS = 10
 
 
 def _vmc_cpu_worker(args):
@@ -634,6 +639,7 @@ def config_arm(args, rank, world, local_rank):
     N, nt, npr = sysobj.N, sysobj.ntypes, sysobj.nprops
     ns = [sysobj.s.np[t] for t in range(nt)]
     x0 = sysobj.read_configs(d, ".0", 0, nw)
+    nw_moves = 1  # walker-moves per walker in one step
     if vmc and args.single:
         delta = 0.045 * rs * rs
         h = q.Handle(sysobj, capacity=nw, seed=walker_seed, device=local_rank)
@@ -642,8 +648,9 @@ def config_arm(args, rank, world, local_rank):
         tuned = None
 
         def step():
-            h.vmc_single(1, delta, 50)
+            h.vmc_single(SINGLE_SWEEPS, delta, 50)
         kernels = (capi.KERNEL_SINGLE,)
+        nw_moves = SINGLE_SWEEPS
     elif vmc:
         delta = 0.045 * rs * rs
         h = q.Handle(sysobj, capacity=nw, seed=walker_seed, device=local_rank)
@@ -707,7 +714,7 @@ def config_arm(args, rank, world, local_rank):
     blk, norm = h.block_get()
     acc = h.counters()
     t_max = max_over_ranks(dev_ms, dist, "cuda")
-    value = whole_job_rate(world, nw, args.steps, t_max * 1e-3)
+    value = whole_job_rate(world, nw * nw_moves, args.steps, t_max * 1e-3)
 
     # e2e through the public C-ABI with pinned host buffers every step
     k2 = max(3, args.steps // 2)
@@ -741,7 +748,7 @@ def config_arm(args, rank, world, local_rank):
         e2e_step()
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
-    e2e = whole_job_rate(world, nw, k2, e2e_s)
+    e2e = whole_job_rate(world, nw * nw_moves, k2, e2e_s)
 
     line = None
     if rank == 0:
@@ -753,7 +760,7 @@ def config_arm(args, rank, world, local_rank):
                flops_per_move(N, ns, K, 0 if vmc else 1, 0 if vmc else 1))
         kern_ms = sum(kms[k][0] for k in kernels)
         n_launch = max(kms[kernels[-1]][1], 1)
-        achieved = fpm * nw / (kern_ms / n_launch * 1e-3) / 1e12
+        achieved = fpm * nw * nw_moves / (kern_ms / n_launch * 1e-3) / 1e12
         peak = fp64_peak_tflops(torch)
         cpu = None
         if world == 1 and not args.no_cpu:
