@@ -216,17 +216,22 @@ __global__ void rmc_init_kernel(const DevSys *sp, RmcArgs a) {
   }
 }
 
+// Evaluate beads b0 .. b0 + gridDim.x - 1 (reptile-major). With kGmat the
+// CTA's determinant matrices take walker block blockIdx.x of the handle's
+// device memory, so a launch covers at most the handle's capacity.
+template <bool kGmat>
 __global__ void __launch_bounds__(kThreads, 2) rmc_eval_beads_kernel(const DevSys *sp, RmcArgs a,
-                                                                  const double *x) {
+                                                                  const double *x, int b0) {
   __shared__ DevSys S;
   extern __shared__ __align__(16) char smem[];
   load_sys(S, sp);
   EvalSmem m;
-  size_t off = eval_carve<0>(S, smem, &m);
+  size_t off = eval_carve<kGmat>(S, smem, &m, kGmat ? gmat_block(S, blockIdx.x) : nullptr);
   double *pn = reinterpret_cast<double *>(smem + off);
   double *hn = pn + S.nprops;
   double *sn = hn + 2;
-  const int r = blockIdx.x / a.ntau, i = blockIdx.x % a.ntau;
+  const int bead_id = b0 + blockIdx.x;
+  const int r = bead_id / a.ntau, i = bead_id % a.ntau;
   const int N2 = 2 * S.N;
   Bead b = bead(S, a, r, i);
   for (int k = threadIdx.x; k < N2; k += blockDim.x) {
@@ -236,7 +241,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_eval_beads_kernel(const DevSy
   }
   __syncthreads();
   long long tph = clock64();
-  int st = eval_walker(S, m, hn, pn, sn, tph);
+  int st = eval_walker<double, kGmat>(S, m, hn, pn, sn, tph);
   for (int k = threadIdx.x; k < N2; k += blockDim.x) b.g[k] = m.g[k];
   for (int k = threadIdx.x; k < S.nprops; k += blockDim.x) b.p[k] = pn[k];
   if (threadIdx.x == 0) {
@@ -246,12 +251,15 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_eval_beads_kernel(const DevSy
   }
 }
 
+// One CTA per reptile; with kGmat reptile r's determinant matrices take
+// walker block r of the handle's device memory (nrep <= capacity).
+template <bool kGmat>
 __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp, RmcArgs a) {
   __shared__ DevSys S;
   extern __shared__ __align__(16) char smem[];
   load_sys(S, sp);
   EvalSmem m;
-  size_t off = eval_carve<0>(S, smem, &m);
+  size_t off = eval_carve<kGmat>(S, smem, &m, kGmat ? gmat_block(S, blockIdx.x) : nullptr);
   double *pn = reinterpret_cast<double *>(smem + off);
   double *pp = pn + S.nprops;   // p_p_new
   double *ppo = pp + S.nprops;  // p_p_old
@@ -309,7 +317,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
       double wold = block_sum(ww, m.red), dold = block_sum(dd, m.red);
       double lng = block_sum(wg, m.red);
       phase_mark(S, PH_PROPOSE, tph);
-      status |= eval_walker(S, m, hn, pn, sc, tph);
+      status |= eval_walker<double, kGmat>(S, m, hn, pn, sc, tph);
       double sn = sc[0];
       double wn = 0.0;
       for (int k = tid; k < N2; k += blockDim.x) {
@@ -675,11 +683,6 @@ extern "C" int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params 
     q2d::set_error("qmc2d_rmc_init: bad argument");
     return QMC2D_ERR_ARG;
   }
-  if (h->hs.gmat) {
-    q2d::set_error("qmc2d_rmc_init: reptation keeps the determinants in shared memory, "
-                   "and this system's do not fit there");
-    return QMC2D_ERR_LIMIT;
-  }
   RCK(cudaSetDevice(h->device));
   RCK(cudaStreamSynchronize(h->stream));
   q2d::rmc_free(&h->rmc);
@@ -715,9 +718,20 @@ extern "C" int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params 
   RCK(cudaMemcpyAsync(dx, x, sizeof(double) * nx, cudaMemcpyHostToDevice, h->stream));
   q2d::RmcArgs a = rmc_args(h, 0);
   size_t sm = q2d::eval_smem_bytes(h->hs);
-  RCK(q2d::raise_smem_limit((const void *)q2d::rmc_eval_beads_kernel, sm));
-  q2d::rmc_eval_beads_kernel<<<nrep * r.ntau, q2d::kThreads, sm, h->stream>>>(h->ds, a, dx);
-  RCK(cudaGetLastError());
+  const void *kb = h->hs.gmat ? (const void *)q2d::rmc_eval_beads_kernel<true>
+                              : (const void *)q2d::rmc_eval_beads_kernel<false>;
+  RCK(q2d::raise_smem_limit(kb, sm));
+  // with determinants in device memory a launch covers at most `capacity`
+  // beads, one walker block each
+  const int total = nrep * r.ntau, chunk = h->hs.gmat ? h->cap : total;
+  for (int b0 = 0; b0 < total; b0 += chunk) {
+    const int nb = total - b0 < chunk ? total - b0 : chunk;
+    if (h->hs.gmat)
+      q2d::rmc_eval_beads_kernel<true><<<nb, q2d::kThreads, sm, h->stream>>>(h->ds, a, dx, b0);
+    else
+      q2d::rmc_eval_beads_kernel<false><<<nb, q2d::kThreads, sm, h->stream>>>(h->ds, a, dx, b0);
+    RCK(cudaGetLastError());
+  }
   q2d::rmc_init_kernel<<<nrep, q2d::kThreads, sizeof(double) * np, h->stream>>>(h->ds, a);
   RCK(cudaGetLastError());
   RCK(cudaStreamSynchronize(h->stream));
@@ -737,10 +751,15 @@ extern "C" int qmc2d_rmc(qmc2d_handle *h, int nstp) {
   RCK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * h->rmc.nrep, h->stream));
   q2d::RmcArgs a = rmc_args(h, nstp);
   size_t sm = rmc_move_smem(h->hs);
-  RCK(q2d::raise_smem_limit((const void *)q2d::rmc_move_kernel, sm));
+  const void *km = h->hs.gmat ? (const void *)q2d::rmc_move_kernel<true>
+                              : (const void *)q2d::rmc_move_kernel<false>;
+  RCK(q2d::raise_smem_limit(km, sm));
   {
     ProfScope ps(h, QMC2D_KERNEL_RMC, h->stream);
-    q2d::rmc_move_kernel<<<h->rmc.nrep, q2d::kThreads, sm, h->stream>>>(h->ds, a);
+    if (h->hs.gmat)
+      q2d::rmc_move_kernel<true><<<h->rmc.nrep, q2d::kThreads, sm, h->stream>>>(h->ds, a);
+    else
+      q2d::rmc_move_kernel<false><<<h->rmc.nrep, q2d::kThreads, sm, h->stream>>>(h->ds, a);
   }
   RCK(cudaGetLastError());
   h->rmc.step += (uint32_t)nstp;

@@ -495,9 +495,9 @@ typedef struct qmc2d_rmc_params {
 } qmc2d_rmc_params;
 
 /* read_path (reptation.f:1775): set up one reptile per slot from
- * nrep*ntau configurations (reptile-major, bead order). QMC2D_ERR_LIMIT
- * for a handle whose determinants live in device memory (qmc2d_create):
- * the reptation kernels keep them in shared memory. */
+ * nrep*ntau configurations (reptile-major, bead order); nrep is at most the
+ * handle's capacity. For systems whose determinants live in device memory
+ * (qmc2d_create) each reptile uses one walker slot's determinant block. */
 int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params *prm,
                    const double *x);
 /* nstp reptation moves (reptation_move + reptation_metropolis_test,

@@ -3,8 +3,8 @@ spin unpolarised, 49 polarised): the orbital, inversion, F and cross-term
 matrices of each walker live in a per-walker block of HBM, the rest of the
 walker in shared memory. Checked against the oracle at 49+49, 57 polarised,
 the largest unpolarised shell, 81+81 (N=162), and 121 and 161 polarised:
-the batched evaluation, VMC moves and DMC generations, bit for bit in the
-Philox stream."""
+the batched evaluation, VMC moves, DMC generations and reptation moves,
+bit for bit in the Philox stream."""
 import importlib
 import os
 
@@ -76,9 +76,34 @@ def test_footprint_counts_the_matrix_blocks(q, large):
     assert big - small >= 3 * len(x) * 16 * n * n
 
 
-def test_reptation_needs_the_matrices_in_shared_memory(q, large):
-    s, x, _ = large
-    with q.Handle(s, capacity=len(x), seed=1) as h:
-        with pytest.raises(q.QMCError) as e:
-            h.rmc_init(1, x[:4], 4, 1, 1, 0.01, -1.0, 50, 50)
-        assert "shared memory" in str(e.value)
+def test_reptation_matches_the_oracle(q, oracle_cls, large):
+    """Reptiles of these shells use one walker slot's determinant block each;
+    with capacity 2 the 6 beads of read_path are evaluated in three launches
+    of two."""
+    capi = importlib.import_module("2degas_b200._capi")
+    from oracle_lib import Reptile
+
+    s, x, rs = large
+    o = oracle_cls(s)
+    nrep, ntau, nstp = 2, 3, 4
+    delta = 0.01 * rs * rs
+    rng = np.random.default_rng(3)
+    st = rng.normal(0.0, np.sqrt(2.0 * delta / rs ** 2), size=(nrep, ntau, x.shape[1]))
+    st[:, 0] = 0.0
+    xp = (x[:nrep, None, :] + np.cumsum(st, axis=1)).reshape(nrep * ntau, -1)
+    prm = capi.RmcParams(ntau, 1, 1, delta, -1.0, 1000, 2)
+    paths, nacc_o = [], 0
+    for r in range(nrep):
+        rep = Reptile(o, prm)
+        rep.init(xp[r * ntau:(r + 1) * ntau])
+        _, na = rep.run(r, SEED, 0, nstp)
+        nacc_o += na
+        paths.append(rep.path())
+    with q.Handle(s, capacity=nrep, seed=SEED) as h:
+        h.rmc_init(nrep, xp, ntau, 1, 1, delta, -1.0, 1000, 2)
+        h.rmc(nstp)
+        assert h.counters()["accepted"] == nacc_o
+        for r in range(nrep):
+            xg, pg = h.rmc_get_path(r, ntau)
+            assert close(xg, paths[r][0]) < 1e-10
+            assert close(pg, paths[r][1]) < 1e-9
