@@ -310,6 +310,13 @@ class Handle:
         warp per spin in shared memory."""
         self._chk(self.lib.qmc2d_set_inversion(self.h, layout))
 
+    def get_launch(self):
+        """(pair-kernel walker groups, staging, inversion layout) in force."""
+        g, st, inv = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._chk(self.lib.qmc2d_get_launch(self.h, ctypes.byref(g), ctypes.byref(st),
+                                            ctypes.byref(inv)))
+        return g.value, st.value, inv.value
+
     def autotune(self):
         """Time the pair kernel's launch choices on the current population,
         keep the fastest; returns (groups, stage, ms per launch)."""

@@ -443,13 +443,51 @@ extern "C" int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *
       bs = v[1];
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   h->hs.tune_groups = bg;
   h->hs.tune_stage = bs;
+  // inversion layout of the determinant section, timed on the evaluation
+  // kernel over the population's configurations (into the staging buffers;
+  // the population is not changed)
+  if (h->hs.has_bf && !h->hs.gmat) {
+    double best_inv = 1e300;
+    int bi = 0;
+    for (int layout = 0; layout < 2; layout++) {
+      h->hs.tune_inv = layout;
+      CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
+      const q2d::DevPop &p = h->pop[h->cur];
+      CK(q2d::launch_eval(h->hs, h->ds, h->nw, p.x, h->d_g, h->d_h, h->d_p, h->d_s, h->d_status,
+                          h->stream));  // warm-up
+      CK(cudaEventRecord(e0, h->stream));
+      for (int r = 0; r < 3; r++)
+        CK(q2d::launch_eval(h->hs, h->ds, h->nw, p.x, h->d_g, h->d_h, h->d_p, h->d_s,
+                            h->d_status, h->stream));
+      CK(cudaEventRecord(e1, h->stream));
+      CK(cudaEventSynchronize(e1));
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, e0, e1));
+      if (t / 3.0 < best_inv) {
+        best_inv = t / 3.0;
+        bi = layout;
+      }
+    }
+    h->hs.tune_inv = bi;
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * h->nw, h->stream));
+  }
+  CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   if (groups) *groups = bg;
   if (stage) *stage = bs;
   if (ms) *ms = best;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_get_launch(qmc2d_handle *h, int *groups, int *stage, int *inversion) {
+  if (!h) return QMC2D_ERR_ARG;
+  if (groups) *groups = h->hs.tune_groups;
+  if (stage) *stage = h->hs.tune_stage;
+  if (inversion) *inversion = h->hs.tune_inv;
   return QMC2D_OK;
 }
 

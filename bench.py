@@ -486,7 +486,8 @@ def b200_arm(args, rank, world, local_rank):
             "dtype": "f64" if args.precision == "fp64" else "f64 (f32 u2 and v2 pair terms)",
             "data": "synthetic",
             "config": config,
-            "pair_launch": {"groups": tuned[0], "stage_rows": tuned[1] == 0},
+            "pair_launch": {"groups": tuned[0], "stage_rows": tuned[1] == 0,
+                            "inversion_layout": h.get_launch()[2]},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,

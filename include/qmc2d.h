@@ -235,7 +235,14 @@ int qmc2d_set_launch(qmc2d_handle *h, int groups, int stage);
  * and give the same values up to round-off. The reference has no
  * counterpart. */
 int qmc2d_set_inversion(qmc2d_handle *h, int layout);
+/* qmc2d_autotune also times the two inversion layouts on the evaluation
+ * kernel over the population's configurations (three launches each into the
+ * handle's staging buffers; the population is not changed) and keeps the
+ * faster; *ms is the chosen pair-kernel time per launch. */
 int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *ms);
+/* The launch choices in force: pair-kernel walker groups and staging, and
+ * the inversion layout. */
+int qmc2d_get_launch(qmc2d_handle *h, int *groups, int *stage, int *inversion);
 
 /* Batches: many independent populations (handles of different systems, on
  * one device) advanced together. The reference runs one population per
