@@ -1,7 +1,9 @@
 """Pair-kernel launch choices (qmc2d_set_launch) and their autotuner
 (qmc2d_autotune): every choice of walker groups per CTA and pair-row
 staging gives the same walkers bit for bit, and tuning leaves the
-population and the random streams where they were."""
+population and the random streams where they were. The autotuner also
+picks the inversion layout (qmc2d_set_inversion), whose two choices agree
+to round-off: bit for bit when it keeps the default, to 1e-12 otherwise."""
 import numpy as np
 import pytest
 
@@ -18,7 +20,7 @@ def _run(q, s, x, seed, launch=None, tune=False, nstp=3):
         got = None
         if tune:
             before = h.population_get()
-            got = h.autotune()
+            got = h.autotune() + (h.get_launch()[2],)
             after = h.population_get()
             assert np.array_equal(before["x"], after["x"])
         h.vmc(nstp, DELTA, 10 ** 9)
@@ -34,9 +36,13 @@ def test_every_launch_choice_gives_the_same_walkers(q, n26, n26_configs, launch)
 
 def test_autotune_picks_a_choice_and_changes_nothing(q, n26, n26_configs):
     ref, _ = _run(q, n26, n26_configs, 9)
-    got, (g, st, ms) = _run(q, n26, n26_configs, 9, tune=True)
-    assert g in (1, 2) and st in (0, 1) and ms > 0
-    assert np.array_equal(got["x"], ref["x"]) and np.array_equal(got["p"], ref["p"])
+    got, (g, st, ms, inv) = _run(q, n26, n26_configs, 9, tune=True)
+    assert g in (1, 2) and st in (0, 1) and inv in (0, 1) and ms > 0
+    if inv == 0:
+        assert np.array_equal(got["x"], ref["x"]) and np.array_equal(got["p"], ref["p"])
+    else:
+        assert np.allclose(got["x"], ref["x"], rtol=1e-12, atol=0)
+        assert np.allclose(got["p"], ref["p"], rtol=1e-10, atol=1e-12)
 
 
 def test_set_launch_rejects_bad_choices(q, n26, n26_configs):
