@@ -182,11 +182,14 @@ void free_pop(q2d::DevPop *p) {
 }
 
 int sync_status(qmc2d_handle *h, int nw) {
+  // the status words follow the kernels on the handle's stream into pinned
+  // host memory: one synchronisation for both
+  if (nw > 0)
+    CK(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(int) * nw, cudaMemcpyDeviceToHost,
+                       h->stream));
   CK(cudaStreamSynchronize(h->stream));
-  std::vector<int> st(nw > 0 ? nw : 1);
-  if (nw > 0) CK(cudaMemcpy(st.data(), h->d_status, sizeof(int) * nw, cudaMemcpyDeviceToHost));
   int any = 0;
-  for (int i = 0; i < nw; i++) any |= st[i];
+  for (int i = 0; i < nw; i++) any |= h->h_status[i];
   if (any & q2d::ST_SINGULAR) {
     q2d::set_error("zero pivot in a Slater matrix");
     return QMC2D_ERR_SINGULAR;
@@ -336,6 +339,8 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
       (e = dalloc(&h->d_blksum, (size_t)np + 1)) != cudaSuccess ||
       (e = dalloc(&h->d_sdrift, (size_t)cap)) != cudaSuccess)
     return fail(cuda_fail(e, "cudaMalloc"));
+  if ((e = cudaMallocHost((void **)&h->h_status, sizeof(int) * (size_t)cap)) != cudaSuccess)
+    return fail(cuda_fail(e, "cudaMallocHost"));
   // a backflow table of zeros only: the determinant of plain plane waves
   h->bf_zero = 0;
   if (h->hs.has_bf) {
@@ -520,6 +525,7 @@ extern "C" int qmc2d_destroy(qmc2d_handle *h) {
                   h->br.ecum, h->br.zrank, h->br.ncapped, h->d_x, h->d_g, h->d_h, h->d_p,
                   h->d_s, h->d_mscr, h->d_blksum, h->hs.phase, h->d_gmat, h->d_sdrift};
   for (void *b : bufs) cudaFree(b);
+  if (h->h_status) cudaFreeHost(h->h_status);
   for (int k = 0; k < QMC2D_NKERNELS; k++)
     for (cudaEvent_t e : h->ev[k]) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);

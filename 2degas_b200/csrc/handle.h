@@ -21,6 +21,7 @@ struct qmc2d_handle {
   q2d::DevPop pop[2]{};
   double *d_blk = nullptr, *d_norm = nullptr, *d_cnt = nullptr, *d_wate = nullptr;
   int *d_status = nullptr;
+  int *h_status = nullptr;  // cap status words in pinned host memory (sync_status)
   double *d_mscr = nullptr;  // move scratch: cap * move_scratch_doubles(hs)
   double *d_blksum = nullptr;  // n_props + 1: block sums over the population
   double *d_gmat = nullptr;    // cap * hs.gmat_stride: determinant matrices (hs.gmat)
