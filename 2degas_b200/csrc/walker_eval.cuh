@@ -1358,6 +1358,9 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
           for (int u = 0; u < 2; u++)
 #pragma unroll
             for (int v = 0; v < 2; v++) f0[u][v] = f1[u][v] = make_double2(0.0, 0.0);
+          // unrolled so that the permuted loads of later columns are in
+          // flight while earlier ones are used
+#pragma unroll 4
           for (int c = 0; c < ns; c++) {
             const int pc = pm[c];
             const double gx = m.gsh[2 * pc], gy = m.gsh[2 * pc + 1];
