@@ -398,7 +398,7 @@ extern "C" int qmc2d_set_launch(qmc2d_handle *h, int groups, int stage) {
 }
 
 extern "C" int qmc2d_set_inversion(qmc2d_handle *h, int layout) {
-  if (!h || layout < 0 || layout > 1) {
+  if (!h || layout < 0 || layout > 2) {
     q2d::set_error("qmc2d_set_inversion: bad argument");
     return QMC2D_ERR_ARG;
   }
@@ -456,7 +456,7 @@ extern "C" int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *
   if (h->hs.has_bf && !h->hs.gmat) {
     double best_inv = 1e300;
     int bi = 0;
-    for (int layout = 0; layout < 2; layout++) {
+    for (int layout = 0; layout < 3; layout++) {
       h->hs.tune_inv = layout;
       CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
       const q2d::DevPop &p = h->pop[h->cur];

@@ -48,6 +48,10 @@ struct EvalSmem {
   // inversion in global memory (gmat): each spin's panel, multipliers and
   // scaled pivot rows (gj_invert_gmem)
   double2 *fcol[2];
+  // blocked inversion with one-warp panels (gj_invert_panel): each spin's
+  // multipliers, scaled pivot rows, pivot reciprocals and rows (inside the
+  // F0 region, like gslot/gkey)
+  double2 *pscr[2];
 };
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
@@ -65,6 +69,13 @@ constexpr int kGjCols = 8;
 constexpr int kGjBlock = 8;
 __host__ __device__ inline size_t gj_gmem_scratch(int n) {
   return sizeof(double2) * (2 * (size_t)kGjBlock * n + kGjBlock) + sizeof(int) * kGjBlock;
+}
+
+// Per-spin scratch of gj_invert_panel (complex elements): multipliers and
+// scaled pivot rows of a block (kGjBlock x n each), the block's pivot
+// reciprocals and, in the last two elements, its pivot rows (ints).
+__host__ __device__ inline size_t gj_panel_scratch(int n) {
+  return 2 * (size_t)kGjBlock * n + kGjBlock + 2;
 }
 
 __host__ __device__ inline int gj_reg_lanes(int n, int nthr) {
@@ -135,6 +146,7 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
   t.dk[0] = t.dk[1] = nullptr;
   t.perm[0] = t.perm[1] = t.used[0] = t.used[1] = nullptr;
   t.fcol[0] = t.fcol[1] = nullptr;
+  t.pscr[0] = t.pscr[1] = nullptr;
   if (s.has_bf) {
     // A[s] and W[s] are adjacent: the 2n x 2n real cross-term matrix of spin
     // s (row stride xt_ldm) overlays them once F0/F1 are formed.
@@ -162,6 +174,8 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
     size_t sbytes = (sizeof(double2) * slot_per_spin + sizeof(unsigned long long) * 2 * gw) * 2;
     size_t rbytes = fbytes > ubytes ? fbytes : ubytes;
     if (sbytes > rbytes) rbytes = sbytes;
+    const size_t pbytes = sizeof(double2) * 2 * gj_panel_scratch(n);
+    if (!gm && pbytes > rbytes) rbytes = pbytes;
     t.F0 = (double2 *)mtake(rbytes);
     t.F1 = t.F0 ? t.F0 + n * n : nullptr;
     t.U = reinterpret_cast<double *>(t.F0);
@@ -170,6 +184,8 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
     t.gslot[1] = t.F0 ? t.F0 + slot_per_spin : nullptr;
     t.gkey[0] = t.F0 ? reinterpret_cast<unsigned long long *>(t.F0 + 2 * slot_per_spin) : nullptr;
     t.gkey[1] = t.gkey[0] ? t.gkey[0] + 2 * gw : nullptr;
+    t.pscr[0] = gm ? nullptr : t.F0;
+    t.pscr[1] = (gm || !t.F0) ? nullptr : t.F0 + gj_panel_scratch(n);
     t.D2 = (double *)take(sizeof(double) * 3 * n);
     t.fdg = (double *)take(sizeof(double) * 4 * n);
     t.gsh = (double *)take(sizeof(double) * 2 * n);
@@ -716,6 +732,139 @@ __device__ inline void gj_invert(double2 *W, int ld, int n, int *perm, double *d
 //     flight per warp: W(r, c) -= F[j][r] Q[j][c] for the block's steps in
 //     order (a pivot row starts from its Q and takes the later steps only).
 // scr: gj_gmem_scratch(n) bytes of shared memory.
+// Gauss-Jordan in blocks of kGjBlock pivot steps for a spin of n <= 32
+// orbitals in shared memory, by a group of G warps. Warp 0 factors each
+// panel of kGjBlock columns in registers (lane r holds row r), with its pivot
+// searches, broadcasts and eliminations warp-synchronous; then the group
+// forms the block's pivot rows outside the panel, scaled as at their step
+// (Q), and applies the block's steps to every row there, in step order. Three
+// group barriers per block instead of one per pivot step. Pivot rule,
+// outputs and per-element operations as gj_invert_gmem (the unused row of
+// largest |re|+|im|, ties to the lowest row; A^-1(k, pi(c)) = W(pi(k), c)).
+__device__ inline void gj_invert_panel(double2 *W, int ld, int n, int *perm, double *dk,
+                                       int *singular, int gt, int G, int bar_id,
+                                       double2 *scr) {
+  constexpr int B = kGjBlock;
+  const int nthr = 32 * G, lane = gt & 31, wg = gt >> 5;
+  double2 *F = scr;              // F[j * n + r]: multiplier of row r at step j
+  double2 *Q = scr + B * n;      // Q[j * n + c]: scaled pivot rows outside the panel
+  double2 *I = scr + 2 * B * n;  // I[j]: 1 / pivot of step j
+  int *PJ = reinterpret_cast<int *>(I + B);  // PJ[j]: pivot row of step j
+  auto gsync = [&]() {
+    if (G == 1) __syncwarp();
+    else asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthr) : "memory");
+  };
+  auto sub = [](double2 &v, double2 f, double2 a) {
+    v.x -= f.x * a.x - f.y * a.y;
+    v.y -= f.x * a.y + f.y * a.x;
+  };
+  bool used = lane >= n;  // warp 0: row `lane` has been a pivot
+  for (int k0 = 0; k0 < n; k0 += B) {
+    const int nb = min(B, n - k0);
+    if (wg == 0) {
+      const int r = lane;
+      const bool valid = r < n;
+      double2 pv[B];
+#pragma unroll
+      for (int j = 0; j < B; j++)
+        pv[j] = (valid && j < nb) ? W[r * ld + k0 + j] : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int j = 0; j < B; j++) {
+        if (j >= nb) break;
+        unsigned long long key = 0ull;
+        if (!used) {
+          const double a = fabs(pv[j].x) + fabs(pv[j].y);
+          key = ((unsigned long long)__double_as_longlong(a) & ~0xFFull) | (unsigned)(255 - r);
+        }
+        {
+          const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+          const unsigned hm = __reduce_max_sync(0xffffffffu, hi);
+          const unsigned lm = __reduce_max_sync(0xffffffffu, hi == hm ? lo : 0u);
+          key = ((unsigned long long)hm << 32) | lm;
+        }
+        // every unused row < n has 255 - r in its key's low byte, so p is
+        // such a row at every step, an exactly zero or NaN column included
+        const int p = 255 - (int)(key & 0xFFull);
+        double2 pr[B];
+#pragma unroll
+        for (int jj = 0; jj < B; jj++) {
+          pr[jj].x = __shfl_sync(0xffffffffu, pv[jj].x, p);
+          pr[jj].y = __shfl_sync(0xffffffffu, pv[jj].y, p);
+        }
+        const double2 piv = pr[j];
+        const double d = piv.x * piv.x + piv.y * piv.y;
+        const double rd = 1.0 / d;
+        const double2 inv = make_double2(piv.x * rd, -piv.y * rd);
+        if (lane == 0) {
+          perm[k0 + j] = p;
+          dk[k0 + j] = d;
+          I[j] = inv;
+          PJ[j] = p;
+          if ((key >> 8) == 0ull) *singular = 1;  // every candidate exactly zero
+        }
+        if (r == p) {
+          used = true;
+#pragma unroll
+          for (int jj = 0; jj < B; jj++) pv[jj] = (jj == j) ? inv : cmul(pv[jj], inv);
+        } else if (valid) {
+          const double2 fi = pv[j];
+          F[j * n + r] = fi;
+#pragma unroll
+          for (int jj = 0; jj < B; jj++)
+            if (jj != j) sub(pv[jj], fi, cmul(pr[jj], inv));
+          const double2 t = cmul(fi, inv);
+          pv[j] = make_double2(-t.x, -t.y);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < B; j++)
+        if (valid && j < nb) W[r * ld + k0 + j] = pv[j];
+    }
+    gsync();
+    // the block's pivot rows outside the panel, as scaled at their step
+    for (int c = gt; c < n; c += nthr) {
+      if (c >= k0 && c < k0 + nb) continue;
+      for (int j = 0; j < nb; j++) {
+        const int prow = PJ[j];
+        double2 x = W[prow * ld + c];
+        for (int jj = 0; jj < j; jj++) sub(x, F[jj * n + prow], Q[jj * n + c]);
+        Q[j * n + c] = cmul(x, I[j]);
+      }
+    }
+    gsync();
+    // every row, outside the panel: the block's steps in order
+    for (int r0 = wg; r0 < n; r0 += 4 * G) {
+      int role[4];  // -2: no row, -1: not a pivot of the block, j: pivot of step j
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int r = r0 + i * G;
+        role[i] = r < n ? -1 : -2;
+        for (int j = 0; j < nb; j++)
+          if (PJ[j] == r) role[i] = j;
+      }
+      for (int c = lane; c < n; c += 32) {
+        if (c >= k0 && c < k0 + nb) continue;
+        double2 v[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+          v[i] = role[i] == -2  ? make_double2(0.0, 0.0)
+                 : role[i] >= 0 ? Q[role[i] * n + c]
+                                : W[(r0 + i * G) * ld + c];
+        for (int j = 0; j < nb; j++) {
+          const double2 a = Q[j * n + c];
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+            if (role[i] != -2 && j > role[i]) sub(v[i], F[j * n + r0 + i * G], a);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+          if (role[i] != -2) W[(r0 + i * G) * ld + c] = v[i];
+      }
+    }
+    gsync();
+  }
+}
+
 __device__ inline void gj_invert_gmem(double2 *W, int ld, int n, int *perm, double *dk,
                                       int *used, int *singular, int gt, int G, int bar_id,
                                       double *gval, int *gidx, double2 *scr) {
@@ -1279,9 +1428,22 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
     // with rho_k on the other warps
     // (determinants in HBM: every warp, coalesced rows, then rho_k)
     const int Gr = gj_reg_warps(nt);
-    bool reg_path = !kGmat && S.tune_inv == 0;
+    bool reg_path = !kGmat && S.tune_inv != 1;
     for (int sp = 0; sp < nt; sp++) reg_path = reg_path && gj_reg_lanes(S.np[sp], 32 * Gr) > 0;
-    if (!kGmat && S.tune_inv == 1) {
+    bool panel_path = reg_path && S.tune_inv == 2;
+    for (int sp = 0; sp < nt; sp++) panel_path = panel_path && S.np[sp] <= 32;
+    if (panel_path) {
+      // blocks of eight pivot steps, one warp per panel, every warp of the
+      // spin's group on the rest; then rho_k on every warp
+      const int sp = nt > 1 ? (tid >> 5) / Gr : 0, gt = tid - sp * 32 * Gr;
+      gj_invert_panel(sp ? m.W[1] : m.W[0], ws_ld(S.np[sp]), S.np[sp],
+                      sp ? m.perm[1] : m.perm[0], sp ? m.dk[1] : m.dk[0], &m.iscal[sp], gt, Gr,
+                      1 + sp, sp ? m.pscr[1] : m.pscr[0]);
+      __syncthreads();
+      phase_mark(S, PH_INVERT, tph);
+      rhok(tid, kThreads);
+      __syncthreads();
+    } else if (!kGmat && S.tune_inv == 1) {
       // one warp per spin, warp-synchronous pivot steps; rho_k on the rest
       const int w = tid >> 5;
       if (w < nt) {

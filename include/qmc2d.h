@@ -230,10 +230,12 @@ int qmc2d_set_launch(qmc2d_handle *h, int groups, int stage);
 /* Inversion layout of the determinant section (compute_properties, VMC,
  * DMC, reptation) for determinants held in shared memory: 0 (the default)
  * the register-resident Gauss-Jordan over every warp of the CTA, 1 one warp
- * per spin in shared memory with rho_k on the other warps. Both pivot as
- * zgefa does (the unused row of largest |re|+|im|, reptation.f:9079-9227)
- * and give the same values up to round-off. The reference has no
- * counterpart. */
+ * per spin in shared memory with rho_k on the other warps, 2 blocks of
+ * eight pivot steps whose panels one warp factors in registers while the
+ * spin's other warps wait for the block update (spins of at most 32
+ * orbitals; larger ones take layout 0's route). All pivot as zgefa does (the
+ * unused row of largest |re|+|im|, reptation.f:9079-9227) and give the same
+ * values up to round-off. The reference has no counterpart. */
 int qmc2d_set_inversion(qmc2d_handle *h, int layout);
 /* qmc2d_autotune also times the two inversion layouts on the evaluation
  * kernel over the population's configurations (three launches each into the

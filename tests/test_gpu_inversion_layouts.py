@@ -1,7 +1,7 @@
-"""Both inversion layouts of the determinant section (qmc2d_set_inversion:
-0 register-resident over every warp, 1 one warp per spin in shared memory)
-against the oracle at 1e-10, and three VMC steps in layout 1 against the
-oracle's replay, on the n26 golden deck (13 + 13, u3, twist), the N = 58
+"""The inversion layouts of the determinant section (qmc2d_set_inversion:
+0 register-resident over every warp, 1 one warp per spin in shared memory,
+2 blocks of eight pivot steps with one-warp panels) against the oracle at
+1e-10, and three VMC steps in layouts 1 and 2 against the oracle's replay, on the n26 golden deck (13 + 13, u3, twist), the N = 58
 benchmark deck and a polarised shell of 25."""
 import importlib
 import os
@@ -35,7 +35,7 @@ def deck(request, q, tmp_path, n26, n26_configs):
     return s, s.read_configs(d, ".0", 0, 8)
 
 
-@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("layout", [0, 1, 2])
 def test_layout_matches_the_oracle(q, oracle_cls, deck, layout):
     s, x = deck
     o = oracle_cls(s)
@@ -49,13 +49,14 @@ def test_layout_matches_the_oracle(q, oracle_cls, deck, layout):
         assert close(hl[k], ho) < 1e-10
 
 
-def test_layout_one_vmc_replays_the_oracle(q, oracle_cls, deck):
+@pytest.mark.parametrize("layout", [1, 2])
+def test_layout_vmc_replays_the_oracle(q, oracle_cls, deck, layout):
     s, x = deck
     o = oracle_cls(s)
     pop = o.population_init(x)
     blk_o, nacc_o = o.vmc_philox(pop, 3, 0.05, 1000, SEED, 0)
     with q.Handle(s, capacity=len(x), seed=SEED) as h:
-        h.set_inversion(1)
+        h.set_inversion(layout)
         h.population_set(x)
         h.block_reset()
         h.vmc(3, 0.05, 1000)
