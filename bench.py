@@ -1126,7 +1126,7 @@ def main():
                     help="dmc workload over N ranks as one population: branch2's comb over "
                          "all ranks' walkers and the walker exchange every generation "
                          "(default: independent populations per rank)")
-    ap.add_argument("--inversion", type=int, default=None, choices=[0, 1],
+    ap.add_argument("--inversion", type=int, default=None, choices=[0, 1, 2],
                     help="determinant inversion layout (qmc2d_set_inversion)")
     ap.add_argument("--single", action="store_true",
                     help="vmc workload with single-electron moves and Sherman-Morrison updates")
