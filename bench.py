@@ -358,11 +358,11 @@ def b200_arm(args, rank, world, local_rank):
     x0 = sysobj.read_configs(d, ".0", 0, nw)
     h = q.Handle(sysobj, capacity=nw, seed=walker_seed, device=local_rank)
     h.set_precision(args.precision)
-    if args.inversion is not None:
-        h.set_inversion(args.inversion)
     h.population_set(x0)
     h.vmc(args.equil, delta, 10 ** 9)  # seeded VMC equilibration
-    tuned = h.autotune()  # pair-kernel launch choice, timed on this population
+    tuned = h.autotune()  # launch choices, timed on this population
+    if args.inversion is not None:  # a fixed inversion layout instead of the tuner's
+        h.set_inversion(args.inversion)
     h.block_reset()
     h.vmc(10, delta, 10 ** 9)
     blk, norm = h.block_get()
