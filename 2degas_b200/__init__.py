@@ -272,6 +272,11 @@ class Handle:
         prm = _capi.RmcParams(ntau, ntauskip, mdelta, delta, etrial, mage, mage_r)
         self._chk(self.lib.qmc2d_rmc_init(self.h, nrep, ctypes.byref(prm), _pd(x)))
 
+    def rmc_set_launch(self, split):
+        """1: pair kernel + determinant kernel per bead growth (default); 0: one
+        kernel per launch for whole moves."""
+        self._chk(self.lib.qmc2d_rmc_set_launch(self.h, split))
+
     def rmc(self, nstp):
         self._chk(self.lib.qmc2d_rmc(self.h, nstp))
 

@@ -67,6 +67,16 @@ __device__ __forceinline__ double fgg(const RmcArgs &a, double e, double gg) {
   return a.ecut == 0 ? e : a.value_ecut + (e - a.value_ecut) * gg;
 }
 
+// Direction and number of bead growths of reptile r's move t
+// (reptation_move, reptation.f:1915-1925): the same draw in every launch
+// of the move.
+__device__ __forceinline__ void rmc_dir(const RmcArgs &a, int r, uint32_t t, int &idir,
+                                        int &ndelta) {
+  const double2 dl = u2(a.seed, 0xFFFFFFF0u, (uint32_t)r, t, 2u);
+  idir = (dl.x - 0.5) >= 0.0 ? 1 : -1;
+  ndelta = 1 + (int)(dl.y * a.mdelta);
+}
+
 // Bead pointers of reptile r, ring slot j.
 struct Bead {
   double *x, *g, *p, *h, *s, *age, *w;
@@ -251,6 +261,182 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_eval_beads_kernel(const DevSy
   }
 }
 
+// The bead growth after its evaluation (reptation_move, reptation.f:1961-2104):
+// the reverse move, the bead's Langevin test (reptation_metropolis_test's
+// per-bead part), the w_stack entries of the link and the new bead jn (a
+// copy of bead j when rejected). m holds the proposal's positions and drift,
+// pn / hn / sc[0] its properties, -lap per type and sign. Every thread of
+// the CTA calls it.
+__device__ void bead_tail(const DevSys &S, const RmcArgs &a, const EvalSmem &m, int r,
+                          uint32_t t, int idir, int idelta, int j, int jn, double wold,
+                          double dold, double lng, const double *pn, const double *hn,
+                          const double *sc) {
+  const int tid = threadIdx.x, N2 = 2 * S.N, nt = S.nt;
+  const uint32_t c3 = 3u + (uint32_t)(idelta - 1);
+  Bead bj = bead(S, a, r, j), bn = bead(S, a, r, jn);
+  double sn = sc[0];
+  double wn = 0.0;
+  for (int k = tid; k < N2; k += blockDim.x) {
+    int ti = type_of(S, k >> 1);
+    double var = 2.0 * S.hbs2m[ti] * a.delta, vari = 1.0 / var;
+    double chi = bj.x[k] - m.x[k] - (-var * m.g[k]);
+    wn -= chi * chi * vari;
+  }
+  double wnew = block_sum(wn, m.red);
+  double p = 2 * (bj.p[QMC2D_JLTF] - pn[QMC2D_JLTF]) + 0.5 * (wnew - wold);
+  p = exp(fmin(0.0, fmax(-50.0, p)));
+  if (a.rejection == 0) p = 1.0;
+  else if (*bj.age == a.mage) p = 1.0;
+  if (*bj.s * sn < 0.0) p = 0.0;
+  double wg2 = a.delta * S.npnorm * (bj.p[QMC2D_JKIN0] + pn[QMC2D_JKIN0]);
+  double ua = u2(a.seed, 0xFFFFFFFEu, (uint32_t)r, t, c3).x;
+  bool rej = p < ua;
+  __syncthreads();
+  Bead ba = idir == 1 ? bj : bn, bb = idir == 1 ? bn : bj;
+  if (rej) {
+    if (tid == 0) {
+      ba.w[JDTP] = 0.5 * dold;
+      ba.w[JBRA] = -a.delta * S.npnorm * (fgg(a, bj.p[QMC2D_JETOT], bj.p[QMC2D_JGG]) - a.etrial);
+      bb.w[JITP] = 0.5 * dold;
+      ba.w[JLNG] = 0.5 * wg2;
+      double nds = 0.0;
+      for (int tt = 0; tt < nt; tt++) {
+        int ju = QMC2D_JUN(nt, tt);
+        double var = 2.0 * S.hbs2m[tt] * a.delta;
+        nds -= log(1.0 - exp(-bj.p[ju] * bj.p[ju] / (0.5 * var)));
+      }
+      ba.w[JNDS] = nds;
+      *bn.age = *bj.age + 1.0;
+      *bn.s = *bj.s;
+      for (int tt = 0; tt < nt; tt++) bn.h[tt] = bj.h[tt];
+    }
+    for (int k = tid; k < N2; k += blockDim.x) {
+      bn.x[k] = bj.x[k];
+      bn.g[k] = bj.g[k];
+    }
+    for (int k = tid; k < S.nprops; k += blockDim.x) bn.p[k] = bj.p[k];
+  } else {
+    lng += wg2;
+    if (tid == 0) {
+      ba.w[JDTP] = idir == 1 ? 0.5 * wold : 0.5 * wnew;
+      ba.w[JBRA] = -0.5 * a.delta * S.npnorm *
+                   ((fgg(a, bj.p[QMC2D_JETOT], bj.p[QMC2D_JGG]) +
+                     fgg(a, pn[QMC2D_JETOT], pn[QMC2D_JGG])) -
+                    2.0 * a.etrial);
+      bb.w[JITP] = idir == 1 ? 0.5 * wnew : 0.5 * wold;
+      ba.w[JLNG] = 0.5 * lng;
+      double nds = 0.0;
+      for (int tt = 0; tt < nt; tt++) {
+        int ju = QMC2D_JUN(nt, tt);
+        double var = 2.0 * S.hbs2m[tt] * a.delta;
+        nds -= log(1.0 - exp(-bj.p[ju] * pn[ju] / (0.5 * var)));
+      }
+      ba.w[JNDS] = nds;
+      *bn.age = 0.0;
+      *bn.s = sn;
+      for (int tt = 0; tt < nt; tt++) bn.h[tt] = hn[tt];
+    }
+    for (int k = tid; k < N2; k += blockDim.x) {
+      bn.x[k] = m.x[k];
+      bn.g[k] = m.g[k];
+    }
+    for (int k = tid; k < S.nprops; k += blockDim.x) bn.p[k] = pn[k];
+  }
+  __syncthreads();
+  if (tid == 0) bn.p[QMC2D_JACC] = p;
+  __syncthreads();
+}
+
+// What a reptation move does after its bead growths (reptation_move's path
+// part, reptation.f:2105-2160, and reptation_metropolis_test :1865-1895):
+// the proposed path's window sums, the action difference, the global test,
+// and the block accumulators. pp is scratch; ppo, blk, psum the reptile's
+// accepted-path averages, block sums and window sums; sc[1] scratch.
+struct PathState {
+  int jfirst, jlast;
+  double age, norm, nacc;
+};
+__device__ void path_tail(const DevSys &S, const RmcArgs &a, int r, uint32_t t, int idir,
+                          int ndelta, PathState &st, double *pp, double *ppo, double *blk,
+                          double *psum, double *sc) {
+  const int tid = threadIdx.x, nb = a.nbuf;
+  double half = 0.5, one = 0.0, one_nds = 0.0, mezzo = 0.0;
+  if (a.wpiu != 0) {
+    mezzo = 0.5;
+  } else if (a.gstorto != 0) {
+    half = 0.0;
+    one = 1.0;
+    if (a.nodalaction != 0) one_nds = 1.0;
+  }
+  int &jfirst = st.jfirst, &jlast = st.jlast;
+  double &age = st.age, &norm = st.norm, &nacc = st.nacc;
+  int kfirst = (jfirst + idir * ndelta + nb) % nb;
+  int klast = (jlast + idir * ndelta + nb) % nb;
+  path_sums(S, a, r, jfirst, idir * ndelta, psum, pp, (t & 255u) == 0u);
+  double wnew = 0.0;
+  if (tid == 0) {
+    auto P = [&](int j) { return bead(S, a, r, j); };
+    wnew = (-P(kfirst).p[QMC2D_JLTF] * (1 + 2 * mezzo) - P(klast).p[QMC2D_JLTF] * (1 - 2 * mezzo) +
+            P(jfirst).p[QMC2D_JLTF] * (1 + 2 * mezzo) + P(jlast).p[QMC2D_JLTF] * (1 - 2 * mezzo));
+    if (idir == 1) {
+      for (int idelta = 1; idelta <= ndelta; idelta++) {
+        int j = (jfirst + idir * (idelta - 1) + nb) % nb;
+        int jn = (jfirst + idir * idelta + nb) % nb;
+        double *wj = P(j).w, *wn = P(jn).w;
+        wnew = wnew - wj[JBRA] - wj[JDTP] * (half + mezzo) + wn[JITP] * (one + half + mezzo) -
+               wj[JLNG] * one + wj[JNDS] * one_nds;
+      }
+      for (int idelta = 1; idelta <= ndelta; idelta++) {
+        int j = (jlast + idir * (idelta - 1) + nb) % nb;
+        int jn = (jlast + idir * idelta + nb) % nb;
+        double *wj = P(j).w, *wn = P(jn).w;
+        wnew = wnew + wj[JBRA] - wj[JDTP] * (one + half - mezzo) + wn[JITP] * (half - mezzo) +
+               wj[JLNG] * one - wj[JNDS] * one_nds;
+      }
+    } else {
+      for (int idelta = 1; idelta <= ndelta; idelta++) {
+        int j = (jlast + idir * (idelta - 1) + nb) % nb;
+        int jn = (jlast + idir * idelta + nb) % nb;
+        double *wj = P(j).w, *wn = P(jn).w;
+        wnew = wnew - wn[JBRA] + wn[JDTP] * (one + half - mezzo) - wj[JITP] * (half - mezzo) -
+               wn[JLNG] * one + wn[JNDS] * one_nds;
+      }
+      for (int idelta = 1; idelta <= ndelta; idelta++) {
+        int j = (jfirst + idir * (idelta - 1) + nb) % nb;
+        int jn = (jfirst + idir * idelta + nb) % nb;
+        double *wj = P(j).w, *wn = P(jn).w;
+        wnew = wnew + wn[JBRA] + wn[JDTP] * (half + mezzo) - wj[JITP] * (one + half + mezzo) +
+               wn[JLNG] * one - wn[JNDS] * one_nds;
+      }
+    }
+    sc[1] = wnew;
+  }
+  __syncthreads();
+  wnew = sc[1];
+  // reptation_metropolis_test (reptation.f:1865-1895)
+  double p = (age == a.mage_r) ? 1.0 : exp(fmin(0.0, fmax(-50.0, wnew)));
+  double ua = u2(a.seed, 0xFFFFFFFDu, (uint32_t)r, t, 2u).x;
+  if (p >= ua) {
+    const double rc = 1.0 / (a.ntau - 2 * a.ntauskip);
+    const double emix =
+        0.5 * (bead(S, a, r, klast).p[QMC2D_JETOT] + bead(S, a, r, kfirst).p[QMC2D_JETOT]);
+    jfirst = kfirst;
+    jlast = klast;
+    for (int ip = tid; ip < S.nprops; ip += blockDim.x) {
+      psum[ip] = pp[ip];
+      ppo[ip] = ip == QMC2D_JETOT ? emix : pp[ip] * rc;
+    }
+    age = 0.0;
+    nacc += 1.0;
+  } else {
+    age += 1.0;
+  }
+  __syncthreads();
+  for (int ip = tid; ip < S.nprops; ip += blockDim.x) blk[ip] += ppo[ip];
+  norm += 1.0;
+  __syncthreads();
+}
+
 // One CTA per reptile; with kGmat reptile r's determinant matrices take
 // walker block r of the handle's device memory (nrep <= capacity).
 template <bool kGmat>
@@ -269,39 +455,27 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
   double *sc = hn + 2;
   const int r = blockIdx.x, tid = threadIdx.x;
   if (r >= a.nrep) return;
-  const int N2 = 2 * S.N, nt = S.nt, nb = a.nbuf;
+  const int N2 = 2 * S.N, nb = a.nbuf;
   for (int ip = tid; ip < S.nprops; ip += blockDim.x) {
     ppo[ip] = a.pp_old[(size_t)r * S.nprops + ip];
     blk[ip] = a.blk[(size_t)r * S.nprops + ip];
     psum[ip] = a.psum[(size_t)r * S.nprops + ip];
   }
-  int jfirst = a.ends[2 * r], jlast = a.ends[2 * r + 1];
-  double age = a.age[r];
-  double norm = a.blk_norm[r];
-  double nacc = 0.0;
+  PathState ps{a.ends[2 * r], a.ends[2 * r + 1], a.age[r], a.blk_norm[r], 0.0};
   int status = 0;
-  double half = 0.5, one = 0.0, one_nds = 0.0, mezzo = 0.0;
-  if (a.wpiu != 0) {
-    mezzo = 0.5;
-  } else if (a.gstorto != 0) {
-    half = 0.0;
-    one = 1.0;
-    if (a.nodalaction != 0) one_nds = 1.0;
-  }
   const double pi = 3.141592653589793;
   __syncthreads();
   for (int istp = 0; istp < a.nstp; istp++) {
     const uint32_t t = a.step0 + (uint32_t)istp;
-    double2 dl = u2(a.seed, 0xFFFFFFF0u, (uint32_t)r, t, 2u);
-    int idir = (dl.x - 0.5) >= 0.0 ? 1 : -1;
-    int ndelta = 1 + (int)(dl.y * a.mdelta);
-    int jstart = idir == 1 ? jlast : jfirst;
+    int idir, ndelta;
+    rmc_dir(a, r, t, idir, ndelta);
+    const int jstart = idir == 1 ? ps.jlast : ps.jfirst;
     for (int idelta = 1; idelta <= ndelta; idelta++) {
-      int j = (jstart + idir * (idelta - 1) + nb) % nb;
-      int jn = (jstart + idir * idelta + nb) % nb;
-      uint32_t c3 = 3u + (uint32_t)(idelta - 1);
+      const int j = (jstart + idir * (idelta - 1) + nb) % nb;
+      const int jn = (jstart + idir * idelta + nb) % nb;
+      const uint32_t c3 = 3u + (uint32_t)(idelta - 1);
       long long tph = clock64();
-      Bead bj = bead(S, a, r, j), bn = bead(S, a, r, jn);
+      Bead bj = bead(S, a, r, j);
       double ww = 0, wg = 0, dd = 0;
       for (int k = tid; k < N2; k += blockDim.x) {
         int ti = type_of(S, k >> 1);
@@ -318,145 +492,11 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
       double lng = block_sum(wg, m.red);
       phase_mark(S, PH_PROPOSE, tph);
       status |= eval_walker<double, kGmat>(S, m, hn, pn, sc, tph);
-      double sn = sc[0];
-      double wn = 0.0;
-      for (int k = tid; k < N2; k += blockDim.x) {
-        int ti = type_of(S, k >> 1);
-        double var = 2.0 * S.hbs2m[ti] * a.delta, vari = 1.0 / var;
-        double chi = bj.x[k] - m.x[k] - (-var * m.g[k]);
-        wn -= chi * chi * vari;
-      }
-      double wnew = block_sum(wn, m.red);
-      double p = 2 * (bj.p[QMC2D_JLTF] - pn[QMC2D_JLTF]) + 0.5 * (wnew - wold);
-      p = exp(fmin(0.0, fmax(-50.0, p)));
-      if (a.rejection == 0) p = 1.0;
-      else if (*bj.age == a.mage) p = 1.0;
-      if (*bj.s * sn < 0.0) p = 0.0;
-      double wg2 = a.delta * S.npnorm * (bj.p[QMC2D_JKIN0] + pn[QMC2D_JKIN0]);
-      double ua = u2(a.seed, 0xFFFFFFFEu, (uint32_t)r, t, c3).x;
-      bool rej = p < ua;
-      __syncthreads();
-      Bead ba = idir == 1 ? bj : bn, bb = idir == 1 ? bn : bj;
-      if (rej) {
-        if (tid == 0) {
-          ba.w[JDTP] = 0.5 * dold;
-          ba.w[JBRA] = -a.delta * S.npnorm * (fgg(a, bj.p[QMC2D_JETOT], bj.p[QMC2D_JGG]) - a.etrial);
-          bb.w[JITP] = 0.5 * dold;
-          ba.w[JLNG] = 0.5 * wg2;
-          double nds = 0.0;
-          for (int tt = 0; tt < nt; tt++) {
-            int ju = QMC2D_JUN(nt, tt);
-            double var = 2.0 * S.hbs2m[tt] * a.delta;
-            nds -= log(1.0 - exp(-bj.p[ju] * bj.p[ju] / (0.5 * var)));
-          }
-          ba.w[JNDS] = nds;
-          *bn.age = *bj.age + 1.0;
-          *bn.s = *bj.s;
-          for (int tt = 0; tt < nt; tt++) bn.h[tt] = bj.h[tt];
-        }
-        for (int k = tid; k < N2; k += blockDim.x) {
-          bn.x[k] = bj.x[k];
-          bn.g[k] = bj.g[k];
-        }
-        for (int k = tid; k < S.nprops; k += blockDim.x) bn.p[k] = bj.p[k];
-      } else {
-        lng += wg2;
-        if (tid == 0) {
-          ba.w[JDTP] = idir == 1 ? 0.5 * wold : 0.5 * wnew;
-          ba.w[JBRA] = -0.5 * a.delta * S.npnorm *
-                       ((fgg(a, bj.p[QMC2D_JETOT], bj.p[QMC2D_JGG]) +
-                         fgg(a, pn[QMC2D_JETOT], pn[QMC2D_JGG])) -
-                        2.0 * a.etrial);
-          bb.w[JITP] = idir == 1 ? 0.5 * wnew : 0.5 * wold;
-          ba.w[JLNG] = 0.5 * lng;
-          double nds = 0.0;
-          for (int tt = 0; tt < nt; tt++) {
-            int ju = QMC2D_JUN(nt, tt);
-            double var = 2.0 * S.hbs2m[tt] * a.delta;
-            nds -= log(1.0 - exp(-bj.p[ju] * pn[ju] / (0.5 * var)));
-          }
-          ba.w[JNDS] = nds;
-          *bn.age = 0.0;
-          *bn.s = sn;
-          for (int tt = 0; tt < nt; tt++) bn.h[tt] = hn[tt];
-        }
-        for (int k = tid; k < N2; k += blockDim.x) {
-          bn.x[k] = m.x[k];
-          bn.g[k] = m.g[k];
-        }
-        for (int k = tid; k < S.nprops; k += blockDim.x) bn.p[k] = pn[k];
-      }
-      __syncthreads();
-      if (tid == 0) bn.p[QMC2D_JACC] = p;
-      __syncthreads();
+      bead_tail(S, a, m, r, t, idir, idelta, j, jn, wold, dold, lng, pn, hn, sc);
       phase_mark(S, PH_ACCEPT, tph);
     }
     long long tpp = clock64();
-    int kfirst = (jfirst + idir * ndelta + nb) % nb;
-    int klast = (jlast + idir * ndelta + nb) % nb;
-    path_sums(S, a, r, jfirst, idir * ndelta, psum, pp, (t & 255u) == 0u);
-    double wnew = 0.0;
-    if (tid == 0) {
-      auto P = [&](int j) { return bead(S, a, r, j); };
-      wnew = (-P(kfirst).p[QMC2D_JLTF] * (1 + 2 * mezzo) - P(klast).p[QMC2D_JLTF] * (1 - 2 * mezzo) +
-              P(jfirst).p[QMC2D_JLTF] * (1 + 2 * mezzo) + P(jlast).p[QMC2D_JLTF] * (1 - 2 * mezzo));
-      if (idir == 1) {
-        for (int idelta = 1; idelta <= ndelta; idelta++) {
-          int j = (jfirst + idir * (idelta - 1) + nb) % nb;
-          int jn = (jfirst + idir * idelta + nb) % nb;
-          double *wj = P(j).w, *wn = P(jn).w;
-          wnew = wnew - wj[JBRA] - wj[JDTP] * (half + mezzo) + wn[JITP] * (one + half + mezzo) -
-                 wj[JLNG] * one + wj[JNDS] * one_nds;
-        }
-        for (int idelta = 1; idelta <= ndelta; idelta++) {
-          int j = (jlast + idir * (idelta - 1) + nb) % nb;
-          int jn = (jlast + idir * idelta + nb) % nb;
-          double *wj = P(j).w, *wn = P(jn).w;
-          wnew = wnew + wj[JBRA] - wj[JDTP] * (one + half - mezzo) + wn[JITP] * (half - mezzo) +
-                 wj[JLNG] * one - wj[JNDS] * one_nds;
-        }
-      } else {
-        for (int idelta = 1; idelta <= ndelta; idelta++) {
-          int j = (jlast + idir * (idelta - 1) + nb) % nb;
-          int jn = (jlast + idir * idelta + nb) % nb;
-          double *wj = P(j).w, *wn = P(jn).w;
-          wnew = wnew - wn[JBRA] + wn[JDTP] * (one + half - mezzo) - wj[JITP] * (half - mezzo) -
-                 wn[JLNG] * one + wn[JNDS] * one_nds;
-        }
-        for (int idelta = 1; idelta <= ndelta; idelta++) {
-          int j = (jfirst + idir * (idelta - 1) + nb) % nb;
-          int jn = (jfirst + idir * idelta + nb) % nb;
-          double *wj = P(j).w, *wn = P(jn).w;
-          wnew = wnew + wn[JBRA] + wn[JDTP] * (half + mezzo) - wj[JITP] * (one + half + mezzo) +
-                 wn[JLNG] * one - wn[JNDS] * one_nds;
-        }
-      }
-      sc[1] = wnew;
-    }
-    __syncthreads();
-    wnew = sc[1];
-    // reptation_metropolis_test (reptation.f:1865-1895)
-    double p = (age == a.mage_r) ? 1.0 : exp(fmin(0.0, fmax(-50.0, wnew)));
-    double ua = u2(a.seed, 0xFFFFFFFDu, (uint32_t)r, t, 2u).x;
-    if (p >= ua) {
-      const double rc = 1.0 / (a.ntau - 2 * a.ntauskip);
-      const double emix =
-          0.5 * (bead(S, a, r, klast).p[QMC2D_JETOT] + bead(S, a, r, kfirst).p[QMC2D_JETOT]);
-      jfirst = kfirst;
-      jlast = klast;
-      for (int ip = tid; ip < S.nprops; ip += blockDim.x) {
-        psum[ip] = pp[ip];
-        ppo[ip] = ip == QMC2D_JETOT ? emix : pp[ip] * rc;
-      }
-      age = 0.0;
-      nacc += 1.0;
-    } else {
-      age += 1.0;
-    }
-    __syncthreads();
-    for (int ip = tid; ip < S.nprops; ip += blockDim.x) blk[ip] += ppo[ip];
-    norm += 1.0;
-    __syncthreads();
+    path_tail(S, a, r, t, idir, ndelta, ps, pp, ppo, blk, psum, sc);
     phase_mark(S, PH_PATH, tpp);
   }
   for (int ip = tid; ip < S.nprops; ip += blockDim.x) {
@@ -465,14 +505,200 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
     a.psum[(size_t)r * S.nprops + ip] = psum[ip];
   }
   if (tid == 0) {
-    a.ends[2 * r] = jfirst;
-    a.ends[2 * r + 1] = jlast;
-    a.age[r] = age;
-    a.blk_norm[r] = norm;
-    a.cnt[4 * r] += nacc;
+    a.ends[2 * r] = ps.jfirst;
+    a.ends[2 * r + 1] = ps.jlast;
+    a.age[r] = ps.age;
+    a.blk_norm[r] = ps.norm;
+    a.cnt[4 * r] += ps.nacc;
     a.cnt[4 * r + 1] += a.nstp;
     a.status[r] |= status;
   }
+}
+
+// ------------------------------------------------ split bead growth
+// The same move as rmc_move_kernel in two launches per bead growth, as a
+// VMC/DMC move is: rmc_pairs_kernel draws the growing end's new bead and
+// runs the pair passes (u2, u3, backflow, v2) and rho_k into the reptile's
+// move scratch, with the pair rows staged in shared memory and G reptiles
+// per CTA; rmc_det_kernel evaluates the determinants from the scratch (the
+// backflow pair values stored by the pair passes), runs the bead's tail
+// and, after the reptile's last growth of the move, the path tail. A move
+// of mdelta > 1 takes mdelta launch pairs; a reptile whose move has fewer
+// growths skips the later ones.
+template <class R, int G>
+__global__ void __launch_bounds__(G * kThreads, 2 / G) rmc_pairs_kernel(const DevSys *sp,
+                                                                        RmcArgs a, double *scr,
+                                                                        int idelta,
+                                                                        int stage_rows) {
+  constexpr int kPairThreads = G * kThreads;
+  __shared__ DevSys S;
+  extern __shared__ __align__(16) char smem[];
+  load_sys(S, sp);
+  const size_t carve = (pair_carve(S, nullptr, nullptr, kThreads) + 127) & ~size_t(127);
+  const int grp = threadIdx.x / kThreads, tid = threadIdx.x - grp * kThreads;
+  EvalSmem m;
+  pair_carve(S, smem + grp * carve, &m, kThreads);
+  const R *rows_g = pair_rows<R>(S);
+  R *rows_s = reinterpret_cast<R *>(smem + G * carve);
+  if (stage_rows) {  // the first copy16 16-byte parts of each global row
+    using Lay = RowLayout<R>;
+    constexpr int V = Lay::copy16, VG = Lay::gstride * (int)sizeof(R) / 16;
+    const int nrow = S.cmb_nblk * (S.cmb_ng + 1);
+    const float4 *src = reinterpret_cast<const float4 *>(rows_g);
+    for (int e = threadIdx.x; e < nrow * V; e += kPairThreads) {
+      const int rr = e / V, q = e - rr * V;
+      reinterpret_cast<float4 *>(rows_s + (size_t)rr * Lay::sstride)[q] =
+          __ldg(src + (size_t)rr * VG + q);
+    }
+  }
+  __syncthreads();
+  const GroupSync sync{1 + grp, kThreads};
+  const int N = S.N, N2 = 2 * N, nb = a.nbuf;
+  const uint32_t t = a.step0;
+  const double pi = 3.141592653589793;
+  const MoveScratch L = move_scratch(S);
+  for (int r = blockIdx.x * G + grp; r < a.nrep; r += gridDim.x * G) {
+    int idir, ndelta;
+    rmc_dir(a, r, t, idir, ndelta);
+    if (idelta > ndelta) continue;  // the whole group: r is the group's
+    long long tph = clock64();
+    const int jstart = idir == 1 ? a.ends[2 * r + 1] : a.ends[2 * r];
+    const int j = (jstart + idir * (idelta - 1) + nb) % nb;
+    const uint32_t c3 = 3u + (uint32_t)(idelta - 1);
+    Bead bj = bead(S, a, r, j);
+    double ww = 0, wg = 0, dd = 0;
+    for (int k = tid; k < N2; k += kThreads) {
+      int ti = type_of(S, k >> 1);
+      double var = 2.0 * S.hbs2m[ti] * a.delta, vari = 1.0 / var;
+      double drift = -var * bj.g[k];
+      dd += drift * drift * vari;
+      double2 u = u2(a.seed, (uint32_t)k, (uint32_t)r, t, c3);
+      double chi = cos(pi * u.x) * sqrt(-2.0 * var * log(u.y));
+      ww -= chi * chi * vari;
+      m.x[k] = chi + drift + bj.x[k];
+      wg -= (chi + drift) * (chi + drift) * vari;
+    }
+    const double wold = block_sum_t<kThreads>(ww, m.red, sync, tid);
+    const double dold = block_sum_t<kThreads>(dd, m.red, sync, tid);
+    const double lng = block_sum_t<kThreads>(wg, m.red, sync, tid);
+    phase_mark(S, PH_PROPOSE, tph, tid == 0);
+    double *o = scr + (size_t)r * L.stride;
+    double *pout = (S.has_bf && !S.bf_zero) ? o + L.pair : nullptr;
+    if (stage_rows)
+      eval_pairs<kThreads, true>(S, m, tph, pout, (const R *)rows_s, sync, tid);
+    else
+      eval_pairs<kThreads, false>(S, m, tph, pout, rows_g, sync, tid);
+    compute_rhok(S, m, tid, kThreads);
+    sync();
+    for (int e = tid; e < 4 * S.nk; e += kThreads) o[L.rhok + e] = m.rhok[e];
+    for (int e = tid; e < N2; e += kThreads) {
+      o[L.x + e] = m.x[e];
+      o[L.g + e] = m.g[e];
+      o[L.q + e] = m.q[e];
+      o[L.qbd + e] = m.qbd[e];
+    }
+    for (int e = tid; e < 3 * N; e += kThreads) o[L.sb + e] = m.Sb[e];
+    for (int e = tid; e < N; e += kThreads) {
+      o[L.lap + e] = m.lap[e];
+      o[L.ltf + e] = m.ltf[e];
+      o[L.vp + e] = m.vp[e];
+    }
+    if (tid == 0) {
+      o[L.wold] = wold;
+      o[L.dold] = dold;
+      o[L.lng] = lng;
+    }
+    sync();  // m is reused by the group's next reptile
+  }
+}
+
+template <bool kGmat>
+__global__ void __launch_bounds__(kThreads, 2) rmc_det_kernel(const DevSys *sp, RmcArgs a,
+                                                              const double *scr, int idelta) {
+  __shared__ DevSys S;
+  extern __shared__ __align__(16) char smem[];
+  load_sys(S, sp);
+  EvalSmem m;
+  size_t off = eval_carve<kGmat>(S, smem, &m, kGmat ? gmat_block(S, blockIdx.x) : nullptr);
+  double *pn = reinterpret_cast<double *>(smem + off);
+  double *pp = pn + S.nprops;
+  double *ppo = pp + S.nprops;
+  double *blk = ppo + S.nprops;
+  double *psum = blk + S.nprops;
+  double *hn = psum + S.nprops;
+  double *sc = hn + 2;
+  const int r = blockIdx.x, tid = threadIdx.x;
+  if (r >= a.nrep) return;
+  const uint32_t t = a.step0;
+  int idir, ndelta;
+  rmc_dir(a, r, t, idir, ndelta);
+  if (idelta > ndelta) return;  // the whole CTA
+  const int N = S.N, N2 = 2 * N, nb = a.nbuf;
+  const MoveScratch L = move_scratch(S);
+  const double *o = scr + (size_t)r * L.stride;
+  const bool pairs_stored = S.has_bf && !S.bf_zero;
+  if (pairs_stored) {
+    // bring the stored pair values back into L2 before the Jacobian build
+    const size_t bytes = (sizeof(double) * 3 * (size_t)N * N) & ~size_t(15);
+    const char *base = reinterpret_cast<const char *>(o + L.pair);
+    for (size_t b0 = (size_t)tid * 32768; b0 < bytes; b0 += (size_t)kThreads * 32768) {
+      const unsigned sz = (unsigned)(bytes - b0 < 32768 ? bytes - b0 : 32768);
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + b0), "r"(sz)
+                   : "memory");
+    }
+  }
+  for (int e = tid; e < N2; e += kThreads) {
+    m.x[e] = o[L.x + e];
+    m.g[e] = o[L.g + e];
+    m.q[e] = o[L.q + e];
+    m.qbd[e] = o[L.qbd + e];
+    m.gd[e] = 0.0;
+  }
+  for (int e = tid; e < 3 * N; e += kThreads) m.Sb[e] = o[L.sb + e];
+  for (int e = tid; e < N; e += kThreads) {
+    m.lap[e] = o[L.lap + e];
+    m.ltf[e] = o[L.ltf + e];
+    m.vp[e] = o[L.vp + e];
+    m.lapd[e] = 0.0;
+    m.ph2[e] = 0.0;
+    m.ph2d[e] = 0.0;
+  }
+  const double wold = o[L.wold], dold = o[L.dold], lng = o[L.lng];
+  __syncthreads();
+  long long tph = clock64();
+  const int status = eval_det<kGmat>(S, m, hn, pn, sc, tph, pairs_stored ? o + L.pair : nullptr,
+                                     o + L.rhok);
+  const int jstart = idir == 1 ? a.ends[2 * r + 1] : a.ends[2 * r];
+  const int j = (jstart + idir * (idelta - 1) + nb) % nb;
+  const int jn = (jstart + idir * idelta + nb) % nb;
+  bead_tail(S, a, m, r, t, idir, idelta, j, jn, wold, dold, lng, pn, hn, sc);
+  phase_mark(S, PH_ACCEPT, tph);
+  if (tid == 0 && status) atomicOr(&a.status[r], status);
+  if (idelta < ndelta) return;  // the whole CTA
+  // the move's end, with the reptile's state from and back to device memory
+  long long tpp = clock64();
+  for (int ip = tid; ip < S.nprops; ip += blockDim.x) {
+    ppo[ip] = a.pp_old[(size_t)r * S.nprops + ip];
+    blk[ip] = a.blk[(size_t)r * S.nprops + ip];
+    psum[ip] = a.psum[(size_t)r * S.nprops + ip];
+  }
+  PathState ps{a.ends[2 * r], a.ends[2 * r + 1], a.age[r], a.blk_norm[r], 0.0};
+  __syncthreads();
+  path_tail(S, a, r, t, idir, ndelta, ps, pp, ppo, blk, psum, sc);
+  for (int ip = tid; ip < S.nprops; ip += blockDim.x) {
+    a.pp_old[(size_t)r * S.nprops + ip] = ppo[ip];
+    a.blk[(size_t)r * S.nprops + ip] = blk[ip];
+    a.psum[(size_t)r * S.nprops + ip] = psum[ip];
+  }
+  if (tid == 0) {
+    a.ends[2 * r] = ps.jfirst;
+    a.ends[2 * r + 1] = ps.jlast;
+    a.age[r] = ps.age;
+    a.blk_norm[r] = ps.norm;
+    a.cnt[4 * r] += ps.nacc;
+    a.cnt[4 * r + 1] += 1.0;
+  }
+  phase_mark(S, PH_PATH, tpp);
 }
 
 // The path estimators of path_props (reptation.f:1578-1737) of reptile r's
@@ -685,8 +911,10 @@ extern "C" int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params 
   }
   RCK(cudaSetDevice(h->device));
   RCK(cudaStreamSynchronize(h->stream));
+  const int split = h->rmc.split;  // a launch choice: kept across set-ups
   q2d::rmc_free(&h->rmc);
   q2d::RmcState &r = h->rmc;
+  r.split = split;
   r.nrep = nrep;
   r.ntau = prm->ntau;
   r.ntauskip = prm->ntauskip;
@@ -740,6 +968,37 @@ extern "C" int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params 
   return q2d_sync_status(h, nrep);
 }
 
+template <int G>
+static cudaError_t launch_rmc_pairs(const q2d::DevSys &hs, const q2d::DevSys *ds,
+                                    const q2d::RmcArgs &a, double *scr, int idelta,
+                                    cudaStream_t st) {
+  int dev = 0, nsm = 0, optin = 0;
+  cudaError_t e;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+    return e;
+  if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) !=
+      cudaSuccess)
+    return e;
+  const void *k = (const void *)q2d::rmc_pairs_kernel<double, G>;
+  const size_t carve =
+      G * ((q2d::pair_carve(hs, nullptr, nullptr, q2d::kThreads) + 127) & ~size_t(127));
+  const size_t rows = sizeof(double) * q2d::RowLayout<double>::sstride * (size_t)hs.cmb_nblk *
+                      (hs.cmb_ng + 1);
+  const int stage =
+      hs.tune_stage != 1 && carve + rows + sizeof(q2d::DevSys) <= (size_t)optin ? 1 : 0;
+  const size_t sm = carve + (stage ? rows : 0);
+  if ((e = q2d::raise_smem_limit(k, sm)) != cudaSuccess) return e;
+  int per_sm = 1;
+  if (G == 1 && (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G * q2d::kThreads,
+                                                                   sm)) != cudaSuccess)
+    return e;
+  const int need = (a.nrep + G - 1) / G, cap = nsm * (per_sm > 0 ? per_sm : 1);
+  q2d::rmc_pairs_kernel<double, G>
+      <<<need < cap ? need : cap, G * q2d::kThreads, sm, st>>>(ds, a, scr, idelta, stage);
+  return cudaGetLastError();
+}
+
 extern "C" int qmc2d_rmc(qmc2d_handle *h, int nstp) {
   if (!h || nstp < 0) return QMC2D_ERR_ARG;
   if (h->rmc.nrep <= 0) {
@@ -751,19 +1010,52 @@ extern "C" int qmc2d_rmc(qmc2d_handle *h, int nstp) {
   RCK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * h->rmc.nrep, h->stream));
   q2d::RmcArgs a = rmc_args(h, nstp);
   size_t sm = rmc_move_smem(h->hs);
-  const void *km = h->hs.gmat ? (const void *)q2d::rmc_move_kernel<true>
-                              : (const void *)q2d::rmc_move_kernel<false>;
-  RCK(q2d::raise_smem_limit(km, sm));
-  {
+  if (!h->rmc.split) {
+    const void *km = h->hs.gmat ? (const void *)q2d::rmc_move_kernel<true>
+                                : (const void *)q2d::rmc_move_kernel<false>;
+    RCK(q2d::raise_smem_limit(km, sm));
     ProfScope ps(h, QMC2D_KERNEL_RMC, h->stream);
     if (h->hs.gmat)
       q2d::rmc_move_kernel<true><<<h->rmc.nrep, q2d::kThreads, sm, h->stream>>>(h->ds, a);
     else
       q2d::rmc_move_kernel<false><<<h->rmc.nrep, q2d::kThreads, sm, h->stream>>>(h->ds, a);
+    RCK(cudaGetLastError());
+  } else {
+    // per move and bead growth: the pair passes, then the rest
+    const void *kd = h->hs.gmat ? (const void *)q2d::rmc_det_kernel<true>
+                                : (const void *)q2d::rmc_det_kernel<false>;
+    RCK(q2d::raise_smem_limit(kd, sm));
+    for (int istp = 0; istp < nstp; istp++) {
+      a.step0 = h->rmc.step + (uint32_t)istp;
+      for (int idelta = 1; idelta <= h->rmc.mdelta; idelta++) {
+        {
+          ProfScope ps(h, QMC2D_KERNEL_PAIRS, h->stream);
+          RCK(h->hs.tune_groups == 1
+                  ? launch_rmc_pairs<1>(h->hs, h->ds, a, h->d_mscr, idelta, h->stream)
+                  : launch_rmc_pairs<2>(h->hs, h->ds, a, h->d_mscr, idelta, h->stream));
+        }
+        ProfScope ps(h, QMC2D_KERNEL_RMC, h->stream);
+        if (h->hs.gmat)
+          q2d::rmc_det_kernel<true>
+              <<<h->rmc.nrep, q2d::kThreads, sm, h->stream>>>(h->ds, a, h->d_mscr, idelta);
+        else
+          q2d::rmc_det_kernel<false>
+              <<<h->rmc.nrep, q2d::kThreads, sm, h->stream>>>(h->ds, a, h->d_mscr, idelta);
+        RCK(cudaGetLastError());
+      }
+    }
   }
-  RCK(cudaGetLastError());
   h->rmc.step += (uint32_t)nstp;
   return q2d_sync_status(h, h->rmc.nrep);
+}
+
+extern "C" int qmc2d_rmc_set_launch(qmc2d_handle *h, int split) {
+  if (!h || split < 0 || split > 1) {
+    q2d::set_error("qmc2d_rmc_set_launch: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  h->rmc.split = split;
+  return QMC2D_OK;
 }
 
 extern "C" int qmc2d_rmc_get_path(qmc2d_handle *h, int rep, double *x, double *props) {

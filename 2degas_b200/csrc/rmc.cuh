@@ -23,6 +23,7 @@ struct RmcState {
   double *psum = nullptr;     // nrep * nprops: the accepted path's window sums (path_props)
   double *age = nullptr;      // nrep
   uint32_t step = 0;
+  int split = 1;  // qmc2d_rmc_set_launch: pair kernel + determinant kernel per growth
   double *est = nullptr;  // path estimators: nrep rows and their mean (qmc2d_rmc_estimators)
   size_t est_cap = 0;
 };

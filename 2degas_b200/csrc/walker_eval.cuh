@@ -243,8 +243,10 @@ __host__ __device__ inline size_t pair_carve(const DevSys &s, char *base, EvalSm
 // density, rho_k (both slots), and (backflow) the spline values of every
 // ordered pair (i, j):
 // eta(r_ij), eta'(r_ij)/r_ij and 3 eta'/r + eta'' at [k N^2 + i N + j].
+// A reptile's bead growth also keeps its proposal's drift term (dold) and
+// the free-propagator sum (lng) of get_w_stack (reptation.f:1804-1851).
 struct MoveScratch {
-  int x, g, q, sb, qbd, lap, ltf, vp, wold, rhok, pair;
+  int x, g, q, sb, qbd, lap, ltf, vp, wold, dold, lng, rhok, pair;
   size_t stride;
 };
 __host__ __device__ inline MoveScratch move_scratch(const DevSys &s) {
@@ -259,8 +261,10 @@ __host__ __device__ inline MoveScratch move_scratch(const DevSys &s) {
   l.ltf = 12 * N;
   l.vp = 13 * N;
   l.wold = 14 * N;
-  l.rhok = 14 * N + 1;
-  l.pair = (14 * N + 1 + 4 * (s.nk > 0 ? s.nk : 1) + 3) & ~3;
+  l.dold = 14 * N + 1;
+  l.lng = 14 * N + 2;
+  l.rhok = 14 * N + 3;
+  l.pair = (14 * N + 3 + 4 * (s.nk > 0 ? s.nk : 1) + 3) & ~3;
   size_t end = (size_t)l.pair + (s.has_bf ? 3 * (size_t)N * N : 0);
   l.stride = (end + 31) & ~size_t(31);  // 256-byte aligned walker blocks
   return l;

@@ -59,7 +59,7 @@ TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum of pairs_kernel + move_kernel (296 w
 
 def move_scratch_bytes(N, nk):
     """Bytes of one walker's move scratch block (MoveScratch, backflow)."""
-    pair = (14 * N + 1 + 4 * max(nk, 1) + 3) & ~3
+    pair = (14 * N + 3 + 4 * max(nk, 1) + 3) & ~3
     return 8 * ((pair + 3 * N * N + 31) & ~31)
 
 
@@ -668,13 +668,15 @@ def config_arm(args, rank, world, local_rank):
         h.population_set(x0)
         h.vmc(args.equil, 0.045 * rs * rs, 10 ** 9)  # seeded VMC start configurations
         x1 = h.population_get()["x"]
+        if args.rmc_split is not None:
+            h.rmc_set_launch(args.rmc_split)
         h.rmc_init(nw, rmc_start_paths(x1, ntau, delta, rs, walker_seed & 0xFFFF), ntau, 1, 1,
                    delta, etrial, 10 ** 9, mage_r)
         tuned = None
 
         def step():
             h.rmc(1)
-        kernels = (capi.KERNEL_RMC,)
+        kernels = (capi.KERNEL_PAIRS, capi.KERNEL_RMC)
     stream = torch.cuda.ExternalStream(h.stream())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     for _ in range(args.warmup):
@@ -781,7 +783,8 @@ def config_arm(args, rank, world, local_rank):
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                          "kernel": ("single_kernel" if vmc and args.single else
-                                    "pairs_kernel + move_kernel" if vmc else "rmc_move_kernel"),
+                                    "pairs_kernel + move_kernel" if vmc else
+                                    "rmc_pairs_kernel + rmc_det_kernel"),
                          "flops_per_move": fpm,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64)"},
             "cpu_baseline": cpu,
@@ -1130,6 +1133,8 @@ def main():
                     help="determinant inversion layout (qmc2d_set_inversion)")
     ap.add_argument("--single", action="store_true",
                     help="vmc workload with single-electron moves and Sherman-Morrison updates")
+    ap.add_argument("--rmc-split", type=int, default=None, choices=[0, 1],
+                    help="reptation launch shape (qmc2d_rmc_set_launch)")
     ap.add_argument("--rmc-n", type=int, default=58, choices=[26, 58],
                     help="electrons of the reptation workload's deck")
     ap.add_argument("--shell", type=lambda v: tuple(int(t) for t in v.split(",")),

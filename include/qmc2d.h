@@ -513,6 +513,12 @@ int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params *prm,
  * reptation.f:1897-1895) on every reptile, accumulating p_old into the
  * block sums. */
 int qmc2d_rmc(qmc2d_handle *h, int nstp);
+/* Launch choice of qmc2d_rmc (the reference has no counterpart): split = 1
+ * (the default) runs each bead growth as two kernels, the pair passes with
+ * the pair rows staged in shared memory and then the rest of the evaluation
+ * and the tests, as a VMC/DMC move; split = 0 runs whole moves in one
+ * kernel per launch. Both compute the same values up to round-off. */
+int qmc2d_rmc_set_launch(qmc2d_handle *h, int split);
 /* Copy reptile r's path (ntau beads, x then props) out. */
 int qmc2d_rmc_get_path(qmc2d_handle *h, int r, double *x, double *props);
 /* Reptation restart: see the restart(0) comment above qmc2d_vmc. */

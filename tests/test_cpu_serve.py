@@ -29,7 +29,7 @@ def test_footprint_is_linear_in_walkers_and_counts_every_record(q, n26):
     # the move scratch: per-particle sums, rho_k and (backflow) 3 N^2 pair
     # values, rounded up to 256 bytes
     nk = s.s.nk
-    pair = (14 * N + 1 + 4 * max(nk, 1) + 3) & ~3
+    pair = (14 * N + 3 + 4 * max(nk, 1) + 3) & ~3
     scr = ((pair + 3 * N * N + 31) // 32) * 32 * 8
     assert per == recs + scr
     with pytest.raises(Exception):

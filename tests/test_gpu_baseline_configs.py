@@ -14,6 +14,8 @@ headline DMC line does not run:
   starts as a random walk of 200 beads with the propagator's link variance;
   a move is forced after two rejections (mage_r = 2, reptation_metropolis_test
   :1865-1895), which keeps about half the moves accepted from that start.
+  Both launch shapes of the moves (qmc2d_rmc_set_launch: the pair passes in a
+  kernel of their own, or whole moves in one kernel) replay it.
 
 Every deck is read by the product and, independently, by the oracle's own
 reader."""
@@ -80,8 +82,9 @@ def test_config0_vmc_replay(q, oracle_cls, tmp_path):
     assert close(blk, blk_o) < 1e-9
 
 
+@pytest.mark.parametrize("split", [1, 0])
 @pytest.mark.parametrize("name", ["rmc_n26_rs10", "rmc_n58_rs10"])
-def test_config2_reptation_ring_wraps(q, oracle_cls, tmp_path, name):
+def test_config2_reptation_ring_wraps(q, oracle_cls, tmp_path, name, split):
     capi = importlib.import_module("2degas_b200._capi")
     nrep, ntau, mdelta, nstp, mage_r = 4, 200, 1, 300, 2
     s, x0, rs = _deck(q, tmp_path, name, nrep)
@@ -106,6 +109,7 @@ def test_config2_reptation_ring_wraps(q, oracle_cls, tmp_path, name):
         nacc_o += na
         paths.append(rep.path())
     with q.Handle(s, capacity=nrep, seed=SEED) as h:
+        h.rmc_set_launch(split)
         h.rmc_init(nrep, x, ntau, 1, mdelta, delta, etrial, 10 ** 6, mage_r)
         h.block_reset()
         h.rmc(nstp)

@@ -84,7 +84,8 @@ def test_dmc_generations(q, oracle_cls, n26, n26_configs):
     assert rel(blk[:14], blk_o[:14]) < 1e-9
 
 
-def test_reptation_moves(q, oracle_cls, n26, n26_configs):
+@pytest.mark.parametrize("split", [1, 0])
+def test_reptation_moves(q, oracle_cls, n26, n26_configs, split):
     from ctypes import c_double, c_int  # noqa: F401
 
     import importlib
@@ -103,6 +104,7 @@ def test_reptation_moves(q, oracle_cls, n26, n26_configs):
         blk_o += b
         paths.append(rep.path())
     with q.Handle(n26, capacity=nrep, seed=SEED) as h:
+        h.rmc_set_launch(split)
         h.rmc_init(nrep, x, ntau, 1, mdelta, 0.05, -0.43, 1000, 1000)
         h.block_reset()
         h.rmc(nstp)
