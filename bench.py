@@ -431,6 +431,7 @@ def b200_arm(args, rank, world, local_rank):
             dev_ms += e0.elapsed_time(e1)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
+    acc = h.counters()
     move_ms, move_n = h.profile_get(capi.KERNEL_MOVE)
     pair_ms, pair_n = h.profile_get(capi.KERNEL_PAIRS)
     br_ms, br_n = h.profile_get(capi.KERNEL_BRANCH)
@@ -503,6 +504,7 @@ def b200_arm(args, rank, world, local_rank):
             "kernel_ms": {"pairs": pair_ms, "move": move_ms, "branch": br_ms, "gather": ga_ms},
             "wall_s": wall,
             "e_mixed": e_mean,
+            "acceptance": acc["accepted"] / max(acc["proposed"], 1),
             "clocks": clk.summary(),
         }
     if dist:
