@@ -1099,6 +1099,10 @@ def batch_arm(args, rank, world):
                    "timing": "host wall clock around one qmc2d_batch_dmc call (synchronised)"},
         "handle_by_handle": {"value": moves / t_seq, "seconds": t_seq},
         "speedup_vs_handle_by_handle": t_seq / t_batch,
+        # each population's autotuned launch: (pair-kernel walker groups,
+        # rows not staged, inversion layout) -> populations
+        "launch_choices": {str(k): v for k, v in sorted(
+            __import__("collections").Counter(tuple(h.get_launch()) for h in handles).items())},
         "clocks": clk.summary(),
     }
     b.close()
