@@ -44,7 +44,7 @@ struct EvalSmem {
   // register-resident inversion: per spin, double-buffered pivot-row slots
   // of every warp and the warps' pivot keys (inside the F0 region)
   double2 *gslot[2];
-  unsigned long long *gkey[2];
+  unsigned *gkey[2];
   // inversion in global memory (gmat): each spin's panel, multipliers and
   // scaled pivot rows (gj_invert_gmem)
   double2 *fcol[2];
@@ -83,6 +83,12 @@ __host__ __device__ inline int gj_reg_lanes(int n, int nthr) {
     if (kGjCols * L >= n && nthr / L >= n) return L;
   return 0;
 }
+// Row slot of the register-resident inversion per warp (complex elements):
+// the warp's candidate pivot row, lane s's kGjCols columns at s (kGjCols+1)
+// (the odd stride keeps the lanes' 16-byte words on distinct banks), then
+// the candidate's reciprocal and |pivot|^2.
+__host__ __device__ inline int gj_reg_slot(int L) { return L * (kGjCols + 1) + 2; }
+
 // Warps per spin for the register-resident inversion (all warps of the CTA).
 __host__ __device__ inline int gj_reg_warps(int nt) { return (kThreads / 32) / (nt > 1 ? 2 : 1); }
 
@@ -170,8 +176,8 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
     const int ldu = xt_ldu(2 * n);
     size_t ubytes = sizeof(double) * ((size_t)kChunk * ldu + (size_t)xt_row_tiles(2 * n) * kChunk);
     const int gw = gj_reg_warps(nsp), gl = gj_reg_lanes(n, 32 * gw);
-    const size_t slot_per_spin = (size_t)2 * gw * kGjCols * gl;  // double2
-    size_t sbytes = (sizeof(double2) * slot_per_spin + sizeof(unsigned long long) * 2 * gw) * 2;
+    const size_t slot_per_spin = (size_t)2 * gw * (gl > 0 ? gj_reg_slot(gl) : 0);  // double2
+    size_t sbytes = sizeof(double2) * 2 * slot_per_spin + sizeof(unsigned) * 2 * 2 * gw;
     size_t rbytes = fbytes > ubytes ? fbytes : ubytes;
     if (sbytes > rbytes) rbytes = sbytes;
     const size_t pbytes = sizeof(double2) * 2 * gj_panel_scratch(n);
@@ -182,7 +188,7 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
     t.part = t.U ? t.U + (size_t)kChunk * ldu : nullptr;
     t.gslot[0] = t.F0;
     t.gslot[1] = t.F0 ? t.F0 + slot_per_spin : nullptr;
-    t.gkey[0] = t.F0 ? reinterpret_cast<unsigned long long *>(t.F0 + 2 * slot_per_spin) : nullptr;
+    t.gkey[0] = t.F0 ? reinterpret_cast<unsigned *>(t.F0 + 2 * slot_per_spin) : nullptr;
     t.gkey[1] = t.gkey[0] ? t.gkey[0] + 2 * gw : nullptr;
     t.pscr[0] = gm ? nullptr : t.F0;
     t.pscr[1] = (gm || !t.F0) ? nullptr : t.F0 + gj_panel_scratch(n);
@@ -1011,113 +1017,155 @@ __device__ inline void gj_invert_gmem(double2 *W, int ld, int n, int *perm, doub
   }
 }
 
-// The same inversion (same pivot rule, same outputs perm, dk, W and the
-// singular flag) with every row held in registers: thread gt of the
-// 32G-thread group owns row r = gt / L and the columns s + L j (s = gt % L,
-// j < kGjCols) with L = gj_reg_lanes(n, 32G). Per step k:
-//   * the owner of column k passes each row's entry to the row's lanes
-//     (width-L shuffle) and the row's lane 0 forms its pivot key: the bits
-//     of |re|+|im| (non-negative doubles order as integers) with the low
-//     byte replaced by 255 - r, so ties go to the lowest row;
-//   * a warp-wide max of the keys (two 32-bit redux steps); the warp's best
-//     row publishes its slice to the warp's slot, lane 0 its key;
-//   * one group barrier; every thread takes the best warp and updates its
-//     registers v -= (f / pivot) * pivot_row, column k becoming -f / pivot.
-// The pivot row is left unscaled (its column k set to 1) and every row is
-// divided by its own pivot at the end, which gives the normalised
-// Gauss-Jordan result. Slots and keys are double-buffered by the parity
-// of k, so one barrier per step separates the writes of step k+2 from the
-// reads of step k. Only the low 8 bits of |re|+|im| are dropped from the
-// comparison (ties within 2^-44 relative go to the lowest row).
-// slots: 2 * G * kGjCols * L double2; keys: 2 * G.
+// 1/d by Newton-Raphson from the hardware estimate (rcp.approx.ftz.f64):
+// each step y <- y + y (1 - d y) doubles the number of correct bits, and
+// two steps bring the estimate to within a few units in the last place.
+// Branch-free, unlike the correctly rounded division, so the scheduler can
+// overlap it with independent work. d = 0 or subnormal gives NaN.
+__device__ __forceinline__ double rcp_newton(double d) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+  double e = fma(-d, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-d, y, 1.0);
+  return fma(y, e, y);
+}
+
+// The same inversion (same pivot rule up to ties, same outputs perm, dk, W
+// and the singular flag) with every row held in registers: thread gt of
+// the 32G-thread group (G = 4 or 8) owns row r = gt / L and the columns
+// s kGjCols + j (s = gt % L, j < kGjCols) with L = gj_reg_lanes(n, 32G).
+// Step k (column k, owned by lane k / kGjCols of each row, register
+// k % kGjCols):
+//   * the owner lane forms the row's pivot key, the top 32 bits of the
+//     double |re|+|im| (non-negative doubles order as integers) with the
+//     low byte replaced by 255 - r (ties within 2^-12 relative go to the
+//     lowest row; rows already used give 0), and the reciprocal of its
+//     candidate, 1 / pivot = conj(pivot) / |pivot|^2 (rcp_newton);
+//   * one redux gives the warp's best row, which publishes its columns,
+//     reciprocal and |pivot|^2 to the warp's slot, lane 0 the key;
+//   * one group barrier; every thread takes the best of the G keys (one or
+//     two 16-byte loads), the pivot row's slot, and updates its registers
+//     v -= (f / pivot) pivot_row, column k becoming -f / pivot.
+// The iteration is software-pipelined: after the barrier of step k a
+// thread first updates the register of column k+1, then forms step k+1's
+// key and reciprocal and starts its redux, then updates its other columns
+// (their loads and FMAs hide the redux and the reciprocal), then publishes
+// for step k+1. The pivot row is left unscaled (its column k set to 1) and
+// every row is divided by its own pivot at the end, which gives the
+// normalised Gauss-Jordan result. Slots and keys are double-buffered by
+// the parity of k: the publications for step k+1 follow the barrier of
+// step k, after every read of step k-1.
+// slots: 2 G gj_reg_slot(L) double2; keys: 2 G unsigned, 16-byte aligned
+// (G is 4 or 8: the keys of a step are one or two 16-byte words).
 __device__ inline void gj_invert_reg(double2 *W, int ld, int n, int *perm, double *dk,
                                      int *singular, int gt, int G, int bar_id, double2 *slots,
-                                     unsigned long long *keys) {
+                                     unsigned *keys) {
+  constexpr int C = kGjCols;
   const int nthr = 32 * G, lane = gt & 31, wg = gt >> 5;
   const int L = gj_reg_lanes(n, nthr);
   const int r = gt / L, s = gt - (gt / L) * L;
-  const int sw = kGjCols * L;
-  auto gsync = [&]() {
-    if (G == 1) __syncwarp();
-    else asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthr) : "memory");
-  };
-  double2 v[kGjCols];
+  const int rpw_log = 5 - (31 - __clz(L));  // log2(32 / L): rows per warp
+  const int SL = gj_reg_slot(L), HDR = L * (C + 1);
+  auto gsync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(nthr) : "memory"); };
+  double2 v[C];
 #pragma unroll
-  for (int j = 0; j < kGjCols; j++) {
-    const int c = s + L * j;
+  for (int j = 0; j < C; j++) {
+    const int c = s * C + j;
     v[j] = (r < n && c < n) ? W[r * ld + c] : make_double2(0.0, 0.0);
   }
   bool used = r >= n;
   double2 my_inv = make_double2(1.0, 0.0);
+  auto pivot_key = [&](double2 f, bool own) -> unsigned {
+    const double a = fabs(f.x) + fabs(f.y);
+    return (own && !used) ? ((unsigned)__double2hiint(a) & ~0xFFu) | (unsigned)(255 - r) : 0u;
+  };
+  // step k's candidates: the warp's best row, its reciprocal and |pivot|^2
+  auto publish = [&](int k, unsigned wk, bool own, double2 f0, double cd, double crd) {
+    const int buf = k & 1;
+    double2 *mys = slots + (buf * G + wg) * SL;
+    if (wk != 0u && r == 255 - (int)(wk & 0xFFu)) {
 #pragma unroll
-  for (int j = 0; j < kGjCols; j++) {
+      for (int jj = 0; jj < C; jj++) mys[s * (C + 1) + jj] = v[jj];
+      if (own) {
+        mys[HDR] = make_double2(f0.x * crd, -f0.y * crd);
+        mys[HDR + 1] = make_double2(cd, 0.0);
+      }
+    }
+    if (lane == 0) keys[buf * G + wg] = wk;
+  };
+  double fx, fy;  // this row's entry in the pivot column (the multiplier source)
+  {
+    const bool own = s == 0;
+    const double2 f0 = v[0];
+    const double cd = f0.x * f0.x + f0.y * f0.y;
+    const unsigned wk = __reduce_max_sync(0xffffffffu, pivot_key(f0, own));
+    publish(0, wk, own, f0, cd, rcp_newton(cd));
+    fx = __shfl_sync(0xffffffffu, f0.x, 0, L);
+    fy = __shfl_sync(0xffffffffu, f0.y, 0, L);
+  }
 #pragma unroll 1
-    for (int ss = 0; ss < L; ss++) {
-      const int k = j * L + ss;
-      if (k >= n) break;
-      const int buf = k & 1;
-      const double fx = __shfl_sync(0xffffffffu, v[j].x, ss, L);
-      const double fy = __shfl_sync(0xffffffffu, v[j].y, ss, L);
-      unsigned long long key = 0ull;
-      if (!used && s == 0) {
-        const double a = fabs(fx) + fabs(fy);
-        key = ((unsigned long long)__double_as_longlong(a) & ~0xFFull) | (unsigned)(255 - r);
-      }
-      {
-        const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
-        const unsigned hm = __reduce_max_sync(0xffffffffu, hi);
-        const unsigned lm = __reduce_max_sync(0xffffffffu, hi == hm ? lo : 0u);
-        key = ((unsigned long long)hm << 32) | lm;
-      }
-      const int pw = 255 - (int)(key & 0xFFull);
-      double2 *mys = slots + (buf * G + wg) * sw;
-      if (key != 0ull && r == pw) {
+  for (int sb = 0; sb * C < n; sb++) {
+    const bool own = s == sb;
 #pragma unroll
-        for (int jj = 0; jj < kGjCols; jj++) mys[s + L * jj] = v[jj];
-      }
-      if (lane == 0) keys[buf * G + wg] = key;
+    for (int j = 0; j < C; j++) {
+      const int k = sb * C + j;
+      const int buf = k & 1;
       gsync();
-      unsigned long long best = keys[buf * G];
-      int bw = 0;
-      for (int w = 1; w < G; w++) {
-        const unsigned long long kw = keys[buf * G + w];
-        if (kw > best) {
-          best = kw;
-          bw = w;
+      unsigned best;
+      {
+        const uint4 k4 = *reinterpret_cast<const uint4 *>(keys + buf * G);
+        best = max(max(k4.x, k4.y), max(k4.z, k4.w));
+        if (G > 4) {
+          const uint4 k8 = *reinterpret_cast<const uint4 *>(keys + buf * G + 4);
+          best = max(best, max(max(k8.x, k8.y), max(k8.z, k8.w)));
         }
       }
-      // Every unused row's key has 255 - r in its low byte, so p is an unused
-      // row < n at every step, an exactly zero or NaN column included.
-      const int p = 255 - (int)(best & 0xFFull);
-      const double2 *ps = slots + (buf * G + bw) * sw;
-      const double2 piv = ps[k];
-      const double d = piv.x * piv.x + piv.y * piv.y;
-      const double rd = 1.0 / d;
-      const double2 inv = make_double2(piv.x * rd, -piv.y * rd);
+      // Every unused row's key has 255 - r in its low byte, so p is an
+      // unused row < n at every step, an exactly zero or NaN column included.
+      const int p = 255 - (int)(best & 0xFFu);
+      const double2 *ps = slots + (buf * G + (p >> rpw_log)) * SL;
+      const double2 inv = ps[HDR];
       if (gt == 0) {
         perm[k] = p;
-        dk[k] = d;
-        if ((best >> 8) == 0ull) *singular = 1;  // every candidate exactly zero
+        dk[k] = ps[HDR + 1].x;
+        if ((best >> 8) == 0u) *singular = 1;  // every candidate zero (or subnormal)
       }
-      if (r == p) {
-        used = true;
-        my_inv = inv;
-        if (s == ss) v[j] = make_double2(1.0, 0.0);
-      } else if (r < n) {
-        const double2 fac = cmul(make_double2(fx, fy), inv);
+      const bool piv = r == p;
+      used = used || piv;
+      my_inv = piv ? inv : my_inv;
+      double2 fac = cmul(make_double2(fx, fy), inv);
+      if (piv) fac = make_double2(0.0, 0.0);
+      // column k+1 first: step k+1's key depends on it
+      const int jn = (j + 1) % C;
+      {
+        const double2 b = ps[s * (C + 1) + jn];
+        v[jn].x = fma(-fac.x, b.x, fma(fac.y, b.y, v[jn].x));
+        v[jn].y = fma(-fac.x, b.y, fma(-fac.y, b.x, v[jn].y));
+      }
+      const int sbn = j + 1 == C ? sb + 1 : sb;
+      const bool ownn = s == sbn;
+      const double2 f0 = v[jn];
+      const double cd = f0.x * f0.x + f0.y * f0.y;
+      const unsigned wk = __reduce_max_sync(0xffffffffu, pivot_key(f0, ownn));
 #pragma unroll
-        for (int jj = 0; jj < kGjCols; jj++) {
-          const double2 a = ps[s + L * jj];
-          v[jj].x = fma(-fac.x, a.x, fma(fac.y, a.y, v[jj].x));
-          v[jj].y = fma(-fac.x, a.y, fma(-fac.y, a.x, v[jj].y));
-        }
-        if (s == ss) v[j] = make_double2(-fac.x, -fac.y);
+      for (int jj = 0; jj < C; jj++) {
+        if (jj == jn) continue;
+        const double2 b = ps[s * (C + 1) + jj];
+        v[jj].x = fma(-fac.x, b.x, fma(fac.y, b.y, v[jj].x));
+        v[jj].y = fma(-fac.x, b.y, fma(-fac.y, b.x, v[jj].y));
       }
+      if (own) v[j] = piv ? make_double2(1.0, 0.0) : make_double2(-fac.x, -fac.y);
+      const double crd = rcp_newton(cd);
+      if (k + 1 >= n) break;
+      publish(k + 1, wk, ownn, f0, cd, crd);
+      fx = __shfl_sync(0xffffffffu, f0.x, sbn, L);
+      fy = __shfl_sync(0xffffffffu, f0.y, sbn, L);
     }
   }
 #pragma unroll
-  for (int j = 0; j < kGjCols; j++) {
-    const int c = s + L * j;
+  for (int j = 0; j < C; j++) {
+    const int c = s * C + j;
     if (r < n && c < n) W[r * ld + c] = cmul(v[j], my_inv);
   }
   gsync();

@@ -415,6 +415,7 @@ def b200_arm(args, rank, world, local_rank):
         dist.barrier()
     h.profile(True)
     h.block_reset()
+    acc0 = h.counters()
     dev_ms = 0.0
     with Clocks(local_rank) as clk:
         torch.cuda.synchronize()
@@ -504,7 +505,8 @@ def b200_arm(args, rank, world, local_rank):
             "kernel_ms": {"pairs": pair_ms, "move": move_ms, "branch": br_ms, "gather": ga_ms},
             "wall_s": wall,
             "e_mixed": e_mean,
-            "acceptance": acc["accepted"] / max(acc["proposed"], 1),
+            "acceptance": (acc["accepted"] - acc0["accepted"]) /
+                          max(acc["proposed"] - acc0["proposed"], 1),  # timed generations
             "clocks": clk.summary(),
         }
     if dist:
