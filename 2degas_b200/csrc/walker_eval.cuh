@@ -1649,9 +1649,12 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
         phase_mark(S, PH_CROSS, tph);
         continue;
       }
-      // cross term: M (2n x 2n, row stride ldM, over A[sp], W[sp]; the
-      // padding columns zero), then per chunk of 16 electrons Y = M U on
-      // the FP64 tensor cores and the quadratic forms sum_p U(p,c) Y(p,c)
+      // cross term: M (2n x 2n, row stride ldM, over A[sp], W[sp]), then
+      // per chunk of 16 electrons Y = M U on the FP64 tensor cores and the
+      // quadratic forms sum_p U(p,c) Y(p,c). M is symmetric, so in 8 x 8
+      // blocks u^T M u = 2 sum_P u_P^T (sum_{Q<P} M_PQ u_Q + M_PP u_P / 2):
+      // only the blocks Q <= P are built, the diagonal ones halved, and the
+      // padding columns of the last block (up to 4 KT) zero.
       const int n2 = 2 * ns, ldM = xt_ldm(2 * ns), ldU = xt_ldu(2 * ns);
       const int RT = xt_row_tiles(n2), KT = (n2 + 3) / 4;
       const int warp = tid >> 5, lane = tid & 31, lg = lane >> 2, lt = tid & 3;
@@ -1659,13 +1662,15 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
       for (int p = warp; p < n2; p += kThreads / 32) {
         const int a = p >= ns ? 1 : 0, j = p - a * ns;
         const double2 *Fa = a ? m.F1 : m.F0;
-        for (int qq = lane; qq < ldM; qq += 32) {
+        const int pb = p >> 3, qend = min(8 * (pb + 1), 4 * KT);
+        for (int qq = lane; qq < qend; qq += 32) {
           double v = 0.0;
           if (qq < n2) {
             const int c = qq >= ns ? 1 : 0, k = qq - c * ns;
             const double2 fa = Fa[k + j * ns];
             const double2 fc = (c ? m.F1 : m.F0)[j + k * ns];
             v = fa.x * fc.x - fa.y * fc.y;
+            if ((qq >> 3) == pb) v *= 0.5;
           }
           M[p * ldM + qq] = v;
         }
@@ -1685,8 +1690,6 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
       for (int col = warp; col < kChunk; col += kThreads / 32)
         for (int r = n2 + lane; r < ldU; r += 32) UT[col * ldU + r] = 0.0;
       phase_mark(S, PH_MBUILD, tph);
-      // work units: (row tile, group of CT column tiles), RT*NTG of them
-      const int NTG = RT >= 5 ? 1 : (RT >= 3 ? 2 : 4), CT = 4 / NTG;
       static_assert(kThreads == 16 * (kChunk / 2), "16 lanes per electron of a chunk");
       for (int i0 = 0; i0 < N; i0 += kChunk / 2) {
         // UT[(i,b)][(a,j)] = J_{j,i}[a][b] for electrons i = i0 .. i0+15,
@@ -1777,36 +1780,42 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
         __syncthreads();
         phase_mark(S, PH_DRIFT, tph);
         // Y = M U by warps, 8x8 output tiles (mma.m8n8k4 f64 fragments:
-        // A(row lg, col lt), B(row lt, col lg), D(row lg, cols 2lt, 2lt+1)).
-        // Rows of the last row tile beyond n2 reuse row n2-1 (their outputs
-        // meet zero rows of UT). Each unit's rows dot their UT rows into
+        // A(row lg, col lt), B(row lt, col lg), D(row lg, cols 2lt, 2lt+1)),
+        // over the block lower triangle: row tile P takes the k-steps of
+        // the column blocks Q <= P. Warp w takes row tiles P = w (mod 8)
+        // with column tiles 0-1 and P = RT-1-w (mod 8) with column tiles
+        // 2-3, so every warp has 2 (RT + 1) k-steps at RT = 8. Rows of the
+        // last row tile beyond n2 reuse row n2-1 (their outputs meet zero
+        // rows of UT). Each tile's rows dot their UT rows into
         // part[row tile][column].
-        for (int u = warp; u < RT * NTG; u += kThreads / 32) {
-          const int mt = u / NTG, nt0 = (u - mt * NTG) * CT;
-          const double *Ma = M + min(8 * mt + lg, n2 - 1) * ldM + lt;
-          double acc[4][2];
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {
+#pragma unroll 1
+          for (int w8 = warp; w8 < RT; w8 += kThreads / 32) {
+            const int P = h == 0 ? w8 : RT - 1 - w8;
+            const int kend = min(2 * P + 2, KT);
+            const double *Ma = M + min(8 * P + lg, n2 - 1) * ldM + lt;
+            const double *Ub = UT + (16 * h + lg) * ldU + lt;
+            double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll 4
+            for (int kt = 0; kt < kend; kt++) {
+              const double a = Ma[4 * kt];
+              dmma_m8n8k4(acc[0], a, Ub[4 * kt]);
+              dmma_m8n8k4(acc[1], a, Ub[8 * ldU + 4 * kt]);
+            }
 #pragma unroll
-          for (int c = 0; c < 4; c++) acc[c][0] = acc[c][1] = 0.0;
-          for (int kt = 0; kt < KT; kt++) {
-            const double a = Ma[4 * kt];
-#pragma unroll
-            for (int c = 0; c < 4; c++)
-              if (c < CT) dmma_m8n8k4(acc[c], a, UT[(8 * (nt0 + c) + lg) * ldU + 4 * kt + lt]);
-          }
-#pragma unroll
-          for (int c = 0; c < 4; c++) {
-            if (c < CT) {
-              const int col = 8 * (nt0 + c) + 2 * lt;
-              double s0 = acc[c][0] * UT[col * ldU + 8 * mt + lg];
-              double s1 = acc[c][1] * UT[(col + 1) * ldU + 8 * mt + lg];
+            for (int c = 0; c < 2; c++) {
+              const int col = 16 * h + 8 * c + 2 * lt;
+              double s0 = acc[c][0] * UT[col * ldU + 8 * P + lg];
+              double s1 = acc[c][1] * UT[(col + 1) * ldU + 8 * P + lg];
 #pragma unroll
               for (int o = 4; o < 32; o <<= 1) {
                 s0 += __shfl_xor_sync(0xffffffffu, s0, o);
                 s1 += __shfl_xor_sync(0xffffffffu, s1, o);
               }
               if (lg == 0) {
-                m.part[mt * kChunk + col] = s0;
-                m.part[mt * kChunk + col + 1] = s1;
+                m.part[P * kChunk + col] = s0;
+                m.part[P * kChunk + col + 1] = s1;
               }
             }
           }
@@ -1818,7 +1827,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
             double t3 = 0.0;
             for (int rt = 0; rt < RT; rt++)
               t3 += m.part[rt * kChunk + 2 * tid] + m.part[rt * kChunk + 2 * tid + 1];
-            m.lapd[i] += t3;
+            m.lapd[i] += 2.0 * t3;
           }
         }
         // The next chunk's Jacobian build touches neither part nor these
