@@ -151,6 +151,7 @@ int build_devsys(const qmc2d_system *sys, q2d::DevSys *hs, std::vector<double> *
     s.tab_tail[t] = tb.tail;
     coef->insert(coef->end(), tb.ut, tb.ut + 4 * (size_t)(tb.ngrid + 1));
     s.tab_nkew[t] = tb.nk_ewald;
+    s.tab_kself[t] = tb.nk_ewald > 0 ? tb.vk[tb.nk_ewald] : 0.0;
     s.tab_vkoff[t] = (int)coef->size();
     if (tb.nk_ewald > 0) coef->insert(coef->end(), tb.vk, tb.vk + tb.nk_ewald + 1);
   }

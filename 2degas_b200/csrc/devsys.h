@@ -35,6 +35,7 @@ struct DevSys {
   int tab_nkew[QMC2D_MAX_TABLES];
   int tab_vkoff[QMC2D_MAX_TABLES];  // offset of v_k in the packed buffer
   double tab_tail[QMC2D_MAX_TABLES];
+  double tab_kself[QMC2D_MAX_TABLES];  // v_k list's closing (self-term) coefficient
   // Pair rows: for type pair (a, b) (block cmb_blk[a][b] of cmb_ng + 1 rows;
   // type pairs with the same four tables share a block) and knot k, 16
   // doubles = the four-coefficient rows of the u2, u3, backflow and v2

@@ -174,6 +174,7 @@ extern "C" int qmc2d_compute_properties_noalloc(const qmc2d_system *sys, int nw,
     s.tab_tail[t] = tb.tail;
     off += 4 * (size_t)(tb.ngrid + 1);
     s.tab_nkew[t] = tb.nk_ewald;
+    s.tab_kself[t] = tb.nk_ewald > 0 ? tb.vk[tb.nk_ewald] : 0.0;
     s.tab_vkoff[t] = (int)off;
     if (tb.nk_ewald > 0) off += tb.nk_ewald + 1;
   }

@@ -428,7 +428,7 @@ __device__ int measure(const DevSys &S, const Sweep &m, const double logdet[2], 
       for (int k = lane; k < S.tab_nkew[iv]; k += 32)
         ks += __ldg(vk + k) * (m.rhok[2 * (it * S.nk + k)] * m.rhok[2 * (jt * S.nk + k)] +
                                m.rhok[2 * (it * S.nk + k) + 1] * m.rhok[2 * (jt * S.nk + k) + 1]);
-      const double c = wsum(ks) + __ldg(vk + S.tab_nkew[iv]) * S.npnorm;
+      const double c = wsum(ks) + S.tab_kself[iv] * S.npnorm;
       pot_t[it] += c;
       pot0 += c;
     }

@@ -1450,7 +1450,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
 
   // ---- backflow Slater determinants (slater_excitations, reptation.f:9967)
   int status = ST_OK;
-  double logdet_sum = 0.0;
+  double logdet_sum = 0.0, ltf_j = 0.0;  // ltf_j: sum of the Jastrow -ln psi terms
   if (S.has_bf) {
     const int n = S.nmax;
     // orbitals of both spins (paho_orbitals, reptation.f:10298-10315)
@@ -1543,11 +1543,14 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
       }
     }
     {
-      double ld_acc = 0.0;
+      double acc[2] = {0.0, 0.0};  // log|det| and the Jastrow terms, one reduction
       for (int sp = 0; sp < nt; sp++)
         for (int k = tid; k < S.np[sp]; k += kThreads)
-          ld_acc += 0.5 * log((sp ? m.dk[1] : m.dk[0])[k]);
-      logdet_sum = block_sum(ld_acc, m.red);
+          acc[0] += 0.5 * log((sp ? m.dk[1] : m.dk[0])[k]);
+      for (int i = tid; i < N; i += kThreads) acc[1] += m.ltf[i];
+      block_sum_n<2>(acc, m.red);
+      logdet_sum = acc[0];
+      ltf_j = acc[1];
       if (m.iscal[0] || m.iscal[1]) status |= ST_SINGULAR;
     }
     phase_mark(S, reg_path ? PH_RHOK : PH_INVERT, tph);
@@ -1840,14 +1843,12 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
     }
   } else {
     rhok(tid, kThreads);
-    __syncthreads();
+    for (int i = tid; i < N; i += kThreads) ltf_j += m.ltf[i];
+    ltf_j = block_sum(ltf_j, m.red);
     phase_mark(S, PH_RHOK, tph);
   }
 
   // ---- assemble: -ln psi, kinetic (reptation.f:2729), potential (:3986)
-  double ltf_j = 0.0;
-  for (int i = tid; i < N; i += kThreads) ltf_j += m.ltf[i];
-  ltf_j = block_sum(ltf_j, m.red);
   double ltf = ltf_j - logdet_sum;
   bool underflow = false;
   if (S.has_bf && S.ref_underflow) underflow = exp(-ltf * 2.0) <= 0.0;
@@ -1929,20 +1930,31 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
   pot0 = pot_t[0] + pot_t[1];
   // k space (reptation.f:4034-4052): rho_k read by type index
   {
+    // every type pair in one loop, so the four v_k loads of a k are in
+    // flight together (the sums keep their order: k ascending per thread)
     double ks[4] = {0, 0, 0, 0};
+    int nkp[4], nkmax = 0;
+    const double *vkp[4];
 #pragma unroll
-    for (int it = 0; it < 2; it++)
+    for (int p = 0; p < 4; p++) {
+      const int it = p >> 1, jt = p & 1;
+      const int iv = (it < nt && jt < nt) ? S.iv2[it][jt] : -1;
+      nkp[p] = iv >= 0 ? S.tab_nkew[iv] : 0;
+      vkp[p] = S.coef + (iv >= 0 ? S.tab_vkoff[iv] : 0);
+      nkmax = max(nkmax, nkp[p]);
+    }
+    for (int k = tid; k < nkmax; k += kThreads) {
+      double vk[4];
 #pragma unroll
-      for (int jt = 0; jt < 2; jt++) {
-        if (it >= nt || jt >= nt) continue;
-        int iv = S.iv2[it][jt];
-        if (iv < 0 || S.tab_nkew[iv] == 0) continue;
-        const double *vk = S.coef + S.tab_vkoff[iv];
-        for (int k = tid; k < S.tab_nkew[iv]; k += kThreads)
-          ks[2 * it + jt] +=
-              __ldg(vk + k) * (m.rhok[2 * (it * S.nk + k)] * m.rhok[2 * (jt * S.nk + k)] +
-                               m.rhok[2 * (it * S.nk + k) + 1] * m.rhok[2 * (jt * S.nk + k) + 1]);
+      for (int p = 0; p < 4; p++) vk[p] = k < nkp[p] ? __ldg(vkp[p] + k) : 0.0;
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        const int it = p >> 1, jt = p & 1;
+        if (k < nkp[p])
+          ks[p] += vk[p] * (m.rhok[2 * (it * S.nk + k)] * m.rhok[2 * (jt * S.nk + k)] +
+                            m.rhok[2 * (it * S.nk + k) + 1] * m.rhok[2 * (jt * S.nk + k) + 1]);
       }
+    }
     block_sum_n<4>(ks, m.red);
 #pragma unroll
     for (int it = 0; it < 2; it++)
@@ -1951,7 +1963,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
         if (it >= nt || jt >= nt) continue;
         int iv = S.iv2[it][jt];
         if (iv < 0 || S.tab_nkew[iv] == 0) continue;
-        double c = ks[2 * it + jt] + __ldg(S.coef + S.tab_vkoff[iv] + S.tab_nkew[iv]) * S.npnorm;
+        double c = ks[2 * it + jt] + S.tab_kself[iv] * S.npnorm;
         pot_t[it] += c;
         pot0 += c;
       }
@@ -1977,6 +1989,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
     props[QMC2D_JETOT] = et;
     props[QMC2D_JE2] = et * et;
     *sign = 1.0;
+    m.red[0] = et;  // for every thread's finiteness check (red is free here)
   }
   // rho_k properties (compute_properties, reptation.f:2672-2683)
   {
@@ -1989,7 +2002,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
     }
   }
   __syncthreads();
-  double et = props[QMC2D_JETOT];
+  const double et = m.red[0];
   if (!isfinite(et) || !isfinite(ltf)) status |= ST_NONFINITE;
   __syncthreads();
   phase_mark(S, PH_ASSEMBLE, tph);
