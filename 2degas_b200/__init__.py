@@ -185,6 +185,11 @@ class Handle:
         """Load walker records from raw host addresses (putconf for a population)."""
         self._chk(self.lib.qmc2d_population_load(self.h, nw, x, g, hl, p, s, age))
 
+    def population_load_async_ptr(self, nw, x, g, hl, p, s, age):
+        """qmc2d_population_load_async: returns at once; the buffers stay in use
+        until the next call that synchronises the handle (a move, a get)."""
+        self._chk(self.lib.qmc2d_population_load_async(self.h, nw, x, g, hl, p, s, age))
+
     def stream(self):
         st = ctypes.c_void_p()
         self._chk(self.lib.qmc2d_stream(self.h, ctypes.byref(st)))

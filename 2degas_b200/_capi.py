@@ -205,6 +205,8 @@ SIGNATURES = {
     "qmc2d_population_set": (c_int, [c_void_p, c_int, PD]),
     "qmc2d_population_size": (c_int, [c_void_p, POINTER(c_int)]),
     "qmc2d_population_get": (c_int, [c_void_p, PD, PD, PD, PD, PD, PD]),
+    "qmc2d_population_load_async": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                                            c_void_p, c_void_p, c_void_p]),
     "qmc2d_population_load": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                       c_void_p, c_void_p]),
     "qmc2d_stream": (c_int, [c_void_p, POINTER(c_void_p)]),

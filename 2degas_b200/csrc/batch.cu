@@ -188,6 +188,7 @@ int run(qmc2d_batch *b, int n, int dmc, const double *delta, const double *etria
   std::vector<uint32_t> ctr(2 * np);
   for (size_t k = 0; k < np; k++) {
     qmc2d_handle *h = b->h[k];
+    BCK(join_side(h));
     BCK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * h->nw, h->stream));
     if (h->hs.delta != delta[k] && h->hs.adrift != 0.0) {  // the drift cutoff reads delta
       h->hs.delta = delta[k];

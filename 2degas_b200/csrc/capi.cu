@@ -184,7 +184,8 @@ void free_pop(q2d::DevPop *p) {
 
 int sync_status(qmc2d_handle *h, int nw) {
   // the status words follow the kernels on the handle's stream into pinned
-  // host memory: one synchronisation for both
+  // host memory: one synchronisation for both (and for pending side copies)
+  CK(join_side(h));
   if (nw > 0)
     CK(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(int) * nw, cudaMemcpyDeviceToHost,
                        h->stream));
@@ -291,8 +292,12 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
     q2d::set_error(buf);
     return fail(QMC2D_ERR_LIMIT);
   }
-  if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
+  if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking)) != cudaSuccess)
     return fail(cuda_fail(e, "cudaStreamCreate"));
+  if ((e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&h->ev_side, cudaEventDisableTiming)) != cudaSuccess)
+    return fail(cuda_fail(e, "cudaEventCreate"));
   int st;
   if ((e = dalloc(&h->d_coef, coef.size())) != cudaSuccess) return fail(cuda_fail(e, "alloc"));
   if ((e = dalloc(&h->d_kvec, 2 * (size_t)std::max(1, sys->nk))) != cudaSuccess)
@@ -373,6 +378,7 @@ extern "C" int qmc2d_set_precision(qmc2d_handle *h, int precision) {
     return QMC2D_ERR_ARG;
   }
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   h->hs.pair_f32 = precision == QMC2D_PRECISION_MIXED ? 1 : 0;
   CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
@@ -404,6 +410,7 @@ extern "C" int qmc2d_set_inversion(qmc2d_handle *h, int layout) {
     return QMC2D_ERR_ARG;
   }
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   h->hs.tune_inv = layout;
   CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));
@@ -417,6 +424,7 @@ extern "C" int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *
     return QMC2D_ERR_STACK;
   }
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   q2d::MoveArgs a{};
   a.nw = h->nw;
   a.scr = h->d_mscr;
@@ -507,6 +515,7 @@ extern "C" int qmc2d_update_twist(qmc2d_handle *h, const qmc2d_system *sys) {
     return QMC2D_ERR_LIMIT;
   }
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   CK(cudaMemcpyAsync(h->d_gvec, sys->gvec, sizeof(double) * 2 * sys->ngvec,
                      cudaMemcpyHostToDevice, h->stream));
   h->hs.ngvec = sys->ngvec;
@@ -518,6 +527,7 @@ extern "C" int qmc2d_update_twist(qmc2d_handle *h, const qmc2d_system *sys) {
 
 extern "C" int qmc2d_destroy(qmc2d_handle *h) {
   if (!h) return QMC2D_OK;
+  if (h->side) cudaStreamSynchronize(h->side);
   if (h->stream) cudaStreamSynchronize(h->stream);
   q2d::rmc_free(&h->rmc);
   for (int k = 0; k < 2; k++) free_pop(&h->pop[k]);
@@ -529,6 +539,9 @@ extern "C" int qmc2d_destroy(qmc2d_handle *h) {
   if (h->h_status) cudaFreeHost(h->h_status);
   for (int k = 0; k < QMC2D_NKERNELS; k++)
     for (cudaEvent_t e : h->ev[k]) cudaEventDestroy(e);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_side) cudaEventDestroy(h->ev_side);
+  if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return QMC2D_OK;
@@ -543,6 +556,7 @@ extern "C" int qmc2d_stream(qmc2d_handle *h, void **stream) {
 extern "C" int qmc2d_profile(qmc2d_handle *h, int enable) {
   if (!h) return QMC2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   CK(cudaStreamSynchronize(h->stream));
   h->prof = enable != 0;
   for (int k = 0; k < QMC2D_NKERNELS; k++) {
@@ -556,6 +570,7 @@ extern "C" int qmc2d_profile(qmc2d_handle *h, int enable) {
 extern "C" int qmc2d_phase_timers(qmc2d_handle *h, int enable, unsigned long long *cycles) {
   if (!h) return QMC2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   CK(cudaStreamSynchronize(h->stream));
   if (enable) {
     if (!h->hs.phase) CK(dalloc(&h->hs.phase, q2d::PH_COUNT));
@@ -574,6 +589,7 @@ extern "C" int qmc2d_phase_timers(qmc2d_handle *h, int enable, unsigned long lon
 extern "C" int qmc2d_profile_get(qmc2d_handle *h, int kernel, double *ms, long *launches) {
   if (!h || kernel < 0 || kernel >= QMC2D_NKERNELS) return QMC2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   CK(cudaStreamSynchronize(h->stream));
   for (int i = 0; i < h->ev_used[kernel]; i++) {
     float t = 0.f;
@@ -596,6 +612,7 @@ extern "C" int qmc2d_compute_properties_dev(qmc2d_handle *h, int nw, const doubl
   }
   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   if (nw > 0) CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * nw, st));
   ProfScope ps(h, QMC2D_KERNEL_EVAL, st);
   CK(q2d::launch_eval(h->hs, h->ds, nw, x_dev, g_dev, hl_dev, props_dev, s_dev, h->d_status,
@@ -609,6 +626,7 @@ extern "C" int qmc2d_compute_properties_dev_status(qmc2d_handle *h, int nw, void
     return QMC2D_ERR_ARG;
   }
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   if (stream) CK(cudaStreamSynchronize((cudaStream_t)stream));
   return sync_status(h, nw);
 }
@@ -621,6 +639,7 @@ extern "C" int qmc2d_compute_properties(qmc2d_handle *h, int nw, const double *x
   }
   if (nw == 0) return QMC2D_OK;
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   size_t N2 = 2 * (size_t)h->N;
   CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * nw, h->stream));
   CK(cudaMemcpyAsync(h->d_x, x, sizeof(double) * N2 * nw, cudaMemcpyHostToDevice, h->stream));
@@ -646,6 +665,7 @@ extern "C" int qmc2d_population_set(qmc2d_handle *h, int nw, const double *x) {
     return QMC2D_ERR_POPULATION;
   }
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   q2d::DevPop &p = h->pop[h->cur];
   size_t N2 = 2 * (size_t)h->N;
   CK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * nw, h->stream));
@@ -671,6 +691,7 @@ extern "C" int qmc2d_population_get(qmc2d_handle *h, double *x, double *g, doubl
                                     double *props, double *s, double *age) {
   if (!h) return QMC2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   q2d::DevPop &p = h->pop[h->cur];
   size_t N2 = 2 * (size_t)h->N, nw = h->nw;
   cudaStream_t st = h->stream;
@@ -693,6 +714,7 @@ extern "C" int qmc2d_population_load(qmc2d_handle *h, int nw, const double *x, c
     return QMC2D_ERR_POPULATION;
   }
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   q2d::DevPop &p = h->pop[h->cur];
   size_t N2 = 2 * (size_t)h->N;
   cudaStream_t st = h->stream;
@@ -707,9 +729,38 @@ extern "C" int qmc2d_population_load(qmc2d_handle *h, int nw, const double *x, c
   return QMC2D_OK;
 }
 
+extern "C" int qmc2d_population_load_async(qmc2d_handle *h, int nw, const double *x,
+                                           const double *g, const double *hl,
+                                           const double *props, const double *s,
+                                           const double *age) {
+  if (!h || !x || !g || !hl || !props || !s || !age || nw <= 0 || nw > h->cap) {
+    q2d::set_error("qmc2d_population_load_async: bad argument or population outside capacity");
+    return QMC2D_ERR_POPULATION;
+  }
+  CK(cudaSetDevice(h->device));
+  CK(join_side(h));
+  q2d::DevPop &p = h->pop[h->cur];
+  const size_t N2 = 2 * (size_t)h->N;
+  // the side copies overwrite buffers that earlier work on the stream uses
+  CK(cudaEventRecord(h->ev_fork, h->stream));
+  CK(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+  CK(cudaMemcpyAsync(p.x, x, sizeof(double) * N2 * nw, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(p.g, g, sizeof(double) * N2 * nw, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(p.h, hl, sizeof(double) * h->nt * nw, cudaMemcpyHostToDevice, h->side));
+  CK(cudaMemcpyAsync(p.p, props, sizeof(double) * h->nprops * nw, cudaMemcpyHostToDevice,
+                     h->side));
+  CK(cudaMemcpyAsync(p.s, s, sizeof(double) * nw, cudaMemcpyHostToDevice, h->side));
+  CK(cudaMemcpyAsync(p.age, age, sizeof(double) * nw, cudaMemcpyHostToDevice, h->side));
+  CK(cudaEventRecord(h->ev_side, h->side));
+  h->side_pending = true;
+  h->nw = nw;
+  return QMC2D_OK;
+}
+
 extern "C" int qmc2d_block_reset(qmc2d_handle *h) {
   if (!h) return QMC2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   CK(cudaMemsetAsync(h->d_blk, 0, sizeof(double) * h->cap * h->nprops, h->stream));
   CK(cudaMemsetAsync(h->d_norm, 0, sizeof(double) * h->cap, h->stream));
   CK(cudaMemsetAsync(h->d_cnt, 0, sizeof(double) * h->cap * 4, h->stream));
@@ -720,6 +771,7 @@ extern "C" int qmc2d_block_reset(qmc2d_handle *h) {
 extern "C" int qmc2d_block_get(qmc2d_handle *h, double *blk_av, double *blk_norm) {
   if (!h) return QMC2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   const int np = h->nprops, n = std::max(h->nw, h->rmc.nrep);
   std::vector<double> sums((size_t)np + 1, 0.0);
   if (n > 0) {
@@ -737,6 +789,7 @@ extern "C" int qmc2d_block_get(qmc2d_handle *h, double *blk_av, double *blk_norm
 extern "C" int qmc2d_counters_get(qmc2d_handle *h, qmc2d_counters *c) {
   if (!h || !c) return QMC2D_ERR_ARG;
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   CK(cudaStreamSynchronize(h->stream));
   int n = std::max(h->nw, h->rmc.nrep);
   std::vector<double> v((size_t)n * 4);
@@ -782,6 +835,7 @@ static int run_moves(qmc2d_handle *h, int nstp, int dmc, double delta, double et
       ProfScope ps(h, QMC2D_KERNEL_PAIRS, h->stream);
       CK(q2d::launch_pairs(h->hs, h->ds, h->pop[h->cur], a, h->stream));
     }
+    CK(join_side(h));  // the pair kernel reads only x and g
     {
       ProfScope ps(h, QMC2D_KERNEL_MOVE, h->stream);
       CK(q2d::launch_move(h->hs, h->ds, h->pop[h->cur], a, h->stream));
@@ -856,6 +910,7 @@ extern "C" int qmc2d_population_resample(qmc2d_handle *h, const int *src) {
       return QMC2D_ERR_ARG;
     }
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   CK(cudaMemcpyAsync(h->br.src, src, sizeof(int) * h->nw, cudaMemcpyHostToDevice, h->stream));
   const int nxt = 1 - h->cur;
   {
@@ -884,6 +939,7 @@ static int records(qmc2d_handle *h, int n, const int *slots, double *buf_dev, vo
     }
   if (n == 0) return QMC2D_OK;
   CK(cudaSetDevice(h->device));
+  CK(join_side(h));
   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
   // the slot list goes through the comb's rank scratch (cap ints), which no
   // other call uses between a generation's weights and its resample

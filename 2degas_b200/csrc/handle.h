@@ -29,6 +29,12 @@ struct qmc2d_handle {
   // staging for the batched evaluation entry point
   double *d_x = nullptr, *d_g = nullptr, *d_h = nullptr, *d_p = nullptr, *d_s = nullptr;
   cudaStream_t stream = nullptr;
+  // qmc2d_population_load_async: the records other than x and g go through
+  // this stream, ordered after the stream's earlier work (ev_fork), and the
+  // stream joins them (ev_side) before anything else reads the population
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_side = nullptr;
+  bool side_pending = false;
   int device = 0;
   uint64_t seed = 0;
   uint32_t move_counter = 0, gen_counter = 0;
@@ -44,6 +50,16 @@ struct qmc2d_handle {
   double prof_ms[QMC2D_NKERNELS] = {0};
   long prof_n[QMC2D_NKERNELS] = {0};
 };
+
+// Orders the handle's stream after the side copies of the last
+// qmc2d_population_load_async (nothing when none are pending). Every entry
+// point that touches the population calls it first; a move calls it after
+// its pair kernel, which reads only x and g.
+inline cudaError_t join_side(qmc2d_handle *h) {
+  if (!h->side_pending) return cudaSuccess;
+  h->side_pending = false;
+  return cudaStreamWaitEvent(h->stream, h->ev_side, 0);
+}
 
 // Bracket one launch of kernel k with an event pair when profiling is on.
 struct ProfScope {

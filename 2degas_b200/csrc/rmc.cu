@@ -910,6 +910,7 @@ extern "C" int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params 
     return QMC2D_ERR_ARG;
   }
   RCK(cudaSetDevice(h->device));
+  RCK(join_side(h));
   RCK(cudaStreamSynchronize(h->stream));
   const int split = h->rmc.split;  // a launch choice: kept across set-ups
   q2d::rmc_free(&h->rmc);
@@ -1007,6 +1008,7 @@ extern "C" int qmc2d_rmc(qmc2d_handle *h, int nstp) {
   }
   if (nstp == 0) return QMC2D_OK;
   RCK(cudaSetDevice(h->device));
+  RCK(join_side(h));
   RCK(cudaMemsetAsync(h->d_status, 0, sizeof(int) * h->rmc.nrep, h->stream));
   q2d::RmcArgs a = rmc_args(h, nstp);
   size_t sm = rmc_move_smem(h->hs);
@@ -1061,6 +1063,7 @@ extern "C" int qmc2d_rmc_set_launch(qmc2d_handle *h, int split) {
 extern "C" int qmc2d_rmc_get_path(qmc2d_handle *h, int rep, double *x, double *props) {
   if (!h || rep < 0 || rep >= h->rmc.nrep) return QMC2D_ERR_ARG;
   RCK(cudaSetDevice(h->device));
+  RCK(join_side(h));
   RCK(cudaStreamSynchronize(h->stream));
   q2d::RmcState &r = h->rmc;
   int ends[2];
@@ -1090,6 +1093,7 @@ extern "C" int qmc2d_rmc_path_estimators(qmc2d_handle *h, const qmc2d_rmc_estima
   }
   if (est->nvalues == 0) return QMC2D_OK;
   RCK(cudaSetDevice(h->device));
+  RCK(join_side(h));
   const size_t need = ((size_t)r.nrep + 1) * est->nvalues;
   if (need > r.est_cap) {
     RCK(cudaStreamSynchronize(h->stream));

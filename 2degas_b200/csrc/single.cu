@@ -721,6 +721,7 @@ extern "C" int qmc2d_vmc_single(qmc2d_handle *h, int nsweep, double delta, int r
     return QMC2D_ERR_CUDA;
   };
   if ((e = cudaSetDevice(h->device)) != cudaSuccess) return fail(e, "cudaSetDevice");
+  if ((e = join_side(h)) != cudaSuccess) return fail(e, "cudaStreamWaitEvent");
   if (h->hs.delta != delta && h->hs.adrift != 0.0) {
     h->hs.delta = delta;
     if ((e = cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice,
@@ -760,7 +761,7 @@ extern "C" int qmc2d_vmc_single(qmc2d_handle *h, int nsweep, double delta, int r
 extern "C" int qmc2d_single_drift(qmc2d_handle *h, double *max_err) {
   if (!h || !max_err) return QMC2D_ERR_ARG;
   cudaError_t e;
-  if ((e = cudaSetDevice(h->device)) != cudaSuccess ||
+  if ((e = cudaSetDevice(h->device)) != cudaSuccess || (e = join_side(h)) != cudaSuccess ||
       (e = cudaStreamSynchronize(h->stream)) != cudaSuccess) {
     q2d::set_error(std::string("qmc2d_single_drift: ") + cudaGetErrorString(e));
     return QMC2D_ERR_CUDA;

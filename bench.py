@@ -13,7 +13,8 @@ One step = one DMC generation over the whole population (4096
 walker-moves: pairs_kernel, move_kernel, branch, gather). `value` times the device work with CUDA events on the
 library's stream (inputs resident in HBM, L2 flushed between steps);
 `e2e` times the same steps through the public C-ABI with the walker records
-copied from and to pinned host memory every step.
+copied from and to pinned host memory every step (qmc2d_population_load_async:
+the records other than x and g arrive while the pair kernel runs).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -458,7 +459,9 @@ def b200_arm(args, rank, world, local_rank):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(k2):
-        h.population_load_ptr(nw, ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"], ptr["a"])
+        # x and g on the library stream, the other records behind the pair kernel
+        h.population_load_async_ptr(nw, ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"],
+                                    ptr["a"])
         step()
         h.population_get_ptr(ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"], ptr["a"])
         h.block_get()
@@ -735,7 +738,8 @@ def config_arm(args, rank, world, local_rank):
         d2h = h2d + npr * 8 + 8
 
         def e2e_step():
-            h.population_load_ptr(nw, ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"], ptr["a"])
+            h.population_load_async_ptr(nw, ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"],
+                                        ptr["a"])
             step()
             h.population_get_ptr(ptr["x"], ptr["g"], ptr["h"], ptr["p"], ptr["s"], ptr["a"])
             h.block_get()

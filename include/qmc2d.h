@@ -340,6 +340,17 @@ int qmc2d_population_get(qmc2d_handle *h, double *x, double *g, double *hl, doub
 int qmc2d_population_load(qmc2d_handle *h, int nw, const double *x, const double *g,
                           const double *hl, const double *props, const double *s,
                           const double *age);
+/* The same load without waiting for it: x and g are copied on the handle's
+ * stream, the other records on a second stream, and the call returns at
+ * once. The next move's pair kernel (which reads only x and g) runs while
+ * the other records are still arriving; the move kernel and every other
+ * call that uses the population wait for them. The caller must leave the
+ * buffers untouched until a call that synchronises the handle (any move,
+ * qmc2d_population_get, qmc2d_block_get) has returned; with pageable
+ * buffers the copies complete before the call returns. */
+int qmc2d_population_load_async(qmc2d_handle *h, int nw, const double *x, const double *g,
+                                const double *hl, const double *props, const double *s,
+                                const double *age);
 
 /* Block accumulators (averages(1/2), reptation.f:4283-4304): weighted sums
  * of p_old over all walkers and steps since the last reset. */
