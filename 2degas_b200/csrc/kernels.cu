@@ -362,30 +362,36 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
 // ------------------------------------------------------------- branch2
 // One block. Population-wide steps of branch2 (reptation.f:2174-2212) and
 // prov_dest's in-rank assignment (reptation.f:2260-2271) on global scratch.
-__device__ void block_exclusive_scan_partials(double *part, int n) {
+// Exclusive scan of one value per thread over the block (warp shuffles,
+// then the warp totals by warp 0); ws holds 33 values, ws[32] the total.
+template <class T>
+__device__ T block_exclusive_scan(T v, T *ws) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  T ex = __shfl_up_sync(0xffffffffu, x, 1);
+  if (lane == 0) ex = T(0);
+  __syncthreads();  // ws may still be read by a previous scan
+  if (lane == 31) ws[w] = x;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double run = 0.0;
-    for (int i = 0; i < n; i++) {
-      double t = part[i];
-      part[i] = run;
-      run += t;
+  if (w == 0) {
+    T t = lane < nwarp ? ws[lane] : T(0);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const T y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
     }
+    T e = __shfl_up_sync(0xffffffffu, t, 1);
+    if (lane == 0) e = T(0);
+    if (lane < nwarp) ws[lane] = e;
+    if (lane == 31) ws[32] = t;
   }
   __syncthreads();
-}
-
-__device__ void block_exclusive_scan_ipartials(int *part, int n) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int run = 0;
-    for (int i = 0; i < n; i++) {
-      int t = part[i];
-      part[i] = run;
-      run += t;
-    }
-  }
-  __syncthreads();
+  return ws[w] + ex;
 }
 
 constexpr int kBranchThreads = 1024;
@@ -395,9 +401,8 @@ __global__ void __launch_bounds__(kBranchThreads) branch_kernel(int nw, double *
                                                                 const uint32_t *ctr,
                                                                 BranchScratch b) {
   const uint32_t gen = gen0 + (ctr ? ctr[1] : 0u);
-  __shared__ double dpart[kBranchThreads];
-  __shared__ int ipart[kBranchThreads];
-  __shared__ int ipart2[kBranchThreads];
+  __shared__ double dws[33];
+  __shared__ int iws[33];
   __shared__ double red[32];
   const int tid = threadIdx.x, nt = blockDim.x;
   const int seg = (nw + nt - 1) / nt;
@@ -430,9 +435,7 @@ __global__ void __launch_bounds__(kBranchThreads) branch_kernel(int nw, double *
     b.delt[i] = ww - tm;
     part += ww - tm;
   }
-  dpart[tid] = part;
-  block_exclusive_scan_partials(dpart, nt);
-  double run = dpart[tid];
+  double run = block_exclusive_scan(part, dws);
   for (int i = lo; i < hi; i++) {
     run += b.delt[i];
     b.csum[i] = run;
@@ -441,18 +444,27 @@ __global__ void __launch_bounds__(kBranchThreads) branch_kernel(int nw, double *
   double k0 = b.csum[nw - 1];
   int ncomb = (int)llround(k0);
   // systematic comb: copy c lands on the first walker whose cumulative
-  // fraction reaches c + r_c (r_c from the shared stream, as rannyu2)
-  for (int c = tid; c < ncomb; c += nt) {
-    double r = uniform2(seed, (uint32_t)c, 0xFFFFFFFFu, gen, 1u).x;
-    double target = c + r;
-    int a0 = 0, a1 = nw;  // lower_bound
-    while (a0 < a1) {
-      int mid = (a0 + a1) >> 1;
-      if (b.csum[mid] < target) a0 = mid + 1;
-      else a1 = mid;
+  // fraction reaches c + r_c (r_c from the shared stream, as rannyu2), the
+  // last walker when none does. csum is non-decreasing, so copy c lands in
+  // this thread's walkers [lo, hi) exactly when csum[lo-1] < c + r_c <=
+  // csum[hi-1] (or beyond csum[nw-1] for the last segment): each thread
+  // draws only the few copies whose c is in that range and finds the walker
+  // among its own.
+  if (lo < hi) {
+    const double cprev = lo > 0 ? b.csum[lo - 1] : -1.0, clast = b.csum[hi - 1];
+    const int cmin = lo > 0 ? max(0, (int)floor(cprev) - 1) : 0;
+    const int cmax = hi == nw ? ncomb - 1 : min(ncomb - 1, (int)floor(clast));
+    for (int c = cmin; c <= cmax; c++) {
+      const double target = c + uniform2(seed, (uint32_t)c, 0xFFFFFFFFu, gen, 1u).x;
+      if (lo > 0 && !(cprev < target)) continue;
+      int i = lo;
+      while (i < hi && b.csum[i] < target) i++;
+      if (i == hi) {
+        if (hi != nw) continue;
+        i = nw - 1;
+      }
+      b.mult[i] += 1;
     }
-    if (a0 >= nw) a0 = nw - 1;
-    atomicAdd(&b.mult[a0], 1);
   }
   __syncthreads();
   // slots left empty take the surplus copies in order of source slot
@@ -462,11 +474,9 @@ __global__ void __launch_bounds__(kBranchThreads) branch_kernel(int nw, double *
     zc += mu == 0;
     ec += mu > 1 ? mu - 1 : 0;
   }
-  ipart[tid] = zc;
-  ipart2[tid] = ec;
-  block_exclusive_scan_ipartials(ipart, nt);
-  block_exclusive_scan_ipartials(ipart2, nt);
-  int zr = ipart[tid], er = ipart2[tid];
+  int zr = block_exclusive_scan(zc, iws);
+  int er = block_exclusive_scan(ec, iws);
+  const int etot = iws[32];  // every thread's extras
   for (int i = lo; i < hi; i++) {
     int mu = b.mult[i];
     b.zrank[i] = zr;
@@ -475,15 +485,6 @@ __global__ void __launch_bounds__(kBranchThreads) branch_kernel(int nw, double *
     er += mu > 1 ? mu - 1 : 0;
   }
   __syncthreads();
-  int etot = ipart2[nt - 1];
-  {
-    // total extras = last exclusive partial + last segment's count
-    int lo2 = min(nw, (nt - 1) * seg), hi2 = min(nw, lo2 + seg);
-    for (int i = lo2; i < hi2; i++) {
-      int mu = b.mult[i];
-      etot += mu > 1 ? mu - 1 : 0;
-    }
-  }
   for (int j = lo; j < hi; j++) {
     int src = j;
     if (b.mult[j] == 0) {
