@@ -317,8 +317,17 @@ class Handle:
 
     def set_inversion(self, layout):
         """0: register-resident Gauss-Jordan over every warp (default); 1: one
-        warp per spin in shared memory."""
+        warp per spin in shared memory; 2: panel-blocked."""
         self._chk(self.lib.qmc2d_set_inversion(self.h, layout))
+
+    def set_pair_lanes(self, lanes):
+        """Lanes per particle of the pair passes: 4, 8 or 16 (0: the default, 8)."""
+        self._chk(self.lib.qmc2d_set_pair_lanes(self.h, lanes))
+
+    def get_pair_lanes(self):
+        v = ctypes.c_int()
+        self._chk(self.lib.qmc2d_get_pair_lanes(self.h, ctypes.byref(v)))
+        return v.value
 
     def get_launch(self):
         """(pair-kernel walker groups, staging, inversion layout) in force."""

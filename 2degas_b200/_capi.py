@@ -191,6 +191,8 @@ SIGNATURES = {
     "qmc2d_compute_properties_noalloc_status": (c_int, [c_int, c_void_p]),
     "qmc2d_vmc_single": (c_int, [c_void_p, c_int, c_double, c_int]),
     "qmc2d_set_inversion": (c_int, [c_void_p, c_int]),
+    "qmc2d_set_pair_lanes": (c_int, [c_void_p, c_int]),
+    "qmc2d_get_pair_lanes": (c_int, [c_void_p, PI]),
     "qmc2d_rmc_set_launch": (c_int, [c_void_p, c_int]),
     "qmc2d_get_launch": (c_int, [c_void_p, PI, PI, PI]),
     "qmc2d_dmc_weights": (c_int, [c_void_p, c_int, c_double, c_double, c_double, c_int, PD]),

@@ -404,6 +404,21 @@ extern "C" int qmc2d_set_launch(qmc2d_handle *h, int groups, int stage) {
   return QMC2D_OK;
 }
 
+extern "C" int qmc2d_set_pair_lanes(qmc2d_handle *h, int lanes) {
+  if (!h || (lanes != 0 && lanes != 4 && lanes != 8 && lanes != 16)) {
+    q2d::set_error("qmc2d_set_pair_lanes: lanes must be 0 (the default), 4, 8 or 16");
+    return QMC2D_ERR_ARG;
+  }
+  h->hs.tune_lanes = lanes;  // host-side launch choice (the kernel is templated on it)
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_get_pair_lanes(qmc2d_handle *h, int *lanes) {
+  if (!h || !lanes) return QMC2D_ERR_ARG;
+  *lanes = h->hs.tune_lanes == 4 || h->hs.tune_lanes == 16 ? h->hs.tune_lanes : 8;
+  return QMC2D_OK;
+}
+
 extern "C" int qmc2d_set_inversion(qmc2d_handle *h, int layout) {
   if (!h || layout < 0 || layout > 2) {
     q2d::set_error("qmc2d_set_inversion: bad argument");
@@ -441,6 +456,7 @@ extern "C" int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *
   CK(cudaEventCreate(&e1));
   double best = 1e300;
   int bg = 2, bs = 0;
+  h->hs.tune_lanes = 8;  // the groups and staging are compared at the default lanes
   for (const auto &v : var) {
     h->hs.tune_groups = v[0];
     h->hs.tune_stage = v[1];
@@ -459,6 +475,28 @@ extern "C" int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *
   }
   h->hs.tune_groups = bg;
   h->hs.tune_stage = bs;
+  // lanes per particle of the pair passes, with the chosen groups and staging
+  // (8 first: the other two must beat it)
+  {
+    const int lanes[3] = {8, 4, 16};
+    int bl = 8;
+    for (int l : lanes) {
+      h->hs.tune_lanes = l;
+      CK(q2d::launch_pairs(h->hs, h->ds, h->pop[h->cur], a, h->stream));  // warm-up
+      CK(cudaEventRecord(e0, h->stream));
+      for (int r = 0; r < 3; r++)
+        CK(q2d::launch_pairs(h->hs, h->ds, h->pop[h->cur], a, h->stream));
+      CK(cudaEventRecord(e1, h->stream));
+      CK(cudaEventSynchronize(e1));
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, e0, e1));
+      if (l == 8 || t / 3.0 < best) {
+        best = t / 3.0;
+        bl = l;
+      }
+    }
+    h->hs.tune_lanes = bl;
+  }
   // inversion layout of the determinant section, timed on the evaluation
   // kernel over the population's configurations (into the staging buffers;
   // the population is not changed)

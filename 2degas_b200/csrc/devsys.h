@@ -54,10 +54,14 @@ struct DevSys {
   // groups per CTA (0: the default, 2) and the staging of the pair rows in
   // shared memory (0: when they fit, 1: never).
   int tune_groups, tune_stage;
+  // Lanes per particle in the pair kernel's two passes (qmc2d_set_pair_lanes,
+  // also timed by qmc2d_autotune): 4, 8 or 16 (0: the default, 8).
+  int tune_lanes;
   // Inversion layout of the determinant section (qmc2d_set_inversion):
   // 0 the register-resident Gauss-Jordan over every warp (4 warps per
   // spin, one CTA barrier per pivot step); 1 one warp per spin in shared
-  // memory (warp-synchronous steps) with rho_k on the other warps.
+  // memory (warp-synchronous steps) with rho_k on the other warps; 2 the
+  // panel-blocked form (one-warp panels of eight pivot steps).
   int tune_inv;
   // Every backflow table identically zero (set by the handle): q = x and the
   // backflow Jacobian is the identity, so the pair passes skip the backflow

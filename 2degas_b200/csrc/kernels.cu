@@ -143,8 +143,10 @@ size_t move_smem_bytes(const DevSys &s) {
 // 512-thread CTA per SM; G = 1: up to two 256-thread CTAs).
 
 //
-// R is the precision of the u2 and v2 pair terms (qmc2d_set_precision).
-template <class R, int G>
+// R is the precision of the u2 and v2 pair terms (qmc2d_set_precision), LG
+// the lanes per particle of the pair passes (4, 8 or 16: a launch choice,
+// DevSys::tune_lanes).
+template <class R, int G, int LG>
 __global__ void __launch_bounds__(G * kThreads, 2 / G) pairs_kernel(const DevSys *sp, DevPop pop,
                                                                     MoveArgs a, int stage_rows) {
   constexpr int kPairGroups = G, kPairThreads = G * kThreads;
@@ -190,10 +192,11 @@ __global__ void __launch_bounds__(G * kThreads, 2 / G) pairs_kernel(const DevSys
     double *o = a.scr + (size_t)w * L.stride;
     double *pout = S.has_bf ? o + L.pair : nullptr;
     if (stage_rows)
-      eval_pairs<kThreads, true>(S, m, tph, pout, (const R *)rows_s, sync, tid);
+      eval_pairs<kThreads, true, R, GroupSync, LG>(S, m, tph, pout, (const R *)rows_s, sync,
+                                                   tid);
     else
-      eval_pairs<kThreads, false>(S, m, tph, pout, rows_g, sync, tid);
-    compute_rhok(S, m, tid, kThreads);
+      eval_pairs<kThreads, false, R, GroupSync, LG>(S, m, tph, pout, rows_g, sync, tid);
+    compute_rhok<LG>(S, m, tid, kThreads);
     sync();
     for (int j = tid; j < 4 * S.nk; j += kThreads) o[L.rhok + j] = m.rhok[j];
     for (int j = tid; j < N2; j += kThreads) {
@@ -602,10 +605,10 @@ cudaError_t launch_eval(const DevSys &hs, const DevSys *ds, int nw, const double
   return cudaGetLastError();
 }
 
-template <class R, int G>
+template <class R, int G, int LG>
 static cudaError_t launch_pairs_t(const DevSys &hs, const DevSys *ds, DevPop pop,
                                   const MoveArgs &a, cudaStream_t st, int nsm, int optin) {
-  const void *k = (const void *)pairs_kernel<R, G>;
+  const void *k = (const void *)pairs_kernel<R, G, LG>;
   const size_t carve = G * ((pair_carve(hs, nullptr, nullptr, kThreads) + 127) & ~size_t(127));
   const size_t rows =
       sizeof(R) * RowLayout<R>::sstride * (size_t)hs.cmb_nblk * (hs.cmb_ng + 1);
@@ -622,8 +625,25 @@ static cudaError_t launch_pairs_t(const DevSys &hs, const DevSys *ds, DevPop pop
   const int need = (a.nw + G - 1) / G;
   const int cap = nsm * (per_sm > 0 ? per_sm : 1);
   const int grid = need < cap ? need : cap;
-  pairs_kernel<R, G><<<grid, G * kThreads, sm, st>>>(ds, pop, a, stage);
+  pairs_kernel<R, G, LG><<<grid, G * kThreads, sm, st>>>(ds, pop, a, stage);
   return cudaGetLastError();
+}
+
+template <class R, int LG>
+static cudaError_t launch_pairs_g(const DevSys &hs, const DevSys *ds, DevPop pop,
+                                  const MoveArgs &a, cudaStream_t st, int nsm, int optin) {
+  return hs.tune_groups == 1 ? launch_pairs_t<R, 1, LG>(hs, ds, pop, a, st, nsm, optin)
+                             : launch_pairs_t<R, 2, LG>(hs, ds, pop, a, st, nsm, optin);
+}
+
+template <class R>
+static cudaError_t launch_pairs_r(const DevSys &hs, const DevSys *ds, DevPop pop,
+                                  const MoveArgs &a, cudaStream_t st, int nsm, int optin) {
+  switch (hs.tune_lanes) {
+    case 4: return launch_pairs_g<R, 4>(hs, ds, pop, a, st, nsm, optin);
+    case 16: return launch_pairs_g<R, 16>(hs, ds, pop, a, st, nsm, optin);
+    default: return launch_pairs_g<R, 8>(hs, ds, pop, a, st, nsm, optin);
+  }
 }
 
 cudaError_t launch_pairs(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
@@ -637,12 +657,8 @@ cudaError_t launch_pairs(const DevSys &hs, const DevSys *ds, DevPop pop, const M
   if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) !=
       cudaSuccess)
     return e;
-  const bool one = hs.tune_groups == 1;
-  if (hs.pair_f32)
-    return one ? launch_pairs_t<float, 1>(hs, ds, pop, a, st, nsm, optin)
-               : launch_pairs_t<float, 2>(hs, ds, pop, a, st, nsm, optin);
-  return one ? launch_pairs_t<double, 1>(hs, ds, pop, a, st, nsm, optin)
-             : launch_pairs_t<double, 2>(hs, ds, pop, a, st, nsm, optin);
+  return hs.pair_f32 ? launch_pairs_r<float>(hs, ds, pop, a, st, nsm, optin)
+                     : launch_pairs_r<double>(hs, ds, pop, a, st, nsm, optin);
 }
 
 cudaError_t launch_move(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,

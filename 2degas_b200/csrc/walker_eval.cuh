@@ -5,9 +5,10 @@
 // shared memory.
 //
 // Layout and parallel decomposition
-//   * pair sums: 8 threads per particle i sweep j != i (each unordered pair
+//   * pair sums: LG threads per particle i sweep j != i (each unordered pair
 //     is visited from both ends, so per-particle sums need no atomics); the
-//     8 partial sums meet by warp shuffles in a fixed order.
+//     LG partial sums meet by warp shuffles in a fixed order. LG is 8, or 4
+//     or 16 as a launch choice of the pair kernel.
 //   * u3 (l=1 factorised triplets): with G_i = -sum_j xi(r_ij) r_ij and
 //     M_ij = xi I + (xi'/r) r r^T, the gradient of -1/2 sum|G|^2 on k is
 //     sum_j M_kj (G_k - G_j) and its Laplacian is
@@ -511,7 +512,6 @@ __device__ __forceinline__ void bf_offdiag(const DevSys &S, const double *x, int
   qby = -w2 * ry;
 }
 
-// Sum within aligned groups of 8 lanes; every lane of the warp must call it.
 // d += a b for one 8x8x4 FP64 tensor-core tile (warp-wide).
 __device__ __forceinline__ void dmma_m8n8k4(double (&d)[2], double a, double b) {
   asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -519,12 +519,15 @@ __device__ __forceinline__ void dmma_m8n8k4(double (&d)[2], double a, double b) 
       : "d"(a), "d"(b));
 }
 
-__device__ __forceinline__ double group8_sum(double v) {
-  v += __shfl_xor_sync(0xffffffffu, v, 4);
-  v += __shfl_xor_sync(0xffffffffu, v, 2);
-  v += __shfl_xor_sync(0xffffffffu, v, 1);
+// Sum over an aligned group of L lanes (L a power of two) in a fixed
+// order; every lane of the warp must call it.
+template <int L>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+__device__ __forceinline__ double group8_sum(double v) { return group_sum<8>(v); }
 
 // Deterministic block sum of K values at once; results valid in every
 // thread. Uses red[0 .. K*8).
@@ -1174,18 +1177,19 @@ __device__ inline void gj_invert_reg(double2 *W, int ld, int n, int *perm, doubl
 // rho_k per rhok slot (distances, reptation.f:4225-4243) by threads
 // t0 .. t0+nthr-1.
 // nthr is a multiple of 32 (whole warps): each (type, k) item is summed by
-// a group of 8 lanes, lane l taking particles l, l+8, ..., then a fixed
-// shuffle tree.
+// a group of LG lanes (8, or the pair kernel's lanes per particle), lane l
+// taking particles l, l+LG, ..., then a fixed shuffle tree.
+template <int LG = kGroup>
 __device__ inline void compute_rhok(const DevSys &S, const EvalSmem &m, int t, int nthr) {
-  const int total = S.nt * S.nk, per_round = nthr / kGroup, l8 = t & (kGroup - 1);
+  const int total = S.nt * S.nk, per_round = nthr / LG, l8 = t & (LG - 1);
   for (int e0 = 0; e0 < total; e0 += per_round) {
-    const int e = e0 + t / kGroup;
+    const int e = e0 + t / LG;
     const int ty = e < total ? e / S.nk : 0, k = e - ty * S.nk;
     const bool on = e < total && S.irhok[ty] != 0;
     double c = 0.0, sn = 0.0;
     if (on) {
       const double kx = __ldg(S.kvec + 2 * k), ky = __ldg(S.kvec + 2 * k + 1);
-      for (int i = S.ipfrst[ty] + l8; i < S.ipfrst[ty] + S.np[ty]; i += kGroup) {
+      for (int i = S.ipfrst[ty] + l8; i < S.ipfrst[ty] + S.np[ty]; i += LG) {
         double kr = kx * m.x[2 * i] + ky * m.x[2 * i + 1];
         double sv, cv;
         sincos(kr, &sv, &cv);
@@ -1193,8 +1197,8 @@ __device__ inline void compute_rhok(const DevSys &S, const EvalSmem &m, int t, i
         sn += sv;
       }
     }
-    c = group8_sum(c);
-    sn = group8_sum(sn);
+    c = group_sum<LG>(c);
+    sn = group_sum<LG>(sn);
     if (on && l8 == 0) {
       const int slot = S.irhok[ty] - 1;
       m.rhok[2 * (slot * S.nk + k)] = c;
@@ -1224,14 +1228,14 @@ __device__ inline void compute_rhok(const DevSys &S, const EvalSmem &m, int t, i
 // distance to the nearest node.
 // Sync is the barrier of the NT threads (the CTA, or a named-barrier group
 // of a CTA that runs several walkers); tid is the thread's index among them.
-template <int NT, bool kSh, class R = double, class Sync = CtaSync>
+template <int NT, bool kSh, class R = double, class Sync = CtaSync, int LG = kGroup>
 __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long &tph,
                                   double *pout, const R *rows, Sync sync = Sync(),
                                   int tid = threadIdx.x) {
   using Lay = RowLayout<R>;
   const int N = S.N;
-  const int lane8 = tid & (kGroup - 1);
-  const int per_round = NT / kGroup;
+  const int lane8 = tid & (LG - 1);
+  const int per_round = NT / LG;
   const size_t NN = (size_t)N * N;
   constexpr int RS = kSh ? Lay::sstride : Lay::gstride;
   constexpr bool kF64 = sizeof(R) == 8;
@@ -1240,7 +1244,7 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
   // ---- pass A: pair sums of u2, the pair part of u3, u3 G vectors and S,
   // backflow displacement, Jacobian diagonal and Laplacian, pair potential.
   for (int base = 0; base < N; base += per_round) {
-    int i = base + tid / kGroup;
+    int i = base + tid / LG;
     bool valid = i < N;
     int ti = valid ? type_of(S, i) : 0;
     PairSum<R> ltf, gx, gy, lap, vp;
@@ -1248,7 +1252,7 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
     PairSum<double> Gx, Gy, s3xx, s3xy, s3yy;
     PairSum<double> qx, qy, sbxx, sbxy, sbyy, qbx, qby;
     if (valid) {
-      for (int j = lane8; j < N; j += kGroup) {
+      for (int j = lane8; j < N; j += LG) {
         if (j == i) continue;
         int tj = type_of(S, j);
         R rx, ry, r, byr, rem;
@@ -1331,28 +1335,28 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
       gy_v += gy3.value();
       lap_v += lap3.value();
     }
-    const double ltf_s = group8_sum(ltf_v);
-    const double gx_s = group8_sum(gx_v);
-    const double gy_s = group8_sum(gy_v);
-    const double lap_s = group8_sum(lap_v);
-    const double vp_s = group8_sum(vp.value());
+    const double ltf_s = group_sum<LG>(ltf_v);
+    const double gx_s = group_sum<LG>(gx_v);
+    const double gy_s = group_sum<LG>(gy_v);
+    const double lap_s = group_sum<LG>(lap_v);
+    const double vp_s = group_sum<LG>(vp.value());
     double Gx_s = 0, Gy_s = 0, s3xx_s = 0, s3xy_s = 0, s3yy_s = 0;
     if (S.has_u3) {
-      Gx_s = group8_sum(Gx.value());
-      Gy_s = group8_sum(Gy.value());
-      s3xx_s = group8_sum(s3xx.value());
-      s3xy_s = group8_sum(s3xy.value());
-      s3yy_s = group8_sum(s3yy.value());
+      Gx_s = group_sum<LG>(Gx.value());
+      Gy_s = group_sum<LG>(Gy.value());
+      s3xx_s = group_sum<LG>(s3xx.value());
+      s3xy_s = group_sum<LG>(s3xy.value());
+      s3yy_s = group_sum<LG>(s3yy.value());
     }
     double qx_s = 0, qy_s = 0, sbxx_s = 0, sbxy_s = 0, sbyy_s = 0, qbx_s = 0, qby_s = 0;
     if (S.has_bf) {
-      qx_s = group8_sum(qx.value());
-      qy_s = group8_sum(qy.value());
-      sbxx_s = group8_sum(sbxx.value());
-      sbxy_s = group8_sum(sbxy.value());
-      sbyy_s = group8_sum(sbyy.value());
-      qbx_s = group8_sum(qbx.value());
-      qby_s = group8_sum(qby.value());
+      qx_s = group_sum<LG>(qx.value());
+      qy_s = group_sum<LG>(qy.value());
+      sbxx_s = group_sum<LG>(sbxx.value());
+      sbxy_s = group_sum<LG>(sbxy.value());
+      sbyy_s = group_sum<LG>(sbyy.value());
+      qbx_s = group_sum<LG>(qbx.value());
+      qby_s = group_sum<LG>(qby.value());
     }
     if (valid && lane8 == 0) {
       m.ltf[i] = ltf_s;
@@ -1387,13 +1391,13 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
   // ---- pass B: u3 gradient and Laplacian from the G vectors (FP64).
   if (S.has_u3) {
     for (int base = 0; base < N; base += per_round) {
-      int k = base + tid / kGroup;
+      int k = base + tid / LG;
       bool valid = k < N;
       int tk = valid ? type_of(S, k) : 0;
       double gx = 0, gy = 0, lap = 0;
       double Gkx = valid ? m.G3[2 * k] : 0.0, Gky = valid ? m.G3[2 * k + 1] : 0.0;
       if (valid) {
-        for (int j = lane8; j < N; j += kGroup) {
+        for (int j = lane8; j < N; j += LG) {
           if (j == k) continue;
           int tj = type_of(S, j);
           double rx, ry, r, byr, rem;
@@ -1412,9 +1416,9 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
           lap += w * (rx * dGx + ry * dGy) - (mxx * mxx + 2.0 * mxy * mxy + myy * myy);
         }
       }
-      gx = group8_sum(gx);
-      gy = group8_sum(gy);
-      lap = group8_sum(lap);
+      gx = group_sum<LG>(gx);
+      gy = group_sum<LG>(gy);
+      lap = group_sum<LG>(lap);
       if (valid && lane8 == 0) {
         double sxx = m.S3[3 * k], sxy = m.S3[3 * k + 1], syy = m.S3[3 * k + 2];
         m.g[2 * k] += gx;

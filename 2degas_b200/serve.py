@@ -147,10 +147,12 @@ def run_request(p, device=0):
             c0 = c1
             dv *= min(2.0, max(0.3, acc / 0.5))
         h.autotune()  # the pair kernel's launch choice for this population
-        # the inversion layouts agree only to round-off, and the autotuner's
-        # pick depends on timing, which the mix changes: keep the default so a
-        # request's result does not depend on what else runs
+        # the inversion layouts and the pair lanes agree only to round-off,
+        # and the autotuner's pick depends on timing, which the mix changes:
+        # keep the defaults so a request's result does not depend on what
+        # else runs
         h.set_inversion(0)
+        h.set_pair_lanes(0)
         # DMC at a tenth of the VMC step (acceptance near 97%)
         tau = req.tau or (dv / 10.0 if req.method == "dmc" else dv)
         if req.method == "dmc":

@@ -364,6 +364,8 @@ def b200_arm(args, rank, world, local_rank):
     tuned = h.autotune()  # launch choices, timed on this population
     if args.inversion is not None:  # a fixed inversion layout instead of the tuner's
         h.set_inversion(args.inversion)
+    if args.pair_lanes is not None:  # fixed lanes per particle instead of the tuner's
+        h.set_pair_lanes(args.pair_lanes)
     h.block_reset()
     h.vmc(10, delta, 10 ** 9)
     blk, norm = h.block_get()
@@ -492,6 +494,7 @@ def b200_arm(args, rank, world, local_rank):
             "data": "synthetic",
             "config": config,
             "pair_launch": {"groups": tuned[0], "stage_rows": tuned[1] == 0,
+                            "lanes_per_particle": h.get_pair_lanes(),
                             "inversion_layout": h.get_launch()[2]},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -1106,9 +1109,10 @@ def batch_arm(args, rank, world):
         "handle_by_handle": {"value": moves / t_seq, "seconds": t_seq},
         "speedup_vs_handle_by_handle": t_seq / t_batch,
         # each population's autotuned launch: (pair-kernel walker groups,
-        # rows not staged, inversion layout) -> populations
+        # rows not staged, inversion layout, lanes per particle) -> populations
         "launch_choices": {str(k): v for k, v in sorted(
-            __import__("collections").Counter(tuple(h.get_launch()) for h in handles).items())},
+            __import__("collections").Counter(tuple(h.get_launch()) + (h.get_pair_lanes(),)
+                                              for h in handles).items())},
         "clocks": clk.summary(),
     }
     b.close()
@@ -1143,6 +1147,8 @@ def main():
                          "(default: independent populations per rank)")
     ap.add_argument("--inversion", type=int, default=None, choices=[0, 1, 2],
                     help="determinant inversion layout (qmc2d_set_inversion)")
+    ap.add_argument("--pair-lanes", type=int, default=None, choices=[4, 8, 16],
+                    help="lanes per particle of the pair passes (qmc2d_set_pair_lanes)")
     ap.add_argument("--single", action="store_true",
                     help="vmc workload with single-electron moves and Sherman-Morrison updates")
     ap.add_argument("--rmc-split", type=int, default=None, choices=[0, 1],

@@ -237,7 +237,15 @@ int qmc2d_set_launch(qmc2d_handle *h, int groups, int stage);
  * unused row of largest |re|+|im|, reptation.f:9079-9227) and give the same
  * values up to round-off. The reference has no counterpart. */
 int qmc2d_set_inversion(qmc2d_handle *h, int layout);
-/* qmc2d_autotune also times the two inversion layouts on the evaluation
+/* Lanes per particle in the pair kernel's two pair passes: 4, 8 or 16
+ * (0: the default, 8). Each particle's sums over its partners are split
+ * over that many lanes and meet in a fixed shuffle order, so a choice
+ * other than 8 changes the sums' rounding (round-off only). qmc2d_autotune
+ * times the three after the groups and staging; qmc2d_get_pair_lanes
+ * reports the choice in force. */
+int qmc2d_set_pair_lanes(qmc2d_handle *h, int lanes);
+int qmc2d_get_pair_lanes(qmc2d_handle *h, int *lanes);
+/* qmc2d_autotune also times the three inversion layouts on the evaluation
  * kernel over the population's configurations (three launches each into the
  * handle's staging buffers; the population is not changed) and keeps the
  * faster; *ms is the chosen pair-kernel time per launch. */
