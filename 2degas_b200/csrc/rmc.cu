@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_move_kernel(const DevSys *sp,
 // and, after the reptile's last growth of the move, the path tail. A move
 // of mdelta > 1 takes mdelta launch pairs; a reptile whose move has fewer
 // growths skips the later ones.
-template <class R, int G>
+template <class R, int G, int LG>
 __global__ void __launch_bounds__(G * kThreads, 2 / G) rmc_pairs_kernel(const DevSys *sp,
                                                                         RmcArgs a, double *scr,
                                                                         int idelta,
@@ -585,10 +585,11 @@ __global__ void __launch_bounds__(G * kThreads, 2 / G) rmc_pairs_kernel(const De
     double *o = scr + (size_t)r * L.stride;
     double *pout = (S.has_bf && !S.bf_zero) ? o + L.pair : nullptr;
     if (stage_rows)
-      eval_pairs<kThreads, true>(S, m, tph, pout, (const R *)rows_s, sync, tid);
+      eval_pairs<kThreads, true, R, GroupSync, LG>(S, m, tph, pout, (const R *)rows_s, sync,
+                                                   tid);
     else
-      eval_pairs<kThreads, false>(S, m, tph, pout, rows_g, sync, tid);
-    compute_rhok(S, m, tid, kThreads);
+      eval_pairs<kThreads, false, R, GroupSync, LG>(S, m, tph, pout, rows_g, sync, tid);
+    compute_rhok<LG>(S, m, tid, kThreads);
     sync();
     for (int e = tid; e < 4 * S.nk; e += kThreads) o[L.rhok + e] = m.rhok[e];
     for (int e = tid; e < N2; e += kThreads) {
@@ -969,10 +970,10 @@ extern "C" int qmc2d_rmc_init(qmc2d_handle *h, int nrep, const qmc2d_rmc_params 
   return q2d_sync_status(h, nrep);
 }
 
-template <int G>
-static cudaError_t launch_rmc_pairs(const q2d::DevSys &hs, const q2d::DevSys *ds,
-                                    const q2d::RmcArgs &a, double *scr, int idelta,
-                                    cudaStream_t st) {
+template <int G, int LG>
+static cudaError_t launch_rmc_pairs_t(const q2d::DevSys &hs, const q2d::DevSys *ds,
+                                      const q2d::RmcArgs &a, double *scr, int idelta,
+                                      cudaStream_t st) {
   int dev = 0, nsm = 0, optin = 0;
   cudaError_t e;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
@@ -981,7 +982,7 @@ static cudaError_t launch_rmc_pairs(const q2d::DevSys &hs, const q2d::DevSys *ds
   if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) !=
       cudaSuccess)
     return e;
-  const void *k = (const void *)q2d::rmc_pairs_kernel<double, G>;
+  const void *k = (const void *)q2d::rmc_pairs_kernel<double, G, LG>;
   const size_t carve =
       G * ((q2d::pair_carve(hs, nullptr, nullptr, q2d::kThreads) + 127) & ~size_t(127));
   const size_t rows = sizeof(double) * q2d::RowLayout<double>::sstride * (size_t)hs.cmb_nblk *
@@ -995,9 +996,21 @@ static cudaError_t launch_rmc_pairs(const q2d::DevSys &hs, const q2d::DevSys *ds
                                                                    sm)) != cudaSuccess)
     return e;
   const int need = (a.nrep + G - 1) / G, cap = nsm * (per_sm > 0 ? per_sm : 1);
-  q2d::rmc_pairs_kernel<double, G>
+  q2d::rmc_pairs_kernel<double, G, LG>
       <<<need < cap ? need : cap, G * q2d::kThreads, sm, st>>>(ds, a, scr, idelta, stage);
   return cudaGetLastError();
+}
+
+// the lanes per particle in force (DevSys::tune_lanes, as the DMC pair kernel)
+template <int G>
+static cudaError_t launch_rmc_pairs(const q2d::DevSys &hs, const q2d::DevSys *ds,
+                                    const q2d::RmcArgs &a, double *scr, int idelta,
+                                    cudaStream_t st) {
+  switch (hs.tune_lanes) {
+    case 4: return launch_rmc_pairs_t<G, 4>(hs, ds, a, scr, idelta, st);
+    case 16: return launch_rmc_pairs_t<G, 16>(hs, ds, a, scr, idelta, st);
+    default: return launch_rmc_pairs_t<G, 8>(hs, ds, a, scr, idelta, st);
+  }
 }
 
 extern "C" int qmc2d_rmc(qmc2d_handle *h, int nstp) {

@@ -678,11 +678,16 @@ def config_arm(args, rank, world, local_rank):
         h.population_set(x0)
         h.vmc(args.equil, 0.045 * rs * rs, 10 ** 9)  # seeded VMC start configurations
         x1 = h.population_get()["x"]
+        # the pair kernel's launch choices (groups, staging, lanes), timed on
+        # the start configurations; the reptation pair kernel uses them too
+        h.autotune()
+        if args.pair_lanes is not None:
+            h.set_pair_lanes(args.pair_lanes)
         if args.rmc_split is not None:
             h.rmc_set_launch(args.rmc_split)
         h.rmc_init(nw, rmc_start_paths(x1, ntau, delta, rs, walker_seed & 0xFFFF), ntau, 1, 1,
                    delta, etrial, 10 ** 9, mage_r)
-        tuned = None
+        tuned = h.get_launch()
 
         def step():
             h.rmc(1)
@@ -787,8 +792,8 @@ def config_arm(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config,
-            "pair_launch": ({"groups": tuned[0], "stage_rows": tuned[1] == 0}
-                            if tuned else None),
+            "pair_launch": ({"groups": tuned[0], "stage_rows": tuned[1] == 0,
+                             "lanes_per_particle": h.get_pair_lanes()} if tuned else None),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,

@@ -65,7 +65,8 @@ def test_vmc_forced_moves(q, oracle_cls, n26, n26_configs):
     assert rel(got["x"], pop["x"]) < 1e-11
 
 
-def test_dmc_generations(q, oracle_cls, n26, n26_configs):
+@pytest.mark.parametrize("lanes", [8, 4, 16])
+def test_dmc_generations(q, oracle_cls, n26, n26_configs, lanes):
     nw, ngen, mmstep, delta = 32, 3, 2, 0.05
     etrial, mmult, mage = -0.43, 5.0, 1000
     x0 = n26_configs[:nw]
@@ -73,6 +74,7 @@ def test_dmc_generations(q, oracle_cls, n26, n26_configs):
     pop = o.population_init(x0)
     blk_o, norm_o, _ = o.dmc_philox(pop, ngen, mmstep, delta, etrial, mmult, mage, SEED)
     with q.Handle(n26, capacity=nw, seed=SEED) as h:
+        h.set_pair_lanes(lanes)  # lanes per particle of the pair passes
         h.population_set(x0)
         h.block_reset()
         h.dmc(ngen, mmstep, delta, etrial, mmult, mage)
@@ -84,8 +86,8 @@ def test_dmc_generations(q, oracle_cls, n26, n26_configs):
     assert rel(blk[:14], blk_o[:14]) < 1e-9
 
 
-@pytest.mark.parametrize("split", [1, 0])
-def test_reptation_moves(q, oracle_cls, n26, n26_configs, split):
+@pytest.mark.parametrize("split,lanes", [(1, 8), (0, 8), (1, 4), (1, 16)])
+def test_reptation_moves(q, oracle_cls, n26, n26_configs, split, lanes):
     from ctypes import c_double, c_int  # noqa: F401
 
     import importlib
@@ -105,6 +107,7 @@ def test_reptation_moves(q, oracle_cls, n26, n26_configs, split):
         paths.append(rep.path())
     with q.Handle(n26, capacity=nrep, seed=SEED) as h:
         h.rmc_set_launch(split)
+        h.set_pair_lanes(lanes)
         h.rmc_init(nrep, x, ntau, 1, mdelta, 0.05, -0.43, 1000, 1000)
         h.block_reset()
         h.rmc(nstp)
