@@ -324,6 +324,16 @@ class Handle:
         """Lanes per particle of the pair passes: 4, 8 or 16 (0: the default, 8)."""
         self._chk(self.lib.qmc2d_set_pair_lanes(self.h, lanes))
 
+    def set_move_inversion(self, batched):
+        """1: orbitals and inversion in their own kernel before the move kernel
+        (default where it applies); 0: inside the move kernel."""
+        self._chk(self.lib.qmc2d_set_move_inversion(self.h, batched))
+
+    def get_move_inversion(self):
+        v = ctypes.c_int()
+        self._chk(self.lib.qmc2d_get_move_inversion(self.h, ctypes.byref(v)))
+        return v.value
+
     def get_pair_lanes(self):
         v = ctypes.c_int()
         self._chk(self.lib.qmc2d_get_pair_lanes(self.h, ctypes.byref(v)))

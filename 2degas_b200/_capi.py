@@ -34,7 +34,7 @@ ERR_STACK = 11
 
 # kernels for qmc2d_profile_get
 (KERNEL_MOVE, KERNEL_BRANCH, KERNEL_GATHER, KERNEL_EVAL, KERNEL_RMC, KERNEL_PAIRS,
- KERNEL_SINGLE) = range(7)
+ KERNEL_SINGLE, KERNEL_ORB_INV) = range(8)
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 
 # property indices (0-based; reptation.f:577-637)
@@ -192,6 +192,8 @@ SIGNATURES = {
     "qmc2d_vmc_single": (c_int, [c_void_p, c_int, c_double, c_int]),
     "qmc2d_set_inversion": (c_int, [c_void_p, c_int]),
     "qmc2d_set_pair_lanes": (c_int, [c_void_p, c_int]),
+    "qmc2d_set_move_inversion": (c_int, [c_void_p, c_int]),
+    "qmc2d_get_move_inversion": (c_int, [c_void_p, PI]),
     "qmc2d_get_pair_lanes": (c_int, [c_void_p, PI]),
     "qmc2d_rmc_set_launch": (c_int, [c_void_p, c_int]),
     "qmc2d_get_launch": (c_int, [c_void_p, PI, PI, PI]),

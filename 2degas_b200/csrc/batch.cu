@@ -102,6 +102,7 @@ cudaError_t enqueue(qmc2d_batch *b, int k, int g0, int ngen, int dmc, double del
     a.status = h->d_status;
     a.ctr = ctr;
     if ((e = q2d::launch_pairs(h->hs, h->ds, h->pop[cur], a, st)) != cudaSuccess) return e;
+    if ((e = q2d::launch_orb_inv(h->hs, h->ds, a, st)) != cudaSuccess) return e;
     if ((e = q2d::launch_move(h->hs, h->ds, h->pop[cur], a, st)) != cudaSuccess) return e;
     if (dmc) {
       if ((e = q2d::launch_branch(h->nw, h->d_wate, h->seed, (uint32_t)(g0 + g), h->br, st,

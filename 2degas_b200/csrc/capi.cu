@@ -292,6 +292,7 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
     q2d::set_error(buf);
     return fail(QMC2D_ERR_LIMIT);
   }
+  h->hs.split_inv = 1;  // moves take orb_inv_kernel where the scratch has its region
   if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking)) != cudaSuccess)
     return fail(cuda_fail(e, "cudaStreamCreate"));
@@ -416,6 +417,25 @@ extern "C" int qmc2d_set_pair_lanes(qmc2d_handle *h, int lanes) {
 extern "C" int qmc2d_get_pair_lanes(qmc2d_handle *h, int *lanes) {
   if (!h || !lanes) return QMC2D_ERR_ARG;
   *lanes = h->hs.tune_lanes == 4 || h->hs.tune_lanes == 16 ? h->hs.tune_lanes : 8;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_set_move_inversion(qmc2d_handle *h, int batched) {
+  if (!h || batched < 0 || batched > 1) {
+    q2d::set_error("qmc2d_set_move_inversion: bad argument");
+    return QMC2D_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  CK(join_side(h));
+  h->hs.split_inv = batched;
+  CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_get_move_inversion(qmc2d_handle *h, int *batched) {
+  if (!h || !batched) return QMC2D_ERR_ARG;
+  *batched = q2d::orb_inv_applies(h->hs) ? 1 : 0;
   return QMC2D_OK;
 }
 
@@ -873,7 +893,11 @@ static int run_moves(qmc2d_handle *h, int nstp, int dmc, double delta, double et
       ProfScope ps(h, QMC2D_KERNEL_PAIRS, h->stream);
       CK(q2d::launch_pairs(h->hs, h->ds, h->pop[h->cur], a, h->stream));
     }
-    CK(join_side(h));  // the pair kernel reads only x and g
+    if (q2d::orb_inv_applies(h->hs)) {
+      ProfScope ps(h, QMC2D_KERNEL_ORB_INV, h->stream);
+      CK(q2d::launch_orb_inv(h->hs, h->ds, a, h->stream));
+    }
+    CK(join_side(h));  // the pair and inversion kernels read only x, g and the scratch
     {
       ProfScope ps(h, QMC2D_KERNEL_MOVE, h->stream);
       CK(q2d::launch_move(h->hs, h->ds, h->pop[h->cur], a, h->stream));

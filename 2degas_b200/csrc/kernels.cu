@@ -218,6 +218,132 @@ __global__ void __launch_bounds__(G * kThreads, 2 / G) pairs_kernel(const DevSys
 
 size_t move_scratch_doubles(const DevSys &hs) { return move_scratch(hs).stride; }
 
+// ------------------------------------------------- orbitals and inversion
+// orb_inv_kernel: for every (walker, spin) of a move, one warp forms the
+// plane-wave orbital matrix A(k, j) = exp(i g_k . q_j) of the proposed
+// backflow coordinates (paho_orbitals, reptation.f:10298-10315) and inverts
+// it by Gauss-Jordan with partial pivoting (zgefa/zgedi, reptation.f:9227,
+// 9338), lane k holding row k in registers: the pivot key is the top word
+// of |re|+|im| with 255 - row in its low byte (one redux per step), the
+// pivot row reaches the other lanes through shared memory, and every lane
+// updates its row, the next pivot column first. Outputs, as gj_invert_reg:
+// W(pi(k), c) = A^-1(k, pi(c)) with the pivot rows unscaled until the end,
+// perm, |pivot|^2 and the singular flag, into the walker's move scratch,
+// where move_kernel reads them instead of inverting. No block barrier after
+// the DevSys load: each warp works alone, many per scheduler, so one
+// matrix's pivot chain hides behind the others' updates.
+constexpr int kOrbWarps = 4;  // warps (spin matrices) per CTA
+
+__host__ __device__ inline size_t orb_inv_warp_doubles(int n) {
+  // the warp's tile of W (n x ws_ld(n) complex), q of its electrons, two pivot rows
+  return (size_t)2 * n * ws_ld(n) + 2 * (size_t)n + 4 * 32;
+}
+
+template <int NM>
+__global__ void __launch_bounds__(32 * kOrbWarps) orb_inv_kernel(const DevSys *sp, MoveArgs a) {
+  __shared__ DevSys S;
+  extern __shared__ __align__(16) char smem[];
+  load_sys(S, sp);
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5, nt = S.nt;
+  const int item = blockIdx.x * kOrbWarps + wl, w = item / nt, spn = item - w * nt;
+  if (w >= a.nw) return;  // whole warps; nothing below waits on other warps
+  const int n = S.np[spn], f0 = S.ipfrst[spn], ld = ws_ld(n), r = lane;
+  size_t wd = 0;
+  for (int t = 0; t < nt; t++) wd = max(wd, orb_inv_warp_doubles(S.np[t]));
+  double *base = reinterpret_cast<double *>(smem) + (size_t)wl * wd;
+  double2 *tile = reinterpret_cast<double2 *>(base);
+  double *qs = base + 2 * (size_t)n * ld;
+  double2 *prow = reinterpret_cast<double2 *>(qs + 2 * n);  // 2 x 32, double-buffered
+  const MoveScratch L = move_scratch(S);
+  double *o = a.scr + (size_t)w * L.stride;
+  size_t off = L.inv;
+  for (int t = 0; t < spn; t++) off += inv_spin_doubles(S.np[t]);
+  double2 *outA = reinterpret_cast<double2 *>(o + off);
+  double2 *outW = outA + (size_t)n * n;
+  double *outD = reinterpret_cast<double *>(outW + (size_t)n * ld);
+  double *outP = outD + n;
+  double *outS = outP + n;
+  for (int e = lane; e < 2 * n; e += 32) qs[e] = o[L.q + 2 * f0 + e];
+  __syncwarp();
+  // orbitals: lane r is orbital r
+  const double gx = r < n ? __ldg(S.gvec + 2 * r) : 0.0, gy = r < n ? __ldg(S.gvec + 2 * r + 1) : 0.0;
+  double2 v[NM];
+#pragma unroll
+  for (int j = 0; j < NM; j++) {
+    const bool on = r < n && j < n;
+    const double kr = on ? qs[2 * j] * gx + qs[2 * j + 1] * gy : 0.0;
+    double sv, cv;
+    sincos(kr, &sv, &cv);
+    v[j] = on ? make_double2(cv, sv) : make_double2(0.0, 0.0);
+  }
+  // A, column-major (A[k + j n]): for each j the lanes write consecutive k
+  if (r < n)
+#pragma unroll
+    for (int j = 0; j < NM; j++)
+      if (j < n) outA[r + (size_t)j * n] = v[j];
+  bool used = r >= n;
+  double2 my_inv = make_double2(1.0, 0.0);
+  int my_perm = 0, sing = 0;
+  double my_dk = 0.0;
+#pragma unroll
+  for (int k = 0; k < NM; k++) {
+    if (k >= n) break;
+    const double av = fabs(v[k].x) + fabs(v[k].y);
+    const unsigned key =
+        used ? 0u : ((unsigned)__double2hiint(av) & ~0xFFu) | (unsigned)(255 - r);
+    const unsigned best = __reduce_max_sync(0xffffffffu, key);
+    // Every unused row's key has 255 - r in its low byte, so p is an unused
+    // row < n at every step, an exactly zero or NaN column included.
+    const int p = 255 - (int)(best & 0xFFu);
+    sing |= (best >> 8) == 0u;  // every candidate zero (or subnormal)
+    double2 *pr = prow + (k & 1) * 32;
+    if (r == p)
+#pragma unroll
+      for (int c = 0; c < NM; c++) pr[c] = v[c];
+    __syncwarp();
+    const double2 piv = pr[k];
+    const double d = piv.x * piv.x + piv.y * piv.y;
+    const double rd = rcp_newton(d);
+    const double2 inv = make_double2(piv.x * rd, -piv.y * rd);
+    if (lane == k) {
+      my_perm = p;
+      my_dk = d;
+    }
+    const bool isp = r == p;
+    used = used || isp;
+    if (isp) my_inv = inv;
+    double2 fac = cmul(v[k], inv);
+    if (isp || r >= n) fac = make_double2(0.0, 0.0);
+    if (k + 1 < NM) {  // the next pivot column first
+      const double2 b = pr[k + 1];
+      v[k + 1].x = fma(-fac.x, b.x, fma(fac.y, b.y, v[k + 1].x));
+      v[k + 1].y = fma(-fac.x, b.y, fma(-fac.y, b.x, v[k + 1].y));
+    }
+#pragma unroll
+    for (int c = 0; c < NM; c++) {
+      if (c == k + 1) continue;
+      const double2 b = pr[c];
+      v[c].x = fma(-fac.x, b.x, fma(fac.y, b.y, v[c].x));
+      v[c].y = fma(-fac.x, b.y, fma(-fac.y, b.x, v[c].y));
+    }
+    v[k] = isp ? make_double2(1.0, 0.0) : make_double2(-fac.x, -fac.y);
+  }
+  // rows normalised by their own pivot, out through shared memory so the
+  // scratch writes are consecutive
+  if (r < n)
+#pragma unroll
+    for (int c = 0; c < NM; c++)
+      if (c < n) tile[(size_t)r * ld + c] = cmul(v[c], my_inv);
+  __syncwarp();
+  for (int e = lane; e < n * ld; e += 32) outW[e] = tile[e];
+  if (lane < n) {
+    outD[lane] = my_dk;
+    outP[lane] = (double)my_perm;
+  }
+  if (lane == 0) outS[0] = (double)sing;
+}
+
+
 template <bool kGmat>
 __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, DevPop pop,
                                                            MoveArgs a) {
@@ -233,20 +359,27 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
   const int N = S.N, N2 = 2 * N, np = S.nprops, nt = S.nt;
   const MoveScratch L = move_scratch(S);
   const double *o = a.scr + (size_t)w * L.stride;
-  if (S.has_bf && !S.bf_zero) {
-    // the pair values are read by the Jacobian build long after this point;
-    // by now the pair kernel's writes for this walker have left L2, so bring
-    // them back (bulk L2 prefetch, 32 KB per request; the block is 256-byte
-    // aligned and 3 N^2 doubles long, a multiple of 8 bytes: round down to
-    // 16 bytes and let the tail come with the loads)
-    const size_t bytes = (sizeof(double) * 3 * (size_t)N * N) & ~size_t(15);
-    const char *base = reinterpret_cast<const char *>(o + L.pair);
+  // the pair values are read by the Jacobian build long after this point,
+  // the orbitals and inverse of orb_inv_kernel at the start of the
+  // determinant section; by now the earlier kernels' writes for this walker
+  // have left L2, so bring them back (bulk L2 prefetch, 32 KB per request;
+  // both blocks start 16-byte aligned and are whole doubles long: round down
+  // to 16 bytes and let the tail come with the loads)
+  auto prefetch_l2 = [&](const double *p, size_t doubles) {
+    const size_t bytes = (sizeof(double) * doubles) & ~size_t(15);
+    const char *base = reinterpret_cast<const char *>(p);
     for (size_t b0 = (size_t)tid * 32768; b0 < bytes; b0 += (size_t)kThreads * 32768) {
       const unsigned sz = (unsigned)(bytes - b0 < 32768 ? bytes - b0 : 32768);
       asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + b0), "r"(sz)
                    : "memory");
     }
+  };
+  if (!kGmat && S.split_inv && L.inv) {
+    size_t nd = 0;
+    for (int t = 0; t < nt; t++) nd += inv_spin_doubles(S.np[t]);
+    prefetch_l2(o + L.inv, nd);
   }
+  if (S.has_bf && !S.bf_zero) prefetch_l2(o + L.pair, 3 * (size_t)N * N);
   for (int j = tid; j < N2; j += kThreads) {
     v.xo[j] = pop.x[(size_t)w * N2 + j];
     v.go[j] = pop.g[(size_t)w * N2 + j];
@@ -282,7 +415,7 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
   long long tph = clock64();
   double sn = 1.0;
   status |= eval_det<kGmat>(S, m, v.hn, v.pn, &v.sc[0], tph, S.has_bf ? o + L.pair : nullptr,
-                     o + L.rhok);
+                            o + L.rhok, !kGmat && S.split_inv && L.inv ? o + L.inv : nullptr);
   sn = v.sc[0];
   // reverse move (reptation.f:4660-4674)
   double wn = 0.0;
@@ -659,6 +792,24 @@ cudaError_t launch_pairs(const DevSys &hs, const DevSys *ds, DevPop pop, const M
     return e;
   return hs.pair_f32 ? launch_pairs_r<float>(hs, ds, pop, a, st, nsm, optin)
                      : launch_pairs_r<double>(hs, ds, pop, a, st, nsm, optin);
+}
+
+bool orb_inv_applies(const DevSys &hs) { return hs.split_inv && orb_inv_fits(hs); }
+
+cudaError_t launch_orb_inv(const DevSys &hs, const DevSys *ds, const MoveArgs &a,
+                           cudaStream_t st) {
+  if (a.nw <= 0 || !orb_inv_applies(hs)) return cudaSuccess;
+  size_t wd = 0;
+  for (int t = 0; t < hs.nt; t++) wd = std::max(wd, orb_inv_warp_doubles(hs.np[t]));
+  const size_t sm = sizeof(double) * wd * kOrbWarps;
+  const int items = a.nw * hs.nt, grid = (items + kOrbWarps - 1) / kOrbWarps;
+  // registers for the rows: 16, 29 (N = 58, the benchmark shell) or 32 columns
+  auto k = hs.nmax <= 16 ? orb_inv_kernel<16>
+                         : (hs.nmax <= 29 ? orb_inv_kernel<29> : orb_inv_kernel<32>);
+  cudaError_t e = set_smem((const void *)k, sm);
+  if (e != cudaSuccess) return e;
+  k<<<grid, 32 * kOrbWarps, sm, st>>>(ds, a);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_move(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,

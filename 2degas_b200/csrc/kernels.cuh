@@ -41,10 +41,16 @@ cudaError_t launch_eval(const DevSys &hs, const DevSys *ds, int nw, const double
                         double *hl, double *props, double *s, int *status, cudaStream_t st);
 
 // One move of a resident population: the proposal and pair passes into the
-// move scratch (launch_pairs), then the rest of the evaluation, the
-// acceptance and the averages (launch_move).
+// move scratch (launch_pairs), the orbitals and their inversion into the
+// move scratch when DevSys::split_inv applies (launch_orb_inv, otherwise
+// nothing), then the rest of the evaluation, the acceptance and the
+// averages (launch_move).
 cudaError_t launch_pairs(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
                          cudaStream_t st);
+cudaError_t launch_orb_inv(const DevSys &hs, const DevSys *ds, const MoveArgs &a,
+                           cudaStream_t st);
+// launch_orb_inv runs (DevSys::split_inv and a scratch region for it).
+bool orb_inv_applies(const DevSys &hs);
 cudaError_t launch_move(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
                         cudaStream_t st);
 // Doubles of move scratch per walker.

@@ -254,8 +254,22 @@ __host__ __device__ inline size_t pair_carve(const DevSys &s, char *base, EvalSm
 // the free-propagator sum (lng) of get_w_stack (reptation.f:1804-1851).
 struct MoveScratch {
   int x, g, q, sb, qbd, lap, ltf, vp, wold, dold, lng, rhok, pair;
+  size_t inv;  // orb_inv_kernel's output per spin (0: no such region)
   size_t stride;
 };
+// Doubles of one spin's block of orb_inv_kernel output (n orbitals): the
+// orbital matrix A (n x n complex, column-major as EvalSmem::A), the
+// inverse W (n x ws_ld(n) complex, as EvalSmem::W), |pivot|^2, the pivot
+// rows (as doubles) and the singular flag; even, so blocks stay 16-byte
+// aligned.
+__host__ __device__ inline size_t inv_spin_doubles(int n) {
+  return ((size_t)2 * n * n + (size_t)2 * n * ws_ld(n) + 2 * (size_t)n + 2 + 1) & ~size_t(1);
+}
+// The batched orbital-and-inversion kernel applies: backflow determinants in
+// shared memory, every spin at most 32 orbitals.
+__host__ __device__ inline bool orb_inv_fits(const DevSys &s) {
+  return s.has_bf && !s.gmat && s.nmax > 0 && s.nmax <= 32;
+}
 __host__ __device__ inline MoveScratch move_scratch(const DevSys &s) {
   const int N = s.N;
   MoveScratch l;
@@ -273,6 +287,12 @@ __host__ __device__ inline MoveScratch move_scratch(const DevSys &s) {
   l.rhok = 14 * N + 3;
   l.pair = (14 * N + 3 + 4 * (s.nk > 0 ? s.nk : 1) + 3) & ~3;
   size_t end = (size_t)l.pair + (s.has_bf ? 3 * (size_t)N * N : 0);
+  l.inv = 0;
+  if (orb_inv_fits(s)) {
+    end = (end + 1) & ~size_t(1);
+    l.inv = end;
+    for (int sp = 0; sp < s.nt; sp++) end += inv_spin_doubles(s.np[sp]);
+  }
   l.stride = (end + 31) & ~size_t(31);  // 256-byte aligned walker blocks
   return l;
 }
@@ -1435,11 +1455,13 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
 // Everything after the pair passes: determinants (orbitals, inversion,
 // F, drift, Laplacian with the cross term), rho_k, assembly. With pin, the
 // backflow Jacobian blocks take the pair spline values written by
-// eval_pairs(pout) instead of evaluating them again.
+// eval_pairs(pout) instead of evaluating them again; with inv_in, the
+// orbitals and their inversion come from orb_inv_kernel.
 template <bool kGmat = false>
 __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, double *props,
                                double *sign, long long &tph, const double *pin,
-                               const double *rhok_in = nullptr) {
+                               const double *rhok_in = nullptr,
+                               const double *inv_in = nullptr) {
   const int tid = threadIdx.x;
   // rho_k of both slots: copied when given (MoveScratch), else summed
   auto rhok = [&](int t0, int nthr) {
@@ -1457,93 +1479,121 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
   double logdet_sum = 0.0, ltf_j = 0.0;  // ltf_j: sum of the Jastrow -ln psi terms
   if (S.has_bf) {
     const int n = S.nmax;
-    // orbitals of both spins (paho_orbitals, reptation.f:10298-10315)
-    int tot = 0;
-    for (int sp = 0; sp < nt; sp++) tot += S.np[sp] * S.np[sp];
-    for (int e = tid; e < tot; e += kThreads) {
-      int sp = 0, ee = e;
-      if (nt > 1 && ee >= S.np[0] * S.np[0]) {
-        ee -= S.np[0] * S.np[0];
-        sp = 1;
+    bool reg_path = true;  // the phase the log|det| sum below is counted in
+    if (inv_in) {
+      // orbitals, inverse, |pivot|^2, pivot rows and singular flags of both
+      // spins from orb_inv_kernel (the walker's move scratch)
+      const double *src = inv_in;
+      for (int sp = 0; sp < nt; sp++) {
+        const int ns = S.np[sp], ld = ws_ld(ns);
+        const double2 *sA = reinterpret_cast<const double2 *>(src);
+        const double2 *sW = sA + (size_t)ns * ns;
+        const double *sD = reinterpret_cast<const double *>(sW + (size_t)ns * ld);
+        double2 *dA = sp ? m.A[1] : m.A[0], *dW = sp ? m.W[1] : m.W[0];
+        for (int e = tid; e < ns * ns; e += kThreads) dA[e] = sA[e];
+        for (int e = tid; e < ns * ld; e += kThreads) dW[e] = sW[e];
+        for (int k = tid; k < ns; k += kThreads) {
+          (sp ? m.dk[1] : m.dk[0])[k] = sD[k];
+          (sp ? m.perm[1] : m.perm[0])[k] = (int)sD[ns + k];
+        }
+        if (tid == sp) m.iscal[sp] = sD[2 * ns] != 0.0;
+        src += inv_spin_doubles(ns);
       }
-      const int ns = S.np[sp], ld = ws_ld(ns), f0 = S.ipfrst[sp];
-      int k = ee % ns, j = ee / ns;
-      double gkx = __ldg(S.gvec + 2 * k), gky = __ldg(S.gvec + 2 * k + 1);
-      double kr = m.q[2 * (f0 + j)] * gkx + m.q[2 * (f0 + j) + 1] * gky;
-      double sv, cv;
-      sincos(kr, &sv, &cv);
-      (sp ? m.A[1] : m.A[0])[k + j * ns] = make_double2(cv, sv);
-      (sp ? m.W[1] : m.W[0])[k * ld + j] = make_double2(cv, sv);
-    }
-    for (int e = tid; e < 2 * n; e += kThreads) m.gsh[e] = __ldg(S.gvec + e);
-    if (tid < 2) m.iscal[tid] = 0;  // singular flags
-    __syncthreads();
-    phase_mark(S, PH_ORBITALS, tph);
-    // inversion: every warp in registers when each spin's matrix fits that
-    // layout (then rho_k), else half the CTA per shared-memory inversion
-    // with rho_k on the other warps
-    // (determinants in HBM: every warp, coalesced rows, then rho_k)
-    const int Gr = gj_reg_warps(nt);
-    bool reg_path = !kGmat && S.tune_inv != 1;
-    for (int sp = 0; sp < nt; sp++) reg_path = reg_path && gj_reg_lanes(S.np[sp], 32 * Gr) > 0;
-    bool panel_path = reg_path && S.tune_inv == 2;
-    for (int sp = 0; sp < nt; sp++) panel_path = panel_path && S.np[sp] <= 32;
-    if (panel_path) {
-      // blocks of eight pivot steps, one warp per panel, every warp of the
-      // spin's group on the rest; then rho_k on every warp
-      const int sp = nt > 1 ? (tid >> 5) / Gr : 0, gt = tid - sp * 32 * Gr;
-      gj_invert_panel(sp ? m.W[1] : m.W[0], ws_ld(S.np[sp]), S.np[sp],
-                      sp ? m.perm[1] : m.perm[0], sp ? m.dk[1] : m.dk[0], &m.iscal[sp], gt, Gr,
-                      1 + sp, sp ? m.pscr[1] : m.pscr[0]);
+      if (tid == 1 && nt == 1) m.iscal[1] = 0;
+      for (int e = tid; e < 2 * n; e += kThreads) m.gsh[e] = __ldg(S.gvec + e);
       __syncthreads();
-      phase_mark(S, PH_INVERT, tph);
-      rhok(tid, kThreads);
-      __syncthreads();
-    } else if (!kGmat && S.tune_inv == 1) {
-      // one warp per spin, warp-synchronous pivot steps; rho_k on the rest
-      const int w = tid >> 5;
-      if (w < nt) {
-        const int ns = S.np[w];
-        gj_invert(w ? m.W[1] : m.W[0], ws_ld(ns), ns, w ? m.perm[1] : m.perm[0],
-                  w ? m.dk[1] : m.dk[0], w ? m.used[1] : m.used[0], &m.iscal[w], tid & 31, 1,
-                  1 + w, m.gval + 8 * w, m.gidx + 8 * w);
-      } else {
-        rhok(tid - 32 * nt, kThreads - 32 * nt);
-      }
-      __syncthreads();
-    } else if (reg_path) {
-      const int sp = nt > 1 ? (tid >> 5) / Gr : 0, gt = tid - sp * 32 * Gr;
-      gj_invert_reg(sp ? m.W[1] : m.W[0], ws_ld(S.np[sp]), S.np[sp], sp ? m.perm[1] : m.perm[0],
-                    sp ? m.dk[1] : m.dk[0], &m.iscal[sp], gt, Gr, 1 + sp,
-                    sp ? m.gslot[1] : m.gslot[0], sp ? m.gkey[1] : m.gkey[0]);
-      __syncthreads();
-      phase_mark(S, PH_INVERT, tph);
+      phase_mark(S, PH_ORBITALS, tph);
       rhok(tid, kThreads);
       __syncthreads();
     } else {
-      // warps per spin: half the CTA for the inversions, the rest for rho_k
-      const int G = kGmat ? (kThreads / 32) / nt
-                          : ((kThreads / 32) / (2 * nt) > 0 ? (kThreads / 32) / (2 * nt) : 1);
-      const int w = tid >> 5;
-      if (w < G * nt) {
-        const int sp = w / G, gt = tid - sp * 32 * G;
-        const int ns = S.np[sp];
-        if (kGmat)
-          gj_invert_gmem(sp ? m.W[1] : m.W[0], ws_ld(ns), ns, sp ? m.perm[1] : m.perm[0],
-                         sp ? m.dk[1] : m.dk[0], sp ? m.used[1] : m.used[0], &m.iscal[sp], gt,
-                         G, 1 + sp, m.gval + 8 * sp, m.gidx + 8 * sp,
-                         sp ? m.fcol[1] : m.fcol[0]);
-        else
-          gj_invert(sp ? m.W[1] : m.W[0], ws_ld(ns), ns, sp ? m.perm[1] : m.perm[0],
-                    sp ? m.dk[1] : m.dk[0], sp ? m.used[1] : m.used[0], &m.iscal[sp], gt,
-                    G, 1 + sp, m.gval + 8 * sp, m.gidx + 8 * sp);
-      } else {
-        rhok(tid - G * nt * 32, kThreads - G * nt * 32);
+      // orbitals of both spins (paho_orbitals, reptation.f:10298-10315)
+      int tot = 0;
+      for (int sp = 0; sp < nt; sp++) tot += S.np[sp] * S.np[sp];
+      for (int e = tid; e < tot; e += kThreads) {
+        int sp = 0, ee = e;
+        if (nt > 1 && ee >= S.np[0] * S.np[0]) {
+          ee -= S.np[0] * S.np[0];
+          sp = 1;
+        }
+        const int ns = S.np[sp], ld = ws_ld(ns), f0 = S.ipfrst[sp];
+        int k = ee % ns, j = ee / ns;
+        double gkx = __ldg(S.gvec + 2 * k), gky = __ldg(S.gvec + 2 * k + 1);
+        double kr = m.q[2 * (f0 + j)] * gkx + m.q[2 * (f0 + j) + 1] * gky;
+        double sv, cv;
+        sincos(kr, &sv, &cv);
+        (sp ? m.A[1] : m.A[0])[k + j * ns] = make_double2(cv, sv);
+        (sp ? m.W[1] : m.W[0])[k * ld + j] = make_double2(cv, sv);
       }
+      for (int e = tid; e < 2 * n; e += kThreads) m.gsh[e] = __ldg(S.gvec + e);
+      if (tid < 2) m.iscal[tid] = 0;  // singular flags
       __syncthreads();
-      if (G * nt == kThreads / 32) {
+      phase_mark(S, PH_ORBITALS, tph);
+      // inversion: every warp in registers when each spin's matrix fits that
+      // layout (then rho_k), else half the CTA per shared-memory inversion
+      // with rho_k on the other warps
+      // (determinants in HBM: every warp, coalesced rows, then rho_k)
+      const int Gr = gj_reg_warps(nt);
+      reg_path = !kGmat && S.tune_inv != 1;
+      for (int sp = 0; sp < nt; sp++) reg_path = reg_path && gj_reg_lanes(S.np[sp], 32 * Gr) > 0;
+      bool panel_path = reg_path && S.tune_inv == 2;
+      for (int sp = 0; sp < nt; sp++) panel_path = panel_path && S.np[sp] <= 32;
+      if (panel_path) {
+        // blocks of eight pivot steps, one warp per panel, every warp of the
+        // spin's group on the rest; then rho_k on every warp
+        const int sp = nt > 1 ? (tid >> 5) / Gr : 0, gt = tid - sp * 32 * Gr;
+        gj_invert_panel(sp ? m.W[1] : m.W[0], ws_ld(S.np[sp]), S.np[sp],
+                        sp ? m.perm[1] : m.perm[0], sp ? m.dk[1] : m.dk[0], &m.iscal[sp], gt, Gr,
+                        1 + sp, sp ? m.pscr[1] : m.pscr[0]);
+        __syncthreads();
+        phase_mark(S, PH_INVERT, tph);
         rhok(tid, kThreads);
         __syncthreads();
+      } else if (!kGmat && S.tune_inv == 1) {
+        // one warp per spin, warp-synchronous pivot steps; rho_k on the rest
+        const int w = tid >> 5;
+        if (w < nt) {
+          const int ns = S.np[w];
+          gj_invert(w ? m.W[1] : m.W[0], ws_ld(ns), ns, w ? m.perm[1] : m.perm[0],
+                    w ? m.dk[1] : m.dk[0], w ? m.used[1] : m.used[0], &m.iscal[w], tid & 31, 1,
+                    1 + w, m.gval + 8 * w, m.gidx + 8 * w);
+        } else {
+          rhok(tid - 32 * nt, kThreads - 32 * nt);
+        }
+        __syncthreads();
+      } else if (reg_path) {
+        const int sp = nt > 1 ? (tid >> 5) / Gr : 0, gt = tid - sp * 32 * Gr;
+        gj_invert_reg(sp ? m.W[1] : m.W[0], ws_ld(S.np[sp]), S.np[sp], sp ? m.perm[1] : m.perm[0],
+                      sp ? m.dk[1] : m.dk[0], &m.iscal[sp], gt, Gr, 1 + sp,
+                      sp ? m.gslot[1] : m.gslot[0], sp ? m.gkey[1] : m.gkey[0]);
+        __syncthreads();
+        phase_mark(S, PH_INVERT, tph);
+        rhok(tid, kThreads);
+        __syncthreads();
+      } else {
+        // warps per spin: half the CTA for the inversions, the rest for rho_k
+        const int G = kGmat ? (kThreads / 32) / nt
+                            : ((kThreads / 32) / (2 * nt) > 0 ? (kThreads / 32) / (2 * nt) : 1);
+        const int w = tid >> 5;
+        if (w < G * nt) {
+          const int sp = w / G, gt = tid - sp * 32 * G;
+          const int ns = S.np[sp];
+          if (kGmat)
+            gj_invert_gmem(sp ? m.W[1] : m.W[0], ws_ld(ns), ns, sp ? m.perm[1] : m.perm[0],
+                           sp ? m.dk[1] : m.dk[0], sp ? m.used[1] : m.used[0], &m.iscal[sp], gt,
+                           G, 1 + sp, m.gval + 8 * sp, m.gidx + 8 * sp,
+                           sp ? m.fcol[1] : m.fcol[0]);
+          else
+            gj_invert(sp ? m.W[1] : m.W[0], ws_ld(ns), ns, sp ? m.perm[1] : m.perm[0],
+                      sp ? m.dk[1] : m.dk[0], sp ? m.used[1] : m.used[0], &m.iscal[sp], gt,
+                      G, 1 + sp, m.gval + 8 * sp, m.gidx + 8 * sp);
+        } else {
+          rhok(tid - G * nt * 32, kThreads - G * nt * 32);
+        }
+        __syncthreads();
+        if (G * nt == kThreads / 32) {
+          rhok(tid, kThreads);
+          __syncthreads();
+        }
       }
     }
     {

@@ -58,10 +58,16 @@ TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum of pairs_kernel + move_kernel (296 w
                   "x walkers/296, + the move scratch written per walker")
 
 
-def move_scratch_bytes(N, nk):
-    """Bytes of one walker's move scratch block (MoveScratch, backflow)."""
+def move_scratch_bytes(N, nk, ns=()):
+    """Bytes of one walker's move scratch block (MoveScratch, backflow; with
+    ns, the spins' orbital counts, the orbitals-and-inversion region when
+    every spin has at most 32 orbitals)."""
     pair = (14 * N + 3 + 4 * max(nk, 1) + 3) & ~3
-    return 8 * ((pair + 3 * N * N + 31) & ~31)
+    end = pair + 3 * N * N
+    if ns and max(ns) <= 32:
+        end = (end + 1) & ~1
+        end += sum((2 * n * n + 2 * n * (n | 1) + 2 * n + 2 + 1) & ~1 for n in ns)
+    return 8 * ((end + 31) & ~31)
 
 
 def flops_per_sweep(N, ns, K):
@@ -366,6 +372,8 @@ def b200_arm(args, rank, world, local_rank):
         h.set_inversion(args.inversion)
     if args.pair_lanes is not None:  # fixed lanes per particle instead of the tuner's
         h.set_pair_lanes(args.pair_lanes)
+    if args.move_inversion is not None:  # orbitals and inversion in their own kernel or not
+        h.set_move_inversion(args.move_inversion)
     h.block_reset()
     h.vmc(10, delta, 10 ** 9)
     blk, norm = h.block_get()
@@ -440,6 +448,7 @@ def b200_arm(args, rank, world, local_rank):
     pair_ms, pair_n = h.profile_get(capi.KERNEL_PAIRS)
     br_ms, br_n = h.profile_get(capi.KERNEL_BRANCH)
     ga_ms, ga_n = h.profile_get(capi.KERNEL_GATHER)
+    oi_ms, oi_n = h.profile_get(capi.KERNEL_ORB_INV)
     h.profile(False)
     blk, norm = h.block_get()
     e_mean = blk[0] / norm
@@ -475,15 +484,16 @@ def b200_arm(args, rank, world, local_rank):
     if rank == 0:
         K = sysobj.s.nk
         fpm = flops_per_move(N, ns, K, 0, 1)
-        # one walker-move of the population = one pairs_kernel + one
-        # move_kernel launch; the roofline covers both
-        achieved = fpm * nw / ((move_ms + pair_ms) / max(move_n, 1) * 1e-3) / 1e12
+        # one walker-move of the population = one pairs_kernel, one
+        # orb_inv_kernel (where it applies) and one move_kernel launch; the
+        # roofline covers them all
+        achieved = fpm * nw / ((move_ms + pair_ms + oi_ms) / max(move_n, 1) * 1e-3) / 1e12
         peak = fp64_peak_tflops(torch)
         cpu = None
         if world == 1 and not args.no_cpu:
             rate, cores, sample = cpu_rate(d, args.cpu_seconds, rs=rs)
             cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
-        launches = pair_n + move_n + br_n + ga_n
+        launches = pair_n + oi_n + move_n + br_n + ga_n
         metric, config = workload_desc(args, world)
         line = {
             "metric": metric,
@@ -500,15 +510,17 @@ def b200_arm(args, rank, world, local_rank):
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": ((MOVE_DRAM_READ_PER_WALKER + move_scratch_bytes(N, K)) * nw
+                         "traffic": ((MOVE_DRAM_READ_PER_WALKER + move_scratch_bytes(N, K, ns)) * nw
                                      if headline else None),
                          "traffic_source": TRAFFIC_SOURCE if headline else None,
-                         "kernel": "pairs_kernel + move_kernel",
+                         "kernel": ("pairs_kernel + orb_inv_kernel + move_kernel" if oi_n
+                                    else "pairs_kernel + move_kernel"),
                          "flops_per_move": fpm,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64)"},
             "cpu_baseline": cpu,
             "gpu_launches": launches,
-            "kernel_ms": {"pairs": pair_ms, "move": move_ms, "branch": br_ms, "gather": ga_ms},
+            "kernel_ms": {"pairs": pair_ms, "orb_inv": oi_ms, "move": move_ms, "branch": br_ms,
+                          "gather": ga_ms},
             "wall_s": wall,
             "e_mixed": e_mean,
             "acceptance": (acc["accepted"] - acc0["accepted"]) /
@@ -671,7 +683,7 @@ def config_arm(args, rank, world, local_rank):
 
         def step():
             h.vmc(1, delta, 10 ** 9)
-        kernels = (capi.KERNEL_PAIRS, capi.KERNEL_MOVE)
+        kernels = (capi.KERNEL_PAIRS, capi.KERNEL_ORB_INV, capi.KERNEL_MOVE)
     else:
         delta, etrial, mage_r = 0.01 * rs * rs, -0.27, 50
         h = q.Handle(sysobj, capacity=nw, seed=walker_seed, device=local_rank)
@@ -1154,6 +1166,9 @@ def main():
                     help="determinant inversion layout (qmc2d_set_inversion)")
     ap.add_argument("--pair-lanes", type=int, default=None, choices=[4, 8, 16],
                     help="lanes per particle of the pair passes (qmc2d_set_pair_lanes)")
+    ap.add_argument("--move-inversion", type=int, default=None, choices=[0, 1],
+                    help="orbitals and inversion of a move in their own kernel "
+                         "(qmc2d_set_move_inversion)")
     ap.add_argument("--single", action="store_true",
                     help="vmc workload with single-electron moves and Sherman-Morrison updates")
     ap.add_argument("--rmc-split", type=int, default=None, choices=[0, 1],

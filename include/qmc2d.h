@@ -245,6 +245,14 @@ int qmc2d_set_inversion(qmc2d_handle *h, int layout);
  * reports the choice in force. */
 int qmc2d_set_pair_lanes(qmc2d_handle *h, int lanes);
 int qmc2d_get_pair_lanes(qmc2d_handle *h, int *lanes);
+/* Where the moves (VMC, DMC) invert their determinants: 1 (the default)
+ * in a kernel of its own between the pair kernel and the move kernel, one
+ * warp per spin matrix, for spins of at most 32 orbitals held in shared
+ * memory; 0 inside the move kernel with the inversion layout in force.
+ * Both pivot as zgefa does and agree to round-off. get reports 1 only where
+ * the separate kernel applies. The reference has no counterpart. */
+int qmc2d_set_move_inversion(qmc2d_handle *h, int batched);
+int qmc2d_get_move_inversion(qmc2d_handle *h, int *batched);
 /* qmc2d_autotune also times the three inversion layouts on the evaluation
  * kernel over the population's configurations (three launches each into the
  * handle's staging buffers; the population is not changed) and keeps the
@@ -609,7 +617,8 @@ enum qmc2d_kernel {
   QMC2D_KERNEL_RMC = 4,     /* reptation moves */
   QMC2D_KERNEL_PAIRS = 5,   /* proposal + pair passes of a VMC/DMC move */
   QMC2D_KERNEL_SINGLE = 6,  /* single-electron VMC sweeps (qmc2d_vmc_single) */
-  QMC2D_NKERNELS = 7
+  QMC2D_KERNEL_ORB_INV = 7, /* orbitals and their inversion of a move (orb_inv_kernel) */
+  QMC2D_NKERNELS = 8
 };
 /* The handle's CUDA stream (a cudaStream_t) so callers can order work and
  * events after the library's launches. */
