@@ -618,6 +618,16 @@ __device__ __forceinline__ void phase_mark(const DevSys &S, int k, long long &t)
   phase_mark(S, k, t, threadIdx.x == 0);
 }
 
+// One 16-byte global-to-shared copy without a register round trip
+// (cp.async.cg: L2 only), and the wait for every copy this thread issued.
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -1490,8 +1500,9 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
         const double2 *sW = sA + (size_t)ns * ns;
         const double *sD = reinterpret_cast<const double *>(sW + (size_t)ns * ld);
         double2 *dA = sp ? m.A[1] : m.A[0], *dW = sp ? m.W[1] : m.W[0];
-        for (int e = tid; e < ns * ns; e += kThreads) dA[e] = sA[e];
-        for (int e = tid; e < ns * ld; e += kThreads) dW[e] = sW[e];
+        // asynchronous 16-byte global-to-shared copies, all in flight at once
+        for (int e = tid; e < ns * ns; e += kThreads) cp_async16(dA + e, sA + e);
+        for (int e = tid; e < ns * ld; e += kThreads) cp_async16(dW + e, sW + e);
         for (int k = tid; k < ns; k += kThreads) {
           (sp ? m.dk[1] : m.dk[0])[k] = sD[k];
           (sp ? m.perm[1] : m.perm[0])[k] = (int)sD[ns + k];
@@ -1501,6 +1512,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
       }
       if (tid == 1 && nt == 1) m.iscal[1] = 0;
       for (int e = tid; e < 2 * n; e += kThreads) m.gsh[e] = __ldg(S.gvec + e);
+      cp_async_wait_all();
       __syncthreads();
       phase_mark(S, PH_ORBITALS, tph);
       rhok(tid, kThreads);
