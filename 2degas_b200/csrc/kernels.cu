@@ -380,30 +380,33 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
     prefetch_l2(o + L.inv, nd);
   }
   if (S.has_bf && !S.bf_zero) prefetch_l2(o + L.pair, 3 * (size_t)N * N);
+  // the walker's state into shared memory: asynchronous 8-byte copies, all
+  // in flight at once
   for (int j = tid; j < N2; j += kThreads) {
-    v.xo[j] = pop.x[(size_t)w * N2 + j];
-    v.go[j] = pop.g[(size_t)w * N2 + j];
-    m.x[j] = o[L.x + j];
-    m.g[j] = o[L.g + j];
-    m.q[j] = o[L.q + j];
-    m.qbd[j] = o[L.qbd + j];
+    cp_async8(v.xo + j, pop.x + (size_t)w * N2 + j);
+    cp_async8(v.go + j, pop.g + (size_t)w * N2 + j);
+    cp_async8(m.x + j, o + L.x + j);
+    cp_async8(m.g + j, o + L.g + j);
+    cp_async8(m.q + j, o + L.q + j);
+    cp_async8(m.qbd + j, o + L.qbd + j);
     m.gd[j] = 0.0;
   }
-  for (int j = tid; j < 3 * N; j += kThreads) m.Sb[j] = o[L.sb + j];
+  for (int j = tid; j < 3 * N; j += kThreads) cp_async8(m.Sb + j, o + L.sb + j);
   for (int j = tid; j < N; j += kThreads) {
-    m.lap[j] = o[L.lap + j];
-    m.ltf[j] = o[L.ltf + j];
-    m.vp[j] = o[L.vp + j];
+    cp_async8(m.lap + j, o + L.lap + j);
+    cp_async8(m.ltf + j, o + L.ltf + j);
+    cp_async8(m.vp + j, o + L.vp + j);
     m.lapd[j] = 0.0;
     m.ph2[j] = 0.0;
     m.ph2d[j] = 0.0;
   }
   for (int j = tid; j < np; j += kThreads) {
-    v.po[j] = pop.p[(size_t)w * np + j];
-    v.blk[j] = a.blk[(size_t)w * np + j];
+    cp_async8(v.po + j, pop.p + (size_t)w * np + j);
+    cp_async8(v.blk + j, a.blk + (size_t)w * np + j);
   }
-  if (tid < nt) v.ho[tid] = pop.h[(size_t)w * nt + tid];
+  if (tid < nt) cp_async8(v.ho + tid, pop.h + (size_t)w * nt + tid);
   const double wold = o[L.wold];
+  cp_async_wait_all();
   __syncthreads();
   double so = pop.s[w];
   double age = pop.age[w];

@@ -618,11 +618,16 @@ __device__ __forceinline__ void phase_mark(const DevSys &S, int k, long long &t)
   phase_mark(S, k, t, threadIdx.x == 0);
 }
 
-// One 16-byte global-to-shared copy without a register round trip
-// (cp.async.cg: L2 only), and the wait for every copy this thread issued.
+// One 16-byte (cp.async.cg, through L2 only) or 8-byte global-to-shared
+// copy without a register round trip, and the wait for every copy this
+// thread issued.
 __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(double *smem_dst, const double *gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem_src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;" ::: "memory");
