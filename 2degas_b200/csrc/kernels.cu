@@ -166,9 +166,10 @@ __global__ void __launch_bounds__(G * kThreads, 2 / G) pairs_kernel(const DevSys
     const float4 *src = reinterpret_cast<const float4 *>(rows_g);
     for (int e = threadIdx.x; e < nrow * V; e += kPairThreads) {
       const int r = e / V, q = e - r * V;
-      reinterpret_cast<float4 *>(rows_s + (size_t)r * Lay::sstride)[q] =
-          __ldg(src + (size_t)r * VG + q);
+      cp_async16(reinterpret_cast<float4 *>(rows_s + (size_t)r * Lay::sstride) + q,
+                 src + (size_t)r * VG + q);
     }
+    cp_async_wait_all();
   }
   __syncthreads();
   const GroupSync sync{1 + grp, kThreads};

@@ -1480,10 +1480,12 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
   const int tid = threadIdx.x;
   // rho_k of both slots: copied when given (MoveScratch), else summed
   auto rhok = [&](int t0, int nthr) {
-    if (rhok_in)
-      for (int e = t0; e < 4 * S.nk; e += nthr) m.rhok[e] = rhok_in[e];
-    else
+    if (rhok_in) {
+      for (int e = t0; e < 4 * S.nk; e += nthr) cp_async8(m.rhok + e, rhok_in + e);
+      cp_async_wait_all();
+    } else {
       compute_rhok(S, m, t0, nthr);
+    }
   };
   const int N = S.N, nt = S.nt;
   const int lane8 = tid & (kGroup - 1);
