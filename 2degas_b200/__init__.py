@@ -324,10 +324,15 @@ class Handle:
         """Lanes per particle of the pair passes: 4, 8 or 16 (0: the default, 8)."""
         self._chk(self.lib.qmc2d_set_pair_lanes(self.h, lanes))
 
-    def set_move_inversion(self, batched):
-        """1: orbitals and inversion in their own kernel before the move kernel
-        (default where it applies); 0: inside the move kernel."""
-        self._chk(self.lib.qmc2d_set_move_inversion(self.h, batched))
+    def set_move_inversion(self, mode):
+        """Orbitals and inversion of a move in their own kernel before the move
+        kernel: 1 when the population is large enough (default), 2 whenever it
+        fits, 0 never (inside the move kernel)."""
+        self._chk(self.lib.qmc2d_set_move_inversion(self.h, mode))
+
+    def set_autotune_scope(self, mask):
+        """What autotune() times: 1 groups/staging, 2 lanes, 4 inversion layout."""
+        self._chk(self.lib.qmc2d_set_autotune_scope(self.h, mask))
 
     def get_move_inversion(self):
         v = ctypes.c_int()

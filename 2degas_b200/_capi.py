@@ -192,6 +192,7 @@ SIGNATURES = {
     "qmc2d_vmc_single": (c_int, [c_void_p, c_int, c_double, c_int]),
     "qmc2d_set_inversion": (c_int, [c_void_p, c_int]),
     "qmc2d_set_pair_lanes": (c_int, [c_void_p, c_int]),
+    "qmc2d_set_autotune_scope": (c_int, [c_void_p, c_int]),
     "qmc2d_set_move_inversion": (c_int, [c_void_p, c_int]),
     "qmc2d_get_move_inversion": (c_int, [c_void_p, PI]),
     "qmc2d_get_pair_lanes": (c_int, [c_void_p, PI]),

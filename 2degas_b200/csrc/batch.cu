@@ -100,6 +100,7 @@ cudaError_t enqueue(qmc2d_batch *b, int k, int g0, int ngen, int dmc, double del
     a.cnt = h->d_cnt;
     a.wate = dmc ? h->d_wate : nullptr;
     a.status = h->d_status;
+    a.orb_inv = move_orb_inv(h) ? 1 : 0;
     a.ctr = ctr;
     if ((e = q2d::launch_pairs(h->hs, h->ds, h->pop[cur], a, st)) != cudaSuccess) return e;
     if ((e = q2d::launch_orb_inv(h->hs, h->ds, a, st)) != cudaSuccess) return e;

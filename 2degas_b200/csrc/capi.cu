@@ -292,7 +292,8 @@ extern "C" int qmc2d_create(const qmc2d_system *sys, const qmc2d_options *opt,
     q2d::set_error(buf);
     return fail(QMC2D_ERR_LIMIT);
   }
-  h->hs.split_inv = 1;  // moves take orb_inv_kernel where the scratch has its region
+  h->hs.split_inv = 1;  // moves may take orb_inv_kernel: the scratch has its region
+  cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device);
   if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking)) != cudaSuccess)
     return fail(cuda_fail(e, "cudaStreamCreate"));
@@ -420,22 +421,18 @@ extern "C" int qmc2d_get_pair_lanes(qmc2d_handle *h, int *lanes) {
   return QMC2D_OK;
 }
 
-extern "C" int qmc2d_set_move_inversion(qmc2d_handle *h, int batched) {
-  if (!h || batched < 0 || batched > 1) {
-    q2d::set_error("qmc2d_set_move_inversion: bad argument");
+extern "C" int qmc2d_set_move_inversion(qmc2d_handle *h, int mode) {
+  if (!h || mode < 0 || mode > 2) {
+    q2d::set_error("qmc2d_set_move_inversion: mode must be 0, 1 or 2");
     return QMC2D_ERR_ARG;
   }
-  CK(cudaSetDevice(h->device));
-  CK(join_side(h));
-  h->hs.split_inv = batched;
-  CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+  h->move_inv_mode = mode;  // host-side launch choice (MoveArgs::orb_inv)
   return QMC2D_OK;
 }
 
 extern "C" int qmc2d_get_move_inversion(qmc2d_handle *h, int *batched) {
   if (!h || !batched) return QMC2D_ERR_ARG;
-  *batched = q2d::orb_inv_applies(h->hs) ? 1 : 0;
+  *batched = move_orb_inv(h) ? 1 : 0;
   return QMC2D_OK;
 }
 
@@ -475,9 +472,11 @@ extern "C" int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   double best = 1e300;
-  int bg = 2, bs = 0;
+  int bg = h->hs.tune_groups ? h->hs.tune_groups : 2, bs = h->hs.tune_stage;
+  const int lanes_in = h->hs.tune_lanes;
   h->hs.tune_lanes = 8;  // the groups and staging are compared at the default lanes
   for (const auto &v : var) {
+    if (!(h->tune_scope & 1)) break;
     h->hs.tune_groups = v[0];
     h->hs.tune_stage = v[1];
     CK(q2d::launch_pairs(h->hs, h->ds, h->pop[h->cur], a, h->stream));  // warm-up
@@ -495,9 +494,10 @@ extern "C" int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *
   }
   h->hs.tune_groups = bg;
   h->hs.tune_stage = bs;
+  h->hs.tune_lanes = lanes_in;
   // lanes per particle of the pair passes, with the chosen groups and staging
   // (8 first: the other two must beat it)
-  {
+  if (h->tune_scope & 2) {
     const int lanes[3] = {8, 4, 16};
     int bl = 8;
     for (int l : lanes) {
@@ -520,7 +520,7 @@ extern "C" int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *
   // inversion layout of the determinant section, timed on the evaluation
   // kernel over the population's configurations (into the staging buffers;
   // the population is not changed)
-  if (h->hs.has_bf && !h->hs.gmat) {
+  if ((h->tune_scope & 4) && h->hs.has_bf && !h->hs.gmat) {
     double best_inv = 1e300;
     int bi = 0;
     for (int layout = 0; layout < 3; layout++) {
@@ -552,6 +552,15 @@ extern "C" int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *
   if (groups) *groups = bg;
   if (stage) *stage = bs;
   if (ms) *ms = best;
+  return QMC2D_OK;
+}
+
+extern "C" int qmc2d_set_autotune_scope(qmc2d_handle *h, int mask) {
+  if (!h || mask < 0 || mask > 7) {
+    q2d::set_error("qmc2d_set_autotune_scope: mask must be in 0..7");
+    return QMC2D_ERR_ARG;
+  }
+  h->tune_scope = mask;
   return QMC2D_OK;
 }
 
@@ -882,6 +891,7 @@ static int run_moves(qmc2d_handle *h, int nstp, int dmc, double delta, double et
   a.cnt = h->d_cnt;
   a.wate = dmc ? h->d_wate : nullptr;
   a.status = h->d_status;
+  a.orb_inv = move_orb_inv(h) ? 1 : 0;
   if (h->hs.delta != delta && h->hs.adrift != 0.0) {
     h->hs.delta = delta;
     CK(cudaMemcpyAsync(h->ds, &h->hs, sizeof(q2d::DevSys), cudaMemcpyHostToDevice, h->stream));
@@ -893,7 +903,7 @@ static int run_moves(qmc2d_handle *h, int nstp, int dmc, double delta, double et
       ProfScope ps(h, QMC2D_KERNEL_PAIRS, h->stream);
       CK(q2d::launch_pairs(h->hs, h->ds, h->pop[h->cur], a, h->stream));
     }
-    if (q2d::orb_inv_applies(h->hs)) {
+    if (a.orb_inv) {
       ProfScope ps(h, QMC2D_KERNEL_ORB_INV, h->stream);
       CK(q2d::launch_orb_inv(h->hs, h->ds, a, h->stream));
     }

@@ -63,11 +63,12 @@ struct DevSys {
   // memory (warp-synchronous steps) with rho_k on the other warps; 2 the
   // panel-blocked form (one-warp panels of eight pivot steps).
   int tune_inv;
-  // Moves of spins of at most 32 orbitals (no HBM determinants): the
-  // orbitals and their inversion run in orb_inv_kernel, one warp per spin
-  // matrix, between the pair kernel and the move kernel, which loads A, the
-  // inverse, the pivots and |pivot|^2 from the move scratch
-  // (qmc2d_set_move_inversion; 1 by default where the scratch has room).
+  // Moves of spins of at most 32 orbitals (no HBM determinants) may run the
+  // orbitals and their inversion in orb_inv_kernel, one warp per spin
+  // matrix, between the pair kernel and the move kernel, which then loads
+  // A, the inverse, the pivots and |pivot|^2 from the move scratch (host
+  // side: 1 once the handle exists; whether a move does so is
+  // MoveArgs::orb_inv, qmc2d_set_move_inversion).
   int split_inv;
   // Every backflow table identically zero (set by the handle): q = x and the
   // backflow Jacobian is the identity, so the pair passes skip the backflow

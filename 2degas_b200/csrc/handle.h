@@ -36,6 +36,14 @@ struct qmc2d_handle {
   cudaEvent_t ev_fork = nullptr, ev_side = nullptr;
   bool side_pending = false;
   int device = 0;
+  int nsm = 0;  // the device's SMs
+  // qmc2d_set_move_inversion: 1 the batched orbital-and-inversion kernel
+  // when the population gives it at least kOrbInvMinPerSM spin matrices per
+  // SM, 2 always (where it fits), 0 never
+  int move_inv_mode = 1;
+  // qmc2d_set_autotune_scope: 1 the pair kernel's groups and staging, 2 its
+  // lanes per particle, 4 the inversion layout
+  int tune_scope = 7;
   uint64_t seed = 0;
   uint32_t move_counter = 0, gen_counter = 0;
   uint32_t sweep_counter = 0;  // Philox c2 of single-electron sweeps (qmc2d_vmc_single)
@@ -50,6 +58,16 @@ struct qmc2d_handle {
   double prof_ms[QMC2D_NKERNELS] = {0};
   long prof_n[QMC2D_NKERNELS] = {0};
 };
+
+// Spin matrices per SM below which a move inverts inside the move kernel
+// instead of in orb_inv_kernel (qmc2d_set_move_inversion mode 1).
+constexpr int kOrbInvMinPerSM = 24;
+
+// Whether this handle's next move batches its orbitals and inversion.
+inline bool move_orb_inv(const qmc2d_handle *h) {
+  if (h->move_inv_mode == 0) return false;
+  return q2d::orb_inv_pays(h->hs, h->nw, h->nsm, h->move_inv_mode == 2 ? 0 : kOrbInvMinPerSM);
+}
 
 // Orders the handle's stream after the side copies of the last
 // qmc2d_population_load_async (nothing when none are pending). Every entry

@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
                    : "memory");
     }
   };
-  if (!kGmat && S.split_inv && L.inv) {
+  if (!kGmat && a.orb_inv && L.inv) {
     size_t nd = 0;
     for (int t = 0; t < nt; t++) nd += inv_spin_doubles(S.np[t]);
     prefetch_l2(o + L.inv, nd);
@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
   long long tph = clock64();
   double sn = 1.0;
   status |= eval_det<kGmat>(S, m, v.hn, v.pn, &v.sc[0], tph, S.has_bf ? o + L.pair : nullptr,
-                            o + L.rhok, !kGmat && S.split_inv && L.inv ? o + L.inv : nullptr);
+                            o + L.rhok, !kGmat && a.orb_inv && L.inv ? o + L.inv : nullptr);
   sn = v.sc[0];
   // reverse move (reptation.f:4660-4674)
   double wn = 0.0;
@@ -799,10 +799,13 @@ cudaError_t launch_pairs(const DevSys &hs, const DevSys *ds, DevPop pop, const M
 }
 
 bool orb_inv_applies(const DevSys &hs) { return hs.split_inv && orb_inv_fits(hs); }
+bool orb_inv_pays(const DevSys &hs, int nw, int nsm, int min_per_sm) {
+  return orb_inv_applies(hs) && (long)nw * hs.nt >= (long)nsm * min_per_sm;
+}
 
 cudaError_t launch_orb_inv(const DevSys &hs, const DevSys *ds, const MoveArgs &a,
                            cudaStream_t st) {
-  if (a.nw <= 0 || !orb_inv_applies(hs)) return cudaSuccess;
+  if (a.nw <= 0 || !a.orb_inv || !orb_inv_applies(hs)) return cudaSuccess;
   size_t wd = 0;
   for (int t = 0; t < hs.nt; t++) wd = std::max(wd, orb_inv_warp_doubles(hs.np[t]));
   const size_t sm = sizeof(double) * wd * kOrbWarps;

@@ -26,6 +26,7 @@ struct MoveArgs {
   double *cnt;        // nw * 4: accepted, proposed, forced, nonzero status
   double *wate;       // nw DMC weights (product over the generation's moves)
   int *status;        // nw status words (OR-ed)
+  int orb_inv;        // 1: orb_inv_kernel ran before the move kernel (its output is in scr)
   // Device counters {move, generation} added to step0 (and to the comb's
   // generation) when non-null: a CUDA graph replays its launches with the
   // same arguments, so the Philox counters that must advance are read here.
@@ -42,15 +43,18 @@ cudaError_t launch_eval(const DevSys &hs, const DevSys *ds, int nw, const double
 
 // One move of a resident population: the proposal and pair passes into the
 // move scratch (launch_pairs), the orbitals and their inversion into the
-// move scratch when DevSys::split_inv applies (launch_orb_inv, otherwise
+// move scratch when MoveArgs::orb_inv is set (launch_orb_inv, otherwise
 // nothing), then the rest of the evaluation, the acceptance and the
 // averages (launch_move).
 cudaError_t launch_pairs(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
                          cudaStream_t st);
 cudaError_t launch_orb_inv(const DevSys &hs, const DevSys *ds, const MoveArgs &a,
                            cudaStream_t st);
-// launch_orb_inv runs (DevSys::split_inv and a scratch region for it).
+// launch_orb_inv can run (DevSys::split_inv and a scratch region for it),
+// and whether it pays for a population of nw walkers on nsm SMs: the
+// batched kernel wants at least min_per_sm spin matrices per SM.
 bool orb_inv_applies(const DevSys &hs);
+bool orb_inv_pays(const DevSys &hs, int nw, int nsm, int min_per_sm);
 cudaError_t launch_move(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
                         cudaStream_t st);
 // Doubles of move scratch per walker.

@@ -146,13 +146,13 @@ def run_request(p, device=0):
             acc = (c1["accepted"] - c0["accepted"]) / max(c1["proposed"] - c0["proposed"], 1.0)
             c0 = c1
             dv *= min(2.0, max(0.3, acc / 0.5))
-        h.autotune()  # the pair kernel's launch choice for this population
-        # the inversion layouts and the pair lanes agree only to round-off,
-        # and the autotuner's pick depends on timing, which the mix changes:
-        # keep the defaults so a request's result does not depend on what
-        # else runs
-        h.set_inversion(0)
-        h.set_pair_lanes(0)
+        # the pair kernel's walker groups and staging for this population; the
+        # inversion layouts and the pair lanes agree only to round-off, and
+        # the autotuner's pick depends on timing, which the mix changes: they
+        # keep their defaults so a request's result does not depend on what
+        # else runs (and are not timed)
+        h.set_autotune_scope(1)
+        h.autotune()
         # DMC at a tenth of the VMC step (acceptance near 97%)
         tau = req.tau or (dv / 10.0 if req.method == "dmc" else dv)
         if req.method == "dmc":

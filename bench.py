@@ -680,6 +680,8 @@ def config_arm(args, rank, world, local_rank):
         h.population_set(x0)
         h.vmc(args.equil, delta, 10 ** 9)
         tuned = h.autotune()
+        if args.move_inversion is not None:
+            h.set_move_inversion(args.move_inversion)
 
         def step():
             h.vmc(1, delta, 10 ** 9)
@@ -1166,7 +1168,7 @@ def main():
                     help="determinant inversion layout (qmc2d_set_inversion)")
     ap.add_argument("--pair-lanes", type=int, default=None, choices=[4, 8, 16],
                     help="lanes per particle of the pair passes (qmc2d_set_pair_lanes)")
-    ap.add_argument("--move-inversion", type=int, default=None, choices=[0, 1],
+    ap.add_argument("--move-inversion", type=int, default=None, choices=[0, 1, 2],
                     help="orbitals and inversion of a move in their own kernel "
                          "(qmc2d_set_move_inversion)")
     ap.add_argument("--single", action="store_true",

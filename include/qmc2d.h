@@ -245,19 +245,28 @@ int qmc2d_set_inversion(qmc2d_handle *h, int layout);
  * reports the choice in force. */
 int qmc2d_set_pair_lanes(qmc2d_handle *h, int lanes);
 int qmc2d_get_pair_lanes(qmc2d_handle *h, int *lanes);
-/* Where the moves (VMC, DMC) invert their determinants: 1 (the default)
- * in a kernel of its own between the pair kernel and the move kernel, one
- * warp per spin matrix, for spins of at most 32 orbitals held in shared
- * memory; 0 inside the move kernel with the inversion layout in force.
- * Both pivot as zgefa does and agree to round-off. get reports 1 only where
- * the separate kernel applies. The reference has no counterpart. */
-int qmc2d_set_move_inversion(qmc2d_handle *h, int batched);
+/* Where the moves (VMC, DMC) invert their determinants. The batched form
+ * runs the orbitals and their inversion in a kernel of its own between the
+ * pair kernel and the move kernel, one warp per spin matrix, for spins of
+ * at most 32 orbitals held in shared memory; otherwise the move kernel
+ * inverts with the inversion layout in force. mode 1 (the default): batched
+ * when the population gives at least 24 spin matrices per SM (a fuller GPU
+ * hides the pivot chains; small populations finish sooner inside the move
+ * kernel); 2: batched whenever it fits; 0: never. Both pivot as zgefa does
+ * and agree to round-off. get reports whether the next move is batched. The
+ * reference has no counterpart. */
+int qmc2d_set_move_inversion(qmc2d_handle *h, int mode);
 int qmc2d_get_move_inversion(qmc2d_handle *h, int *batched);
 /* qmc2d_autotune also times the three inversion layouts on the evaluation
  * kernel over the population's configurations (three launches each into the
  * handle's staging buffers; the population is not changed) and keeps the
  * faster; *ms is the chosen pair-kernel time per launch. */
 int qmc2d_autotune(qmc2d_handle *h, int *groups, int *stage, double *ms);
+/* What qmc2d_autotune times (a bit mask, 7 by default): 1 the pair kernel's
+ * walker groups and staging (every choice gives the same values bit for
+ * bit), 2 its lanes per particle, 4 the inversion layout (these two change
+ * the rounding). Choices outside the mask keep their current values. */
+int qmc2d_set_autotune_scope(qmc2d_handle *h, int mask);
 /* The launch choices in force: pair-kernel walker groups and staging, and
  * the inversion layout. */
 int qmc2d_get_launch(qmc2d_handle *h, int *groups, int *stage, int *inversion);
