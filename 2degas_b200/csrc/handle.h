@@ -61,12 +61,21 @@ struct qmc2d_handle {
 
 // Spin matrices per SM below which a move inverts inside the move kernel
 // instead of in orb_inv_kernel (qmc2d_set_move_inversion mode 1).
-constexpr int kOrbInvMinPerSM = 24;
+// Measured crossovers (1024 to 4096 walkers at N = 26, 42, 58 and 25
+// polarised): two spins of more than 16 orbitals gain from about 24
+// matrices per SM, smaller ones (the 16-column kernel, 124 registers) from
+// about 12; a single spin, whose in-kernel inversion spreads one matrix over
+// every warp of the CTA, from about 6.
+constexpr int kOrbInvMinPerSM = 24, kOrbInvMinPerSMSmall = 12, kOrbInvMinPerSMOneSpin = 6;
 
 // Whether this handle's next move batches its orbitals and inversion.
 inline bool move_orb_inv(const qmc2d_handle *h) {
   if (h->move_inv_mode == 0) return false;
-  return q2d::orb_inv_pays(h->hs, h->nw, h->nsm, h->move_inv_mode == 2 ? 0 : kOrbInvMinPerSM);
+  const int need = h->move_inv_mode == 2 ? 0
+                   : h->hs.nt == 1       ? kOrbInvMinPerSMOneSpin
+                   : h->hs.nmax <= 16    ? kOrbInvMinPerSMSmall
+                                         : kOrbInvMinPerSM;
+  return q2d::orb_inv_pays(h->hs, h->nw, h->nsm, need);
 }
 
 // Orders the handle's stream after the side copies of the last

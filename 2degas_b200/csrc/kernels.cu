@@ -382,32 +382,39 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
   }
   if (S.has_bf && !S.bf_zero) prefetch_l2(o + L.pair, 3 * (size_t)N * N);
   // the walker's state into shared memory: asynchronous 8-byte copies, all
-  // in flight at once
+  // in flight at once (plain loads in the HBM-determinant instance, whose
+  // register budget they would push into spills)
+  auto ld8 = [&](double *dst, const double *src) {
+    if (kGmat)
+      *dst = *src;
+    else
+      cp_async8(dst, src);
+  };
   for (int j = tid; j < N2; j += kThreads) {
-    cp_async8(v.xo + j, pop.x + (size_t)w * N2 + j);
-    cp_async8(v.go + j, pop.g + (size_t)w * N2 + j);
-    cp_async8(m.x + j, o + L.x + j);
-    cp_async8(m.g + j, o + L.g + j);
-    cp_async8(m.q + j, o + L.q + j);
-    cp_async8(m.qbd + j, o + L.qbd + j);
+    ld8(v.xo + j, pop.x + (size_t)w * N2 + j);
+    ld8(v.go + j, pop.g + (size_t)w * N2 + j);
+    ld8(m.x + j, o + L.x + j);
+    ld8(m.g + j, o + L.g + j);
+    ld8(m.q + j, o + L.q + j);
+    ld8(m.qbd + j, o + L.qbd + j);
     m.gd[j] = 0.0;
   }
-  for (int j = tid; j < 3 * N; j += kThreads) cp_async8(m.Sb + j, o + L.sb + j);
+  for (int j = tid; j < 3 * N; j += kThreads) ld8(m.Sb + j, o + L.sb + j);
   for (int j = tid; j < N; j += kThreads) {
-    cp_async8(m.lap + j, o + L.lap + j);
-    cp_async8(m.ltf + j, o + L.ltf + j);
-    cp_async8(m.vp + j, o + L.vp + j);
+    ld8(m.lap + j, o + L.lap + j);
+    ld8(m.ltf + j, o + L.ltf + j);
+    ld8(m.vp + j, o + L.vp + j);
     m.lapd[j] = 0.0;
     m.ph2[j] = 0.0;
     m.ph2d[j] = 0.0;
   }
   for (int j = tid; j < np; j += kThreads) {
-    cp_async8(v.po + j, pop.p + (size_t)w * np + j);
-    cp_async8(v.blk + j, a.blk + (size_t)w * np + j);
+    ld8(v.po + j, pop.p + (size_t)w * np + j);
+    ld8(v.blk + j, a.blk + (size_t)w * np + j);
   }
-  if (tid < nt) cp_async8(v.ho + tid, pop.h + (size_t)w * nt + tid);
+  if (tid < nt) ld8(v.ho + tid, pop.h + (size_t)w * nt + tid);
   const double wold = o[L.wold];
-  cp_async_wait_all();
+  if (!kGmat) cp_async_wait_all();
   __syncthreads();
   double so = pop.s[w];
   double age = pop.age[w];

@@ -556,7 +556,7 @@ __global__ void __launch_bounds__(G * kThreads, 2 / G) rmc_pairs_kernel(const De
   const int N = S.N, N2 = 2 * N, nb = a.nbuf;
   const uint32_t t = a.step0;
   const double pi = 3.141592653589793;
-  const MoveScratch L = move_scratch(S);
+  const MoveScratch L = move_scratch(S, false);
   for (int r = blockIdx.x * G + grp; r < a.nrep; r += gridDim.x * G) {
     int idir, ndelta;
     rmc_dir(a, r, t, idir, ndelta);
@@ -635,7 +635,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_det_kernel(const DevSys *sp, 
   rmc_dir(a, r, t, idir, ndelta);
   if (idelta > ndelta) return;  // the whole CTA
   const int N = S.N, N2 = 2 * N, nb = a.nbuf;
-  const MoveScratch L = move_scratch(S);
+  const MoveScratch L = move_scratch(S, false);
   const double *o = scr + (size_t)r * L.stride;
   const bool pairs_stored = S.has_bf && !S.bf_zero;
   if (pairs_stored) {

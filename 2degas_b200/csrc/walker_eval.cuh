@@ -270,7 +270,10 @@ __host__ __device__ inline size_t inv_spin_doubles(int n) {
 __host__ __device__ inline bool orb_inv_fits(const DevSys &s) {
   return s.has_bf && !s.gmat && s.nmax > 0 && s.nmax <= 32;
 }
-__host__ __device__ inline MoveScratch move_scratch(const DevSys &s) {
+// with_inv: the layout of VMC/DMC moves, which may batch their inversion;
+// reptation's kernels never do and lay their blocks out without that region
+// (the same allocation holds them, closer together).
+__host__ __device__ inline MoveScratch move_scratch(const DevSys &s, bool with_inv = true) {
   const int N = s.N;
   MoveScratch l;
   l.x = 0;
@@ -288,7 +291,7 @@ __host__ __device__ inline MoveScratch move_scratch(const DevSys &s) {
   l.pair = (14 * N + 3 + 4 * (s.nk > 0 ? s.nk : 1) + 3) & ~3;
   size_t end = (size_t)l.pair + (s.has_bf ? 3 * (size_t)N * N : 0);
   l.inv = 0;
-  if (orb_inv_fits(s)) {
+  if (with_inv && orb_inv_fits(s)) {
     end = (end + 1) & ~size_t(1);
     l.inv = end;
     for (int sp = 0; sp < s.nt; sp++) end += inv_spin_doubles(s.np[sp]);
@@ -1480,7 +1483,9 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
   const int tid = threadIdx.x;
   // rho_k of both slots: copied when given (MoveScratch), else summed
   auto rhok = [&](int t0, int nthr) {
-    if (rhok_in) {
+    if (rhok_in && kGmat) {  // plain loads: the HBM-determinant instance's registers are full
+      for (int e = t0; e < 4 * S.nk; e += nthr) m.rhok[e] = rhok_in[e];
+    } else if (rhok_in) {
       for (int e = t0; e < 4 * S.nk; e += nthr) cp_async8(m.rhok + e, rhok_in + e);
       cp_async_wait_all();
     } else {

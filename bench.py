@@ -1087,6 +1087,8 @@ def batch_arm(args, rank, world):
     for h, (_, _, rs) in zip(handles, specs):
         h.vmc(args.equil, 0.05 * rs * rs, 10 ** 9)
         h.autotune()
+        if args.move_inversion is not None:
+            h.set_move_inversion(args.move_inversion)
     et = []
     for h, t in zip(handles, taus):
         h.block_reset()
