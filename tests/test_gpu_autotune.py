@@ -58,6 +58,18 @@ def test_autotune_picks_a_choice_and_changes_nothing(q, n26, n26_configs):
         assert np.allclose(got["p"], ref["p"], rtol=1e-10, atol=1e-12)
 
 
+def test_autotune_scope_keeps_the_choices_outside_it(q, n26, n26_configs):
+    with q.Handle(n26, capacity=len(n26_configs), seed=4) as h:
+        h.population_set(n26_configs)
+        h.set_pair_lanes(16)
+        h.set_inversion(1)
+        h.set_autotune_scope(1)  # the walker groups and staging only
+        h.autotune()
+        assert h.get_pair_lanes() == 16 and h.get_launch()[2] == 1
+        with pytest.raises(q.QMCError):
+            h.set_autotune_scope(8)
+
+
 def test_set_launch_rejects_bad_choices(q, n26, n26_configs):
     with q.Handle(n26, capacity=4, seed=1) as h:
         with pytest.raises(q.QMCError):
@@ -68,3 +80,5 @@ def test_set_launch_rejects_bad_choices(q, n26, n26_configs):
             with pytest.raises(q.QMCError):
                 h.set_pair_lanes(bad)
         assert h.get_pair_lanes() == 8
+        with pytest.raises(q.QMCError):
+            h.set_move_inversion(3)

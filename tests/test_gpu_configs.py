@@ -14,7 +14,10 @@ paths the n26 deck does not reach:
 
 Each case checks compute_properties on fresh configurations (1e-10, as the
 n26 tests) and three VMC steps against the oracle's replay of the same
-Philox streams."""
+Philox streams, with the moves' orbitals and inversion inside the move
+kernel and, forced (qmc2d_set_move_inversion mode 2), in orb_inv_kernel
+(its 16-column instance for n26_u3_fine, the 29-column one for n58_bf and
+pol25_bf; n74_bf does not fit it and stays in the move kernel)."""
 import importlib
 import os
 
@@ -69,7 +72,8 @@ def test_evaluation_parity(q, oracle_cls, deck):
         assert sg[k] == so, f"{name}: sign, config {k}"
 
 
-def test_vmc_parity(q, oracle_cls, deck):
+@pytest.mark.parametrize("move_inv", [0, 2])
+def test_vmc_parity(q, oracle_cls, deck, move_inv):
     name, s, x = deck
     nw, nstp = len(x), 3
     delta = 0.02 * CASES[name]["rs"] ** 2
@@ -77,7 +81,9 @@ def test_vmc_parity(q, oracle_cls, deck):
     pop = o.population_init(x)
     blk_o, nacc_o = o.vmc_philox(pop, nstp, delta, 1000, SEED, 0)
     with q.Handle(s, capacity=nw, seed=SEED) as h:
+        h.set_move_inversion(move_inv)
         h.population_set(x)
+        assert h.get_move_inversion() == (move_inv == 2 and name != "n74_bf")
         h.block_reset()
         h.vmc(nstp, delta, 1000)
         got = h.population_get()

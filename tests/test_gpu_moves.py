@@ -65,8 +65,8 @@ def test_vmc_forced_moves(q, oracle_cls, n26, n26_configs):
     assert rel(got["x"], pop["x"]) < 1e-11
 
 
-@pytest.mark.parametrize("lanes", [8, 4, 16])
-def test_dmc_generations(q, oracle_cls, n26, n26_configs, lanes):
+@pytest.mark.parametrize("lanes,move_inv", [(8, 1), (4, 1), (16, 1), (8, 2)])
+def test_dmc_generations(q, oracle_cls, n26, n26_configs, lanes, move_inv):
     nw, ngen, mmstep, delta = 32, 3, 2, 0.05
     etrial, mmult, mage = -0.43, 5.0, 1000
     x0 = n26_configs[:nw]
@@ -75,6 +75,7 @@ def test_dmc_generations(q, oracle_cls, n26, n26_configs, lanes):
     blk_o, norm_o, _ = o.dmc_philox(pop, ngen, mmstep, delta, etrial, mmult, mage, SEED)
     with q.Handle(n26, capacity=nw, seed=SEED) as h:
         h.set_pair_lanes(lanes)  # lanes per particle of the pair passes
+        h.set_move_inversion(move_inv)  # 2: orbitals and inversion in orb_inv_kernel
         h.population_set(x0)
         h.block_reset()
         h.dmc(ngen, mmstep, delta, etrial, mmult, mage)
