@@ -47,15 +47,15 @@ import numpy as np  # noqa: E402
 CONFIG = "dmc_bf_n58_rs5"
 METRIC = "walker-moves/sec (DMC with backflow, N=58 r_s=5, 4096 walkers)"
 UNIT = "walker-moves/s"
-# DRAM bytes read per walker by one pairs_kernel + move_kernel pair of
-# launches, from the ncu capture summarised in
+# DRAM bytes read per walker by one pairs_kernel + orb_inv_kernel +
+# move_kernel generation, from the ncu capture summarised in
 # profiles/move_kernels_dmc_bf_n58_296w.md (296 walkers, scaled linearly: the
-# walker records and the move scratch), plus the move scratch block the pair
-# kernel writes, which reaches DRAM at 4096 walkers (356 MB > L2) though not
-# in the 296-walker capture.
-MOVE_DRAM_READ_PER_WALKER = (1.086976e6 + 28.344320e6) / 296
-TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum of pairs_kernel + move_kernel (296 walkers) "
-                  "x walkers/296, + the move scratch written per walker")
+# walker records and the move scratch, read cold in ncu's replays), plus the
+# move scratch block the pair and orbital kernels write, which reaches DRAM at
+# 4096 walkers (the blocks exceed L2) though not in the 296-walker capture.
+MOVE_DRAM_READ_PER_WALKER = (1.010176e6 + 0.476416e6 + 44.548096e6) / 296
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum of pairs_kernel + orb_inv_kernel + move_kernel "
+                  "(296 walkers) x walkers/296, + the move scratch written per walker")
 
 
 def move_scratch_bytes(N, nk, ns=()):
