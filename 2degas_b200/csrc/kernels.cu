@@ -227,12 +227,19 @@ size_t move_scratch_doubles(const DevSys &hs) { return move_scratch(hs).stride; 
 // 9338), lane k holding row k in registers: the pivot key is the top word
 // of |re|+|im| with 255 - row in its low byte (one redux per step), the
 // pivot row reaches the other lanes through shared memory, and every lane
-// updates its row, the next pivot column first. Outputs, as gj_invert_reg:
-// W(pi(k), c) = A^-1(k, pi(c)) with the pivot rows unscaled until the end,
-// perm, |pivot|^2 and the singular flag, into the walker's move scratch,
-// where move_kernel reads them instead of inverting. No block barrier after
-// the DevSys load: each warp works alone, many per scheduler, so one
-// matrix's pivot chain hides behind the others' updates.
+// updates its row. The row is held rotated: at step k register j holds
+// column (k + j) mod NM, so the pivot column is always register 0, each
+// update writes its result one register down (no moves) and the eliminated
+// column enters at register NM - 1; after NM steps the columns are back in
+// place. The step loop is therefore not unrolled and its code stays in the
+// instruction cache. A spin with n < NM orbitals is padded to NM with
+// identity rows, whose steps k >= n pivot on row k and leave rows < n
+// unchanged. Outputs, as gj_invert_reg: W(pi(k), c) = A^-1(k, pi(c)) with
+// the pivot rows unscaled until the end, perm, |pivot|^2 and the singular
+// flag, into the walker's move scratch, where move_kernel reads them
+// instead of inverting. No block barrier after the DevSys load: each warp
+// works alone, many per scheduler, so one matrix's pivot chain hides
+// behind the others' updates.
 constexpr int kOrbWarps = 4;  // warps (spin matrices) per CTA
 
 __host__ __device__ inline size_t orb_inv_warp_doubles(int n) {
@@ -242,6 +249,7 @@ __host__ __device__ inline size_t orb_inv_warp_doubles(int n) {
 
 template <int NM>
 __global__ void __launch_bounds__(32 * kOrbWarps) orb_inv_kernel(const DevSys *sp, MoveArgs a) {
+  static_assert(NM <= 32, "one lane per row");
   __shared__ DevSys S;
   extern __shared__ __align__(16) char smem[];
   load_sys(S, sp);
@@ -266,7 +274,7 @@ __global__ void __launch_bounds__(32 * kOrbWarps) orb_inv_kernel(const DevSys *s
   double *outS = outP + n;
   for (int e = lane; e < 2 * n; e += 32) qs[e] = o[L.q + 2 * f0 + e];
   __syncwarp();
-  // orbitals: lane r is orbital r
+  // orbitals: lane r is orbital r; rows n .. NM-1 are identity rows
   const double gx = r < n ? __ldg(S.gvec + 2 * r) : 0.0, gy = r < n ? __ldg(S.gvec + 2 * r + 1) : 0.0;
   double2 v[NM];
 #pragma unroll
@@ -275,7 +283,7 @@ __global__ void __launch_bounds__(32 * kOrbWarps) orb_inv_kernel(const DevSys *s
     const double kr = on ? qs[2 * j] * gx + qs[2 * j + 1] * gy : 0.0;
     double sv, cv;
     sincos(kr, &sv, &cv);
-    v[j] = on ? make_double2(cv, sv) : make_double2(0.0, 0.0);
+    v[j] = on ? make_double2(cv, sv) : make_double2(r == j ? 1.0 : 0.0, 0.0);
   }
   // A, column-major (A[k + j n]): for each j the lanes write consecutive k
   if (r < n)
@@ -286,48 +294,45 @@ __global__ void __launch_bounds__(32 * kOrbWarps) orb_inv_kernel(const DevSys *s
   double2 my_inv = make_double2(1.0, 0.0);
   int my_perm = 0, sing = 0;
   double my_dk = 0.0;
-#pragma unroll
+#pragma unroll 1
   for (int k = 0; k < NM; k++) {
-    if (k >= n) break;
-    const double av = fabs(v[k].x) + fabs(v[k].y);
-    const unsigned key =
-        used ? 0u : ((unsigned)__double2hiint(av) & ~0xFFu) | (unsigned)(255 - r);
-    const unsigned best = __reduce_max_sync(0xffffffffu, key);
-    // Every unused row's key has 255 - r in its low byte, so p is an unused
-    // row < n at every step, an exactly zero or NaN column included.
-    const int p = 255 - (int)(best & 0xFFu);
-    sing |= (best >> 8) == 0u;  // every candidate zero (or subnormal)
+    int p = k;  // an identity row's own step
+    if (k < n) {
+      const double av = fabs(v[0].x) + fabs(v[0].y);
+      const unsigned key =
+          used ? 0u : ((unsigned)__double2hiint(av) & ~0xFFu) | (unsigned)(255 - r);
+      const unsigned best = __reduce_max_sync(0xffffffffu, key);
+      // Every unused row's key has 255 - r in its low byte, so p is an
+      // unused row < n at every step, an exactly zero or NaN column included.
+      p = 255 - (int)(best & 0xFFu);
+      sing |= (best >> 8) == 0u;  // every candidate zero (or subnormal)
+    }
     double2 *pr = prow + (k & 1) * 32;
     if (r == p)
 #pragma unroll
       for (int c = 0; c < NM; c++) pr[c] = v[c];
     __syncwarp();
-    const double2 piv = pr[k];
+    const double2 piv = pr[0];
     const double d = piv.x * piv.x + piv.y * piv.y;
     const double rd = rcp_newton(d);
     const double2 inv = make_double2(piv.x * rd, -piv.y * rd);
-    if (lane == k) {
+    if (lane == k && k < n) {
       my_perm = p;
       my_dk = d;
     }
     const bool isp = r == p;
     used = used || isp;
     if (isp) my_inv = inv;
-    double2 fac = cmul(v[k], inv);
+    double2 fac = cmul(v[0], inv);
     if (isp || r >= n) fac = make_double2(0.0, 0.0);
-    if (k + 1 < NM) {  // the next pivot column first
-      const double2 b = pr[k + 1];
-      v[k + 1].x = fma(-fac.x, b.x, fma(fac.y, b.y, v[k + 1].x));
-      v[k + 1].y = fma(-fac.x, b.y, fma(-fac.y, b.x, v[k + 1].y));
-    }
+    // register j - 1 <- column (k + j) mod NM, the next pivot column first
 #pragma unroll
-    for (int c = 0; c < NM; c++) {
-      if (c == k + 1) continue;
-      const double2 b = pr[c];
-      v[c].x = fma(-fac.x, b.x, fma(fac.y, b.y, v[c].x));
-      v[c].y = fma(-fac.x, b.y, fma(-fac.y, b.x, v[c].y));
+    for (int j = 1; j < NM; j++) {
+      const double2 b = pr[j];
+      v[j - 1].x = fma(-fac.x, b.x, fma(fac.y, b.y, v[j].x));
+      v[j - 1].y = fma(-fac.x, b.y, fma(-fac.y, b.x, v[j].y));
     }
-    v[k] = isp ? make_double2(1.0, 0.0) : make_double2(-fac.x, -fac.y);
+    v[NM - 1] = isp ? make_double2(1.0, 0.0) : make_double2(-fac.x, -fac.y);
   }
   // rows normalised by their own pivot, out through shared memory so the
   // scratch writes are consecutive
@@ -817,9 +822,15 @@ cudaError_t launch_orb_inv(const DevSys &hs, const DevSys *ds, const MoveArgs &a
   for (int t = 0; t < hs.nt; t++) wd = std::max(wd, orb_inv_warp_doubles(hs.np[t]));
   const size_t sm = sizeof(double) * wd * kOrbWarps;
   const int items = a.nw * hs.nt, grid = (items + kOrbWarps - 1) / kOrbWarps;
-  // registers for the rows: 16, 29 (N = 58, the benchmark shell) or 32 columns
-  auto k = hs.nmax <= 16 ? orb_inv_kernel<16>
-                         : (hs.nmax <= 29 ? orb_inv_kernel<29> : orb_inv_kernel<32>);
+  // registers for the rows: the closed shells' sizes 13, 21, 25, 29 (N = 58,
+  // the benchmark shell) exactly, others padded to 16 or 32 columns
+  const int nm = hs.nmax;
+  auto k = nm <= 13   ? orb_inv_kernel<13>
+           : nm <= 16 ? orb_inv_kernel<16>
+           : nm <= 21 ? orb_inv_kernel<21>
+           : nm <= 25 ? orb_inv_kernel<25>
+           : nm <= 29 ? orb_inv_kernel<29>
+                      : orb_inv_kernel<32>;
   cudaError_t e = set_smem((const void *)k, sm);
   if (e != cudaSuccess) return e;
   k<<<grid, 32 * kOrbWarps, sm, st>>>(ds, a);

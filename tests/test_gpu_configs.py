@@ -10,14 +10,17 @@ paths the n26 deck does not reach:
   eight warps on one spin;
 - n26_u3_fine: u2 + u3 + backflow on 6001-knot tables, whose pair rows
   (864 KB) do not fit in shared memory: the pair kernel reads them from
-  global memory.
+  global memory;
+- n22_mixed: 13 + 9, spins of different sizes: orb_inv_kernel's 13-column
+  instance pads the 9-orbital spin with four identity rows.
 
 Each case checks compute_properties on fresh configurations (1e-10, as the
 n26 tests) and three VMC steps against the oracle's replay of the same
 Philox streams, with the moves' orbitals and inversion inside the move
 kernel and, forced (qmc2d_set_move_inversion mode 2), in orb_inv_kernel
-(its 16-column instance for n26_u3_fine, the 29-column one for n58_bf and
-pol25_bf; n74_bf does not fit it and stays in the move kernel)."""
+(its 13-column instance for n26_u3_fine and n22_mixed, the 25-column one
+for pol25_bf, the 29-column one for n58_bf; n74_bf does not fit it and
+stays in the move kernel)."""
 import importlib
 import os
 
@@ -35,6 +38,7 @@ CASES = {
     "pol25_bf": dict(n_up=25, n_down=0, rs=3.0, backflow=(0.2, 3.0, 2.0)),
     "n26_u3_fine": dict(n_up=13, n_down=13, rs=10.0, backflow=(0.2, 10.0, 6.0), u3=True,
                         nknots=6000),
+    "n22_mixed": dict(n_up=13, n_down=9, rs=5.0, backflow=(0.2, 5.0, 3.0)),
 }
 
 
