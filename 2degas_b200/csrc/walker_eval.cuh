@@ -1931,8 +1931,12 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
   bool underflow = false;
   if (S.has_bf && S.ref_underflow) underflow = exp(-ltf * 2.0) <= 0.0;
   if (underflow) status |= ST_UNDERFLOW;
-  // determinant terms and the drift cutoff (kinetic, reptation.f:2748-2763)
-  double gga = 0.0;
+  // determinant terms and the drift cutoff (kinetic, reptation.f:2748-2763),
+  // and on the way the per-type sums: Laplacian, |g|^2, pair potential,
+  // phase gradient^2 (register arrays with compile-time indices only:
+  // nt <= 2), the drift cutoff factors, and the k-space sums of every type
+  // pair (reptation.f:4034-4052), all in one block reduction
+  double sums[13] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int i = tid; i < N; i += kThreads) {
     double gx = m.g[2 * i], gy = m.g[2 * i + 1], lp = m.lap[i], ph = 0.0;
     if (S.has_bf && !underflow) {
@@ -1942,12 +1946,12 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
       ph = m.ph2d[i];
     }
     double x2 = gx * gx + gy * gy;
+    const int ti = type_of(S, i);
     if (S.adrift != 0.0) {
-      int ti = type_of(S, i);
       double vari = 1.0 / (2.0 * S.hbs2m[ti] * S.delta);
       double gg = x2 * S.adrift * S.delta * S.delta * vari;
       gg = (-1.0 + sqrt(1.0 + 2.0 * gg)) / gg;
-      gga += gg;
+      sums[8] += gg;
       gx *= gg;
       gy *= gg;
     }
@@ -1956,24 +1960,44 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
     m.lap[i] = lp;
     m.ph2[i] = ph;
     m.ph2d[i] = x2;  // |g|^2 before the cutoff, for the kinetic energy
-  }
-  __syncthreads();
-  // per-type sums: Laplacian, |g|^2, pair potential, phase gradient^2
-  // (register arrays with compile-time indices only: nt <= 2)
-  double sums[9] = {0, 0, 0, 0, 0, 0, 0, 0, gga};
-  for (int i = tid; i < N; i += kThreads) {
-    const bool t1 = type_of(S, i) == 1;
-    const double l = m.lap[i], g2 = m.ph2d[i], v = m.vp[i], p = m.ph2[i];
-    sums[0] += t1 ? 0.0 : l;
-    sums[1] += t1 ? 0.0 : g2;
+    const bool t1 = ti == 1;
+    const double v = m.vp[i];
+    sums[0] += t1 ? 0.0 : lp;
+    sums[1] += t1 ? 0.0 : x2;
     sums[2] += t1 ? 0.0 : v;
-    sums[3] += t1 ? 0.0 : p;
-    sums[4] += t1 ? l : 0.0;
-    sums[5] += t1 ? g2 : 0.0;
+    sums[3] += t1 ? 0.0 : ph;
+    sums[4] += t1 ? lp : 0.0;
+    sums[5] += t1 ? x2 : 0.0;
     sums[6] += t1 ? v : 0.0;
-    sums[7] += t1 ? p : 0.0;
+    sums[7] += t1 ? ph : 0.0;
   }
-  block_sum_n<9>(sums, m.red);
+  {
+    // every type pair in one loop, so the four v_k loads of a k are in
+    // flight together (the sums keep their order: k ascending per thread)
+    int nkp[4], nkmax = 0;
+    const double *vkp[4];
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const int it = p >> 1, jt = p & 1;
+      const int iv = (it < nt && jt < nt) ? S.iv2[it][jt] : -1;
+      nkp[p] = iv >= 0 ? S.tab_nkew[iv] : 0;
+      vkp[p] = S.coef + (iv >= 0 ? S.tab_vkoff[iv] : 0);
+      nkmax = max(nkmax, nkp[p]);
+    }
+    for (int k = tid; k < nkmax; k += kThreads) {
+      double vk[4];
+#pragma unroll
+      for (int p = 0; p < 4; p++) vk[p] = k < nkp[p] ? __ldg(vkp[p] + k) : 0.0;
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        const int it = p >> 1, jt = p & 1;
+        if (k < nkp[p])
+          sums[9 + p] += vk[p] * (m.rhok[2 * (it * S.nk + k)] * m.rhok[2 * (jt * S.nk + k)] +
+                                  m.rhok[2 * (it * S.nk + k) + 1] * m.rhok[2 * (jt * S.nk + k) + 1]);
+      }
+    }
+  }
+  block_sum_n<13>(sums, m.red);
   double kin0 = 0.0, pot0 = 0.0, efp = 0.0;
   double kin_t[2] = {0, 0}, un_t[2] = {0, 0}, pot_t[2] = {0, 0};
 #pragma unroll
@@ -2006,46 +2030,18 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
     }
   }
   pot0 = pot_t[0] + pot_t[1];
-  // k space (reptation.f:4034-4052): rho_k read by type index
-  {
-    // every type pair in one loop, so the four v_k loads of a k are in
-    // flight together (the sums keep their order: k ascending per thread)
-    double ks[4] = {0, 0, 0, 0};
-    int nkp[4], nkmax = 0;
-    const double *vkp[4];
+  // k space (reptation.f:4034-4052): the type pairs' sums from above
 #pragma unroll
-    for (int p = 0; p < 4; p++) {
-      const int it = p >> 1, jt = p & 1;
-      const int iv = (it < nt && jt < nt) ? S.iv2[it][jt] : -1;
-      nkp[p] = iv >= 0 ? S.tab_nkew[iv] : 0;
-      vkp[p] = S.coef + (iv >= 0 ? S.tab_vkoff[iv] : 0);
-      nkmax = max(nkmax, nkp[p]);
+  for (int it = 0; it < 2; it++)
+#pragma unroll
+    for (int jt = 0; jt < 2; jt++) {
+      if (it >= nt || jt >= nt) continue;
+      int iv = S.iv2[it][jt];
+      if (iv < 0 || S.tab_nkew[iv] == 0) continue;
+      double c = sums[9 + 2 * it + jt] + S.tab_kself[iv] * S.npnorm;
+      pot_t[it] += c;
+      pot0 += c;
     }
-    for (int k = tid; k < nkmax; k += kThreads) {
-      double vk[4];
-#pragma unroll
-      for (int p = 0; p < 4; p++) vk[p] = k < nkp[p] ? __ldg(vkp[p] + k) : 0.0;
-#pragma unroll
-      for (int p = 0; p < 4; p++) {
-        const int it = p >> 1, jt = p & 1;
-        if (k < nkp[p])
-          ks[p] += vk[p] * (m.rhok[2 * (it * S.nk + k)] * m.rhok[2 * (jt * S.nk + k)] +
-                            m.rhok[2 * (it * S.nk + k) + 1] * m.rhok[2 * (jt * S.nk + k) + 1]);
-      }
-    }
-    block_sum_n<4>(ks, m.red);
-#pragma unroll
-    for (int it = 0; it < 2; it++)
-#pragma unroll
-      for (int jt = 0; jt < 2; jt++) {
-        if (it >= nt || jt >= nt) continue;
-        int iv = S.iv2[it][jt];
-        if (iv < 0 || S.tab_nkew[iv] == 0) continue;
-        double c = ks[2 * it + jt] + S.tab_kself[iv] * S.npnorm;
-        pot_t[it] += c;
-        pot0 += c;
-      }
-  }
   pot0 = (pot0 + S.v0) / S.npnorm;
   efp = S.ntheta != 0 ? efp / S.npnorm : 0.0;
   if (tid == 0) {
@@ -2067,7 +2063,6 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
     props[QMC2D_JETOT] = et;
     props[QMC2D_JE2] = et * et;
     *sign = 1.0;
-    m.red[0] = et;  // for every thread's finiteness check (red is free here)
   }
   // rho_k properties (compute_properties, reptation.f:2672-2683)
   {
@@ -2079,9 +2074,8 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
       cnt += 2 * S.nk;
     }
   }
-  __syncthreads();
-  const double et = m.red[0];
-  if (!isfinite(et) || !isfinite(ltf)) status |= ST_NONFINITE;
+  // every thread holds the same sums, so the same total energy
+  if (!isfinite(pot0 + kin0 + efp) || !isfinite(ltf)) status |= ST_NONFINITE;
   __syncthreads();
   phase_mark(S, PH_ASSEMBLE, tph);
   return status;
