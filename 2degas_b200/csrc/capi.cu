@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -114,6 +115,30 @@ int build_devsys(const qmc2d_system *sys, q2d::DevSys *hs, std::vector<double> *
   for (int d = 0; d < 2; d++) {
     s.el[d] = sys->el[d];
     s.eli[d] = sys->eli[d];
+  }
+  // rho_k from lattice power tables (DevSys::rk_lat) when every k vector is
+  // 2 pi n / L per axis to 1e-14 and the tables stay small
+  if (sys->nk > 0 && sys->kvec) {
+    const double twopi = 6.283185307179586;
+    bool lat = true;
+    int pmax[2] = {0, 0};
+    for (int k = 0; k < sys->nk && lat; k++)
+      for (int d = 0; d < 2; d++) {
+        const double kv = sys->kvec[2 * k + d], unit = twopi / sys->el[d];
+        const double a = kv / unit;
+        const long n = std::lround(a);
+        if (!(std::fabs(a) < 64.0) || std::fabs(kv - n * unit) > 1e-14 * std::max(std::fabs(kv), unit)) {
+          lat = false;
+          break;
+        }
+        pmax[d] = std::max(pmax[d], (int)std::labs(n));
+      }
+    const size_t tbytes = sizeof(double) * 2 * (pmax[0] + pmax[1] + 2) * (size_t)sys->nptot;
+    if (lat && tbytes <= 48 * 1024) {
+      s.rk_lat = 1;
+      s.rk_p1 = pmax[0];
+      s.rk_p2 = pmax[1];
+    }
   }
   s.drt = sys->drt;
   s.drti = sys->drti;

@@ -75,6 +75,11 @@ struct DevSys {
   // terms and the determinant's drift and Laplacian come from the diagonals
   // of F and D2 without the cross-term GEMM.
   int bf_zero;
+  // Every Ewald k vector on the reciprocal lattice, k = 2 pi (n1 / Lx,
+  // n2 / Ly) to 1e-14 (set by the handle; |n1| <= rk_p1, |n2| <= rk_p2): the
+  // pair kernels form rho_k from per-particle tables of exp(2 pi i p x / L)
+  // instead of a sincos per (k, particle).
+  int rk_lat, rk_p1, rk_p2;
   // Determinants too large for one CTA's shared memory (gmat = 1): the
   // orbital, inversion, F and cross-term matrices of walker (CTA) b live at
   // gmat_base + b * gmat_stride (doubles) in global memory; everything

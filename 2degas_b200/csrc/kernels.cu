@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(G * kThreads, 2 / G) pairs_kernel(const DevSys
                                                    tid);
     else
       eval_pairs<kThreads, false, R, GroupSync, LG>(S, m, tph, pout, rows_g, sync, tid);
-    compute_rhok<LG>(S, m, tid, kThreads);
+    pair_rhok<LG>(S, m, tid, kThreads, sync);
     sync();
     for (int j = tid; j < 4 * S.nk; j += kThreads) o[L.rhok + j] = m.rhok[j];
     for (int j = tid; j < N2; j += kThreads) {

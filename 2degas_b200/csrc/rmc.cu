@@ -589,7 +589,7 @@ __global__ void __launch_bounds__(G * kThreads, 2 / G) rmc_pairs_kernel(const De
                                                    tid);
     else
       eval_pairs<kThreads, false, R, GroupSync, LG>(S, m, tph, pout, rows_g, sync, tid);
-    compute_rhok<LG>(S, m, tid, kThreads);
+    pair_rhok<LG>(S, m, tid, kThreads, sync);
     sync();
     for (int e = tid; e < 4 * S.nk; e += kThreads) o[L.rhok + e] = m.rhok[e];
     for (int e = tid; e < N2; e += kThreads) {

@@ -53,6 +53,9 @@ struct EvalSmem {
   // multipliers, scaled pivot rows, pivot reciprocals and rows (inside the
   // F0 region, like gslot/gkey)
   double2 *pscr[2];
+  // lattice power tables of rho_k in the pair kernels (DevSys::rk_lat):
+  // exp(2 pi i p x_i / Lx) at [p N + i], p <= rk_p1, then exp(2 pi i p y_i / Ly)
+  double2 *rkt = nullptr;
 };
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
@@ -240,6 +243,7 @@ __host__ __device__ inline size_t pair_carve(const DevSys &s, char *base, EvalSm
   t.ph2d = (double *)take(sizeof(double) * N);
   t.rhok = (double *)take(sizeof(double) * 2 * (s.nk > 0 ? s.nk : 1) * 2);
   t.red = (double *)take(sizeof(double) * nthreads);
+  t.rkt = s.rk_lat ? (double2 *)take(sizeof(double2) * (s.rk_p1 + s.rk_p2 + 2) * N) : nullptr;
   if (m) *m = t;
   return off;
 }
@@ -1243,6 +1247,76 @@ __device__ inline void compute_rhok(const DevSys &S, const EvalSmem &m, int t, i
       m.rhok[2 * (slot * S.nk + k) + 1] = sn;
     }
   }
+}
+
+// rho_k of the pair kernels when every k vector is on the reciprocal lattice
+// (DevSys::rk_lat): with k = 2 pi (n1 / Lx, n2 / Ly), exp(i k.x) =
+// X_{n1}(x) Y_{n2}(y), X_p(x) = exp(2 pi i p x / Lx), and each particle's
+// X_0 .. X_{rk_p1}, Y_0 .. Y_{rk_p2} are built once by repeated complex
+// multiplication (conjugates for negative indices), so a (k, particle) term
+// is one complex product instead of a sincos. Items, lanes and the shuffle
+// tree as compute_rhok; each term agrees with its sincos to a few ulp.
+// Threads t .. t+nthr-1 of the group whose barrier is sync.
+template <int LG, class Sync>
+__device__ inline void compute_rhok_lattice(const DevSys &S, const EvalSmem &m, int t, int nthr,
+                                            Sync sync) {
+  const int N = S.N, P1 = S.rk_p1, P2 = S.rk_p2;
+  double2 *X = m.rkt, *Y = m.rkt + (size_t)(P1 + 1) * N;
+  for (int i = t; i < N; i += nthr) {
+    double sx, cx, sy, cy;
+    sincospi(2.0 * (m.x[2 * i] * S.eli[0]), &sx, &cx);
+    sincospi(2.0 * (m.x[2 * i + 1] * S.eli[1]), &sy, &cy);
+    const double2 bx = make_double2(cx, sx), by = make_double2(cy, sy);
+    double2 px = make_double2(1.0, 0.0), py = px;
+    X[i] = px;
+    Y[i] = py;
+    for (int p = 1; p <= P1; p++) {
+      px = cmul(px, bx);
+      X[(size_t)p * N + i] = px;
+    }
+    for (int p = 1; p <= P2; p++) {
+      py = cmul(py, by);
+      Y[(size_t)p * N + i] = py;
+    }
+  }
+  sync();
+  const double c1 = S.el[0] * 0.15915494309189535, c2 = S.el[1] * 0.15915494309189535;
+  const int total = S.nt * S.nk, per_round = nthr / LG, l8 = t & (LG - 1);
+  for (int e0 = 0; e0 < total; e0 += per_round) {
+    const int e = e0 + t / LG;
+    const int ty = e < total ? e / S.nk : 0, k = e - ty * S.nk;
+    const bool on = e < total && S.irhok[ty] != 0;
+    double c = 0.0, sn = 0.0;
+    if (on) {
+      const int n1 = __double2int_rn(__ldg(S.kvec + 2 * k) * c1);
+      const int n2 = __double2int_rn(__ldg(S.kvec + 2 * k + 1) * c2);
+      const double2 *xp = X + (size_t)abs(n1) * N, *yp = Y + (size_t)abs(n2) * N;
+      for (int i = S.ipfrst[ty] + l8; i < S.ipfrst[ty] + S.np[ty]; i += LG) {
+        double2 xv = xp[i], yv = yp[i];
+        if (n1 < 0) xv.y = -xv.y;
+        if (n2 < 0) yv.y = -yv.y;
+        c += xv.x * yv.x - xv.y * yv.y;
+        sn += xv.x * yv.y + xv.y * yv.x;
+      }
+    }
+    c = group_sum<LG>(c);
+    sn = group_sum<LG>(sn);
+    if (on && l8 == 0) {
+      const int slot = S.irhok[ty] - 1;
+      m.rhok[2 * (slot * S.nk + k)] = c;
+      m.rhok[2 * (slot * S.nk + k) + 1] = sn;
+    }
+  }
+}
+
+// rho_k in a pair kernel: from the lattice tables when the group's shared
+// memory has them, else one sincos per (k, particle).
+template <int LG, class Sync>
+__device__ inline void pair_rhok(const DevSys &S, const EvalSmem &m, int t, int nthr, Sync sync) {
+  if (m.rkt)
+    compute_rhok_lattice<LG>(S, m, t, nthr, sync);
+  else
+    compute_rhok<LG>(S, m, t, nthr);
 }
 
 // ---------------------------------------------------------- the evaluation
