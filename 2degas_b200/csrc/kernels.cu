@@ -100,7 +100,11 @@ struct MoveSmem {
   double *xo, *go, *po, *pn, *blk, *ho, *hn, *sc;
 };
 
-__host__ __device__ inline size_t move_carve(const DevSys &s, char *base, MoveSmem *m) {
+// props_in_buf (the one-buffer move kernel): po, pn and blk are placed by
+// the kernel in the orbital buffer, which is free once the determinants
+// are done (props_buf_fits).
+__host__ __device__ inline size_t move_carve(const DevSys &s, char *base, MoveSmem *m,
+                                             bool props_in_buf = false) {
   size_t off = 0;
   auto take = [&](size_t bytes) -> char * {
     char *p = base ? base + off : nullptr;
@@ -110,9 +114,12 @@ __host__ __device__ inline size_t move_carve(const DevSys &s, char *base, MoveSm
   MoveSmem t;
   t.xo = (double *)take(sizeof(double) * 2 * s.N);
   t.go = (double *)take(sizeof(double) * 2 * s.N);
-  t.po = (double *)take(sizeof(double) * s.nprops);
-  t.pn = (double *)take(sizeof(double) * s.nprops);
-  t.blk = (double *)take(sizeof(double) * s.nprops);
+  t.po = t.pn = t.blk = nullptr;
+  if (!props_in_buf) {
+    t.po = (double *)take(sizeof(double) * s.nprops);
+    t.pn = (double *)take(sizeof(double) * s.nprops);
+    t.blk = (double *)take(sizeof(double) * s.nprops);
+  }
   t.ho = (double *)take(sizeof(double) * 2);
   t.hn = (double *)take(sizeof(double) * 2);
   t.sc = (double *)take(sizeof(double) * 8);
@@ -122,6 +129,22 @@ __host__ __device__ inline size_t move_carve(const DevSys &s, char *base, MoveSm
 
 size_t move_smem_bytes(const DevSys &s) {
   return eval_carve(s, nullptr, nullptr) + move_carve(s, nullptr, nullptr);
+}
+
+// The one-buffer move kernel (move_kernel<false, true>): both spins'
+// orbitals and inverses come from orb_inv_kernel and take one shared
+// buffer in turn, and the walker's old, new and accumulated properties use
+// that buffer after the determinants, so three CTAs fit an SM.
+__host__ __device__ inline size_t props_stride(const DevSys &s) { return (s.nprops + 1) & ~1; }
+inline bool props_buf_fits(const DevSys &s) {
+  const int n = s.nmax > 0 ? s.nmax : 1;
+  const size_t awbytes = sizeof(double2) * (n * n + n * ws_ld(n));
+  const size_t mbytes = sizeof(double) * 2 * n * xt_ldm(2 * n);
+  return sizeof(double) * 3 * props_stride(s) <= std::max(awbytes, mbytes);
+}
+size_t move_smem_bytes_seq(const DevSys &s) {
+  return eval_carve(s, nullptr, nullptr, nullptr, nullptr, true) +
+         move_carve(s, nullptr, nullptr, true);
 }
 
 // One move of one walker is two launches. pairs_kernel: the proposal
@@ -350,16 +373,24 @@ __global__ void __launch_bounds__(32 * kOrbWarps) orb_inv_kernel(const DevSys *s
 }
 
 
-template <bool kGmat>
-__global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, DevPop pop,
-                                                           MoveArgs a) {
+// kSeq: the one-buffer form for moves whose orbitals and inverses come from
+// orb_inv_kernel (smaller shared memory, 80 registers: three CTAs per SM).
+template <bool kGmat, bool kSeq>
+__global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevSys *sp, DevPop pop,
+                                                                      MoveArgs a) {
   __shared__ DevSys S;
   extern __shared__ __align__(16) char smem[];
   load_sys(S, sp);
   EvalSmem m;
-  size_t off = eval_carve<kGmat>(S, smem, &m, kGmat ? gmat_block(S, blockIdx.x) : nullptr);
+  size_t off = eval_carve<kGmat>(S, smem, &m, kGmat ? gmat_block(S, blockIdx.x) : nullptr,
+                                 nullptr, kSeq);
   MoveSmem v;
-  move_carve(S, smem + off, &v);
+  move_carve(S, smem + off, &v, kSeq);
+  if (kSeq) {
+    v.pn = reinterpret_cast<double *>(m.A[0]);
+    v.po = v.pn + props_stride(S);
+    v.blk = v.po + props_stride(S);
+  }
   const int w = blockIdx.x, tid = threadIdx.x;
   if (w >= a.nw) return;
   const int N = S.N, N2 = 2 * N, np = S.nprops, nt = S.nt;
@@ -386,6 +417,11 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
     prefetch_l2(o + L.inv, nd);
   }
   if (S.has_bf && !S.bf_zero) prefetch_l2(o + L.pair, 3 * (size_t)N * N);
+  if (kSeq) {  // read after the determinants (from a 16-byte boundary)
+    const size_t e0 = (size_t)w * np, e1 = (e0 + 1) & ~size_t(1);
+    prefetch_l2(pop.p + e1, np - (e1 - e0));
+    prefetch_l2(a.blk + e1, np - (e1 - e0));
+  }
   // the walker's state into shared memory: asynchronous 8-byte copies, all
   // in flight at once (plain loads in the HBM-determinant instance, whose
   // register budget they would push into spills)
@@ -413,10 +449,11 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
     m.ph2[j] = 0.0;
     m.ph2d[j] = 0.0;
   }
-  for (int j = tid; j < np; j += kThreads) {
-    ld8(v.po + j, pop.p + (size_t)w * np + j);
-    ld8(v.blk + j, a.blk + (size_t)w * np + j);
-  }
+  if (!kSeq)
+    for (int j = tid; j < np; j += kThreads) {
+      ld8(v.po + j, pop.p + (size_t)w * np + j);
+      ld8(v.blk + j, a.blk + (size_t)w * np + j);
+    }
   if (tid < nt) ld8(v.ho + tid, pop.h + (size_t)w * nt + tid);
   const double wold = o[L.wold];
   if (!kGmat) cp_async_wait_all();
@@ -430,9 +467,16 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
   const uint32_t step = a.step0 + (a.ctr ? a.ctr[0] : 0u);
   long long tph = clock64();
   double sn = 1.0;
-  status |= eval_det<kGmat>(S, m, v.hn, v.pn, &v.sc[0], tph, S.has_bf ? o + L.pair : nullptr,
-                            o + L.rhok, !kGmat && a.orb_inv && L.inv ? o + L.inv : nullptr);
+  status |= eval_det<kGmat, kSeq>(S, m, v.hn, v.pn, &v.sc[0], tph,
+                                  S.has_bf ? o + L.pair : nullptr, o + L.rhok,
+                                  !kGmat && a.orb_inv && L.inv ? o + L.inv : nullptr);
   sn = v.sc[0];
+  if (kSeq) {  // into the orbital buffer, free now, while the reverse move is formed
+    for (int j = tid; j < np; j += kThreads) {
+      cp_async8(v.po + j, pop.p + (size_t)w * np + j);
+      cp_async8(v.blk + j, a.blk + (size_t)w * np + j);
+    }
+  }
   // reverse move (reptation.f:4660-4674)
   double wn = 0.0;
   for (int j = tid; j < N2; j += kThreads) {
@@ -441,6 +485,7 @@ __global__ void __launch_bounds__(kThreads, 2) move_kernel(const DevSys *sp, Dev
     double chi = v.xo[j] - m.x[j] - (-var * m.g[j]);
     wn -= chi * chi * vari;
   }
+  if (kSeq) cp_async_wait_all();  // block_sum's barriers publish the copies
   double wnew = block_sum(wn, m.red);
   double p;
   if (age == a.mage) {
@@ -840,8 +885,10 @@ cudaError_t launch_orb_inv(const DevSys &hs, const DevSys *ds, const MoveArgs &a
 cudaError_t launch_move(const DevSys &hs, const DevSys *ds, DevPop pop, const MoveArgs &a,
                         cudaStream_t st) {
   if (a.nw <= 0) return cudaSuccess;
-  size_t sm = move_smem_bytes(hs);
-  auto k = hs.gmat ? move_kernel<true> : move_kernel<false>;
+  const bool seq = !hs.gmat && a.orb_inv && orb_inv_applies(hs) && props_buf_fits(hs);
+  size_t sm = seq ? move_smem_bytes_seq(hs) : move_smem_bytes(hs);
+  auto k = hs.gmat ? move_kernel<true, false>
+                   : (seq ? move_kernel<false, true> : move_kernel<false, false>);
   cudaError_t e = set_smem((const void *)k, sm);
   if (e != cudaSuccess) return e;
   k<<<a.nw, kThreads, sm, st>>>(ds, pop, a);

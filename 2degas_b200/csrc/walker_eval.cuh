@@ -112,10 +112,13 @@ __host__ __device__ inline int xt_ldu(int n2) { return 8 * xt_row_tiles(n2) + 4;
 // determinant matrices (A, W, F0 region) come from gbase instead, the
 // walker's block of global memory, and *gbytes (when given) receives its
 // size. kG fixes s.gmat at compile time in the kernels (0 off, 1 on); the
-// host's sizing reads it (-1).
+// host's sizing reads it (-1). one_buf: a single orbital/inverse/M buffer
+// that the spins take in turn (the move kernel when orb_inv_kernel has
+// formed both spins' orbitals and inverses: m.A[1] = m.A[0]).
 template <int kG = -1>
 __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSmem *m,
-                                             char *gbase = nullptr, size_t *gbytes = nullptr) {
+                                             char *gbase = nullptr, size_t *gbytes = nullptr,
+                                             bool one_buf = false) {
   const bool gm = kG < 0 ? s.gmat != 0 : kG != 0;
   size_t off = 0, goff = 0;
   auto take = [&](size_t bytes) -> char * {
@@ -165,7 +168,7 @@ __host__ __device__ inline size_t eval_carve(const DevSys &s, char *base, EvalSm
 #pragma unroll
     for (int sp = 0; sp < 2; sp++) {
       if (sp >= nsp) continue;
-      t.A[sp] = (double2 *)mtake(awbytes > mbytes ? awbytes : mbytes);
+      t.A[sp] = (one_buf && sp > 0) ? t.A[0] : (double2 *)mtake(awbytes > mbytes ? awbytes : mbytes);
       t.W[sp] = t.A[sp] ? t.A[sp] + n * n : nullptr;
       t.dk[sp] = (double *)take(sizeof(double) * n);
       t.perm[sp] = (int *)take(sizeof(int) * n);
@@ -1549,7 +1552,11 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
 // backflow Jacobian blocks take the pair spline values written by
 // eval_pairs(pout) instead of evaluating them again; with inv_in, the
 // orbitals and their inversion come from orb_inv_kernel.
-template <bool kGmat = false>
+// kSeq (with inv_in, m carved with one_buf): the spins' orbitals and
+// inverses are copied in turn into the one buffer, each just before its
+// spin's F matrix, since the cross-term matrix M of the spin before it
+// overlays the buffer until its last chunk.
+template <bool kGmat = false, bool kSeq = false>
 __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, double *props,
                                double *sign, long long &tph, const double *pin,
                                const double *rhok_in = nullptr,
@@ -1576,7 +1583,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
   if (S.has_bf) {
     const int n = S.nmax;
     bool reg_path = true;  // the phase the log|det| sum below is counted in
-    if (inv_in) {
+    if (kSeq || inv_in) {  // (kSeq has inv_in: the in-kernel inversion is compiled out)
       // orbitals, inverse, |pivot|^2, pivot rows and singular flags of both
       // spins from orb_inv_kernel (the walker's move scratch)
       const double *src = inv_in;
@@ -1587,8 +1594,11 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
         const double *sD = reinterpret_cast<const double *>(sW + (size_t)ns * ld);
         double2 *dA = sp ? m.A[1] : m.A[0], *dW = sp ? m.W[1] : m.W[0];
         // asynchronous 16-byte global-to-shared copies, all in flight at once
-        for (int e = tid; e < ns * ns; e += kThreads) cp_async16(dA + e, sA + e);
-        for (int e = tid; e < ns * ld; e += kThreads) cp_async16(dW + e, sW + e);
+        // (kSeq: the first spin's now, the others' before their F matrix)
+        if (!kSeq || sp == 0) {
+          for (int e = tid; e < ns * ns; e += kThreads) cp_async16(dA + e, sA + e);
+          for (int e = tid; e < ns * ld; e += kThreads) cp_async16(dW + e, sW + e);
+        }
         for (int k = tid; k < ns; k += kThreads) {
           (sp ? m.dk[1] : m.dk[0])[k] = sD[k];
           (sp ? m.perm[1] : m.perm[0])[k] = (int)sD[ns + k];
@@ -1711,9 +1721,77 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
       const int ns = S.np[sp], ld = ws_ld(ns), f0 = S.ipfrst[sp];
       const double2 *A = sp ? m.A[1] : m.A[0], *W = sp ? m.W[1] : m.W[0];
       const int *pm = sp ? m.perm[1] : m.perm[0];
+      if (kSeq && sp > 0) {
+        // this spin's orbitals and inverse into the buffer that the spin
+        // before it has finished with (its last chunk ended on a barrier)
+        const double2 *sA = reinterpret_cast<const double2 *>(inv_in);
+        for (int t = 0; t < sp; t++) sA += inv_spin_doubles(S.np[t]) / 2;
+        const double2 *sW = sA + (size_t)ns * ns;
+        double2 *dA = m.A[sp], *dW = m.W[sp];
+        for (int e = tid; e < ns * ns; e += kThreads) cp_async16(dA + e, sA + e);
+        for (int e = tid; e < ns * ld; e += kThreads) cp_async16(dW + e, sW + e);
+        cp_async_wait_all();
+        __syncthreads();
+      }
       // F_a(l,j) = sum_k Ainv(l,k) (i g_k[a]) A(k,j) (zv, reptation.f:10189-10200)
-      // with Ainv(l, pi(c)) = W(pi(l), c): 2x2 (l,j) tiles per thread.
-      {
+      // with Ainv(l, pi(c)) = W(pi(l), c).
+      if (kSeq) {
+        // On the FP64 tensor cores (mma.m8n8k4, fragments as in the cross
+        // term below): F_a = (W_pi diag(g_a)) (i A_pi), rows of W and of A
+        // taken in pivot order. A warp takes a row tile of 8 l and two
+        // column tiles of 8 j, k-steps of 4 c; its A fragment is
+        // W(pi(l), c) g_a(pi(c)) (zero for c >= ns), its B fragment
+        // i A(pi(c), j), and per column tile eight products form the real
+        // and imaginary parts of F_x and F_y. Rows and columns beyond ns
+        // repeat the last one and are not stored.
+        const int RTf = (ns + 7) >> 3, KTf = (ns + 3) >> 2, CP = (RTf + 1) >> 1;
+        const int warp = tid >> 5, lane = tid & 31, lg = lane >> 2, lt = lane & 3;
+        for (int pt = warp; pt < RTf * CP; pt += kThreads / 32) {
+          const int Lt = pt / CP, J0 = 2 * (pt - Lt * CP);
+          const double2 *wrow = W + pm[min(8 * Lt + lg, ns - 1)] * ld;
+          const double2 *acol0 = A + min(8 * J0 + lg, ns - 1) * ns;
+          const double2 *acol1 = A + min(8 * J0 + 8 + lg, ns - 1) * ns;
+          double acc[2][4][2];  // [column tile][F_x re, F_x im, F_y re, F_y im][column]
+#pragma unroll
+          for (int t = 0; t < 2; t++)
+#pragma unroll
+            for (int u = 0; u < 4; u++) acc[t][u][0] = acc[t][u][1] = 0.0;
+#pragma unroll 2
+          for (int kt = 0; kt < KTf; kt++) {
+            const int c = 4 * kt + lt;
+            const bool cok = c < ns;
+            const int pc = pm[cok ? c : ns - 1];
+            const double2 wv = cok ? wrow[c] : make_double2(0.0, 0.0);
+            const double gx = m.gsh[2 * pc], gy = m.gsh[2 * pc + 1];
+            const double wxr = wv.x * gx, wxi = wv.y * gx, wyr = wv.x * gy, wyi = wv.y * gy;
+#pragma unroll
+            for (int t = 0; t < 2; t++) {
+              const double2 av = (t ? acol1 : acol0)[pc];
+              const double nai = -av.y;  // i A = (-Im A, Re A)
+              dmma_m8n8k4(acc[t][0], wxr, nai);
+              dmma_m8n8k4(acc[t][0], -wxi, av.x);
+              dmma_m8n8k4(acc[t][1], wxr, av.x);
+              dmma_m8n8k4(acc[t][1], wxi, nai);
+              dmma_m8n8k4(acc[t][2], wyr, nai);
+              dmma_m8n8k4(acc[t][2], -wyi, av.x);
+              dmma_m8n8k4(acc[t][3], wyr, av.x);
+              dmma_m8n8k4(acc[t][3], wyi, nai);
+            }
+          }
+          const int l = 8 * Lt + lg;
+#pragma unroll
+          for (int t = 0; t < 2; t++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+              const int j = 8 * (J0 + t) + 2 * lt + e;
+              if (l < ns && j < ns && J0 + t < RTf) {
+                m.F0[l + j * ns] = make_double2(acc[t][0][e], acc[t][1][e]);
+                m.F1[l + j * ns] = make_double2(acc[t][2][e], acc[t][3][e]);
+              }
+            }
+        }
+      } else {
+        // 2x2 (l,j) tiles per thread
         const int nh = (ns + 1) / 2;
         for (int tile = tid; tile < nh * nh; tile += kThreads) {
           const int l0 = 2 * (tile % nh), j0 = 2 * (tile / nh);
