@@ -100,9 +100,9 @@ struct MoveSmem {
   double *xo, *go, *po, *pn, *blk, *ho, *hn, *sc;
 };
 
-// props_in_buf (the one-buffer move kernel): po, pn and blk are placed by
-// the kernel in the orbital buffer, which is free once the determinants
-// are done (props_buf_fits).
+// props_in_buf (the one-buffer move kernel): the new properties pn go to the
+// orbital buffer, which is free once the determinants are done
+// (props_buf_fits); the old ones and the block sums stay in HBM.
 __host__ __device__ inline size_t move_carve(const DevSys &s, char *base, MoveSmem *m,
                                              bool props_in_buf = false) {
   size_t off = 0;
@@ -133,14 +133,14 @@ size_t move_smem_bytes(const DevSys &s) {
 
 // The one-buffer move kernel (move_kernel<false, true>): both spins'
 // orbitals and inverses come from orb_inv_kernel and take one shared
-// buffer in turn, and the walker's old, new and accumulated properties use
-// that buffer after the determinants, so three CTAs fit an SM.
-__host__ __device__ inline size_t props_stride(const DevSys &s) { return (s.nprops + 1) & ~1; }
+// buffer in turn, the new properties use that buffer after the
+// determinants, and the old properties and block sums are read from HBM at
+// the write-back, so three CTAs fit an SM.
 inline bool props_buf_fits(const DevSys &s) {
   const int n = s.nmax > 0 ? s.nmax : 1;
   const size_t awbytes = sizeof(double2) * (n * n + n * ws_ld(n));
   const size_t mbytes = sizeof(double) * 2 * n * xt_ldm(2 * n);
-  return sizeof(double) * 3 * props_stride(s) <= std::max(awbytes, mbytes);
+  return sizeof(double) * (size_t)s.nprops <= std::max(awbytes, mbytes);
 }
 size_t move_smem_bytes_seq(const DevSys &s) {
   return eval_carve(s, nullptr, nullptr, nullptr, nullptr, true) +
@@ -386,11 +386,7 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
                                  nullptr, kSeq);
   MoveSmem v;
   move_carve(S, smem + off, &v, kSeq);
-  if (kSeq) {
-    v.pn = reinterpret_cast<double *>(m.A[0]);
-    v.po = v.pn + props_stride(S);
-    v.blk = v.po + props_stride(S);
-  }
+  if (kSeq) v.pn = reinterpret_cast<double *>(m.A[0]);  // po and blk stay in HBM
   const int w = blockIdx.x, tid = threadIdx.x;
   if (w >= a.nw) return;
   const int N = S.N, N2 = 2 * N, np = S.nprops, nt = S.nt;
@@ -417,7 +413,7 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
     prefetch_l2(o + L.inv, nd);
   }
   if (S.has_bf && !S.bf_zero) prefetch_l2(o + L.pair, 3 * (size_t)N * N);
-  if (kSeq) {  // read after the determinants (from a 16-byte boundary)
+  if (kSeq) {  // read at the write-back (from a 16-byte boundary)
     const size_t e0 = (size_t)w * np, e1 = (e0 + 1) & ~size_t(1);
     prefetch_l2(pop.p + e1, np - (e1 - e0));
     prefetch_l2(a.blk + e1, np - (e1 - e0));
@@ -456,6 +452,9 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
     }
   if (tid < nt) ld8(v.ho + tid, pop.h + (size_t)w * nt + tid);
   const double wold = o[L.wold];
+  // kSeq: of the old properties only these two before the write-back
+  const double po_ltf = kSeq ? pop.p[(size_t)w * np + QMC2D_JLTF] : 0.0;
+  const double po_et = kSeq ? pop.p[(size_t)w * np + QMC2D_JETOT] : 0.0;
   if (!kGmat) cp_async_wait_all();
   __syncthreads();
   double so = pop.s[w];
@@ -471,12 +470,6 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
                                   S.has_bf ? o + L.pair : nullptr, o + L.rhok,
                                   !kGmat && a.orb_inv && L.inv ? o + L.inv : nullptr);
   sn = v.sc[0];
-  if (kSeq) {  // into the orbital buffer, free now, while the reverse move is formed
-    for (int j = tid; j < np; j += kThreads) {
-      cp_async8(v.po + j, pop.p + (size_t)w * np + j);
-      cp_async8(v.blk + j, a.blk + (size_t)w * np + j);
-    }
-  }
   // reverse move (reptation.f:4660-4674)
   double wn = 0.0;
   for (int j = tid; j < N2; j += kThreads) {
@@ -485,14 +478,13 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
     double chi = v.xo[j] - m.x[j] - (-var * m.g[j]);
     wn -= chi * chi * vari;
   }
-  if (kSeq) cp_async_wait_all();  // block_sum's barriers publish the copies
   double wnew = block_sum(wn, m.red);
   double p;
   if (age == a.mage) {
     p = 1.0;
     nforced += 1.0;
   } else {
-    p = (v.po[QMC2D_JLTF] - v.pn[QMC2D_JLTF]) * 2.0 + 0.5 * (wnew - wold);
+    p = ((kSeq ? po_ltf : v.po[QMC2D_JLTF]) - v.pn[QMC2D_JLTF]) * 2.0 + 0.5 * (wnew - wold);
     p = fmin(0.0, fmax(-50.0, p));
     p = exp(p);
   }
@@ -500,14 +492,16 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
   double xr = 1.0;
   if (p < 1.0) xr = uniform2(a.seed, 0xFFFFFFFEu, (uint32_t)w, step, 0u).x;
   bool acc = p >= xr;
-  double elocal = acc ? 0.5 * (v.pn[QMC2D_JETOT] + v.po[QMC2D_JETOT]) : v.po[QMC2D_JETOT];
+  const double et_old = kSeq ? po_et : v.po[QMC2D_JETOT];
+  double elocal = acc ? 0.5 * (v.pn[QMC2D_JETOT] + et_old) : et_old;
   __syncthreads();
   if (acc) {
     for (int j = tid; j < N2; j += kThreads) {
       v.xo[j] = m.x[j];
       v.go[j] = m.g[j];
     }
-    for (int j = tid; j < np; j += kThreads) v.po[j] = v.pn[j];
+    if (!kSeq)
+      for (int j = tid; j < np; j += kThreads) v.po[j] = v.pn[j];
     if (tid < nt) v.ho[tid] = v.hn[tid];
     so = sn;
     age = 0.0;
@@ -516,7 +510,7 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
     age += 1.0;
   }
   __syncthreads();
-  if (tid == 0) v.po[QMC2D_JACC] = p;
+  if (tid == 0 && !kSeq) v.po[QMC2D_JACC] = p;
   double wgt = 1.0;
   if (a.dmc) {
     // dmc weight (reptation.f:898-903), multiplied over the generation's moves;
@@ -530,7 +524,8 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
     wgt = wate;
   }
   __syncthreads();
-  for (int j = tid; j < np; j += kThreads) v.blk[j] += v.po[j] * wgt;
+  if (!kSeq)
+    for (int j = tid; j < np; j += kThreads) v.blk[j] += v.po[j] * wgt;
   norm += wgt;
   phase_mark(S, PH_ACCEPT, tph);
   __syncthreads();
@@ -538,9 +533,23 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
     pop.x[(size_t)w * N2 + j] = v.xo[j];
     pop.g[(size_t)w * N2 + j] = v.go[j];
   }
-  for (int j = tid; j < np; j += kThreads) {
-    pop.p[(size_t)w * np + j] = v.po[j];
-    a.blk[(size_t)w * np + j] = v.blk[j];
+  if (kSeq) {
+    // the walker's properties: the new ones if accepted, else the old ones
+    // in HBM, with the acceptance probability; the block sums in HBM
+    for (int j = tid; j < np; j += kThreads) {
+      const size_t i = (size_t)w * np + j;
+      double val = acc ? v.pn[j] : pop.p[i];
+      if (j == QMC2D_JACC) val = p;
+      double b = a.blk[i];
+      b += val * wgt;
+      a.blk[i] = b;
+      if (acc || j == QMC2D_JACC) pop.p[i] = val;
+    }
+  } else {
+    for (int j = tid; j < np; j += kThreads) {
+      pop.p[(size_t)w * np + j] = v.po[j];
+      a.blk[(size_t)w * np + j] = v.blk[j];
+    }
   }
   if (tid < nt) pop.h[(size_t)w * nt + tid] = v.ho[tid];
   if (tid == 0) {

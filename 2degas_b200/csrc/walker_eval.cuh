@@ -1735,7 +1735,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
       }
       // F_a(l,j) = sum_k Ainv(l,k) (i g_k[a]) A(k,j) (zv, reptation.f:10189-10200)
       // with Ainv(l, pi(c)) = W(pi(l), c).
-      if (kSeq) {
+      if (!kGmat) {
         // On the FP64 tensor cores (mma.m8n8k4, fragments as in the cross
         // term below): F_a = (W_pi diag(g_a)) (i A_pi), rows of W and of A
         // taken in pivot order. A warp takes a row tile of 8 l and two
@@ -1791,7 +1791,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
             }
         }
       } else {
-        // 2x2 (l,j) tiles per thread
+        // determinants in HBM: 2x2 (l,j) tiles per thread
         const int nh = (ns + 1) / 2;
         for (int tile = tid; tile < nh * nh; tile += kThreads) {
           const int l0 = 2 * (tile % nh), j0 = 2 * (tile / nh);
