@@ -494,7 +494,10 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
   bool acc = p >= xr;
   const double et_old = kSeq ? po_et : v.po[QMC2D_JETOT];
   double elocal = acc ? 0.5 * (v.pn[QMC2D_JETOT] + et_old) : et_old;
-  __syncthreads();
+  // the old properties read above before the copy below overwrites them;
+  // kSeq reads them from registers, and block_sum's last barrier already
+  // follows every read of xo and go
+  if (!kSeq) __syncthreads();
   if (acc) {
     for (int j = tid; j < N2; j += kThreads) {
       v.xo[j] = m.x[j];
@@ -509,7 +512,7 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
   } else {
     age += 1.0;
   }
-  __syncthreads();
+  if (!kSeq) __syncthreads();  // po's copy before its acceptance entry
   if (tid == 0 && !kSeq) v.po[QMC2D_JACC] = p;
   double wgt = 1.0;
   if (a.dmc) {
@@ -523,9 +526,10 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
     wate *= peso;
     wgt = wate;
   }
-  __syncthreads();
-  if (!kSeq)
+  if (!kSeq) {
+    __syncthreads();  // the acceptance entry before the sums
     for (int j = tid; j < np; j += kThreads) v.blk[j] += v.po[j] * wgt;
+  }
   norm += wgt;
   phase_mark(S, PH_ACCEPT, tph);
   __syncthreads();
