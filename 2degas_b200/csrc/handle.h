@@ -60,13 +60,14 @@ struct qmc2d_handle {
 };
 
 // Spin matrices per SM below which a move inverts inside the move kernel
-// instead of in orb_inv_kernel (qmc2d_set_move_inversion mode 1).
-// Measured crossovers (1024 to 4096 walkers at N = 26, 42, 58 and 25
-// polarised): two spins of more than 16 orbitals gain from about 24
-// matrices per SM, smaller ones (the 16-column kernel, 124 registers) from
-// about 12; a single spin, whose in-kernel inversion spreads one matrix over
-// every warp of the CTA, from about 6.
-constexpr int kOrbInvMinPerSM = 24, kOrbInvMinPerSMSmall = 12, kOrbInvMinPerSMOneSpin = 6;
+// instead of in orb_inv_kernel (qmc2d_set_move_inversion mode 1). With the
+// batched form the move runs in the one-buffer move kernel (three CTAs per
+// SM). Measured crossovers (DMC, 512 to 2048 walkers): two spins of 29
+// orbitals lose 3% at 7 matrices per SM and gain 6% at 14, two of 13
+// orbitals break even at 7 and gain 13% at 14; a single spin of 25
+// orbitals, whose in-kernel inversion spreads one matrix over every warp
+// of the CTA, gains 4% at 3.5 and 21% at 7.
+constexpr int kOrbInvMinPerSM = 10, kOrbInvMinPerSMSmall = 10, kOrbInvMinPerSMOneSpin = 3;
 
 // Whether this handle's next move batches its orbitals and inversion.
 inline bool move_orb_inv(const qmc2d_handle *h) {

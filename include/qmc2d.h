@@ -250,8 +250,8 @@ int qmc2d_get_pair_lanes(qmc2d_handle *h, int *lanes);
  * pair kernel and the move kernel, one warp per spin matrix, for spins of
  * at most 32 orbitals held in shared memory; otherwise the move kernel
  * inverts with the inversion layout in force. mode 1 (the default): batched
- * when the population gives at least 24 spin matrices per SM (12 for spins
- * of at most 16 orbitals, 6 for a single spin): a fuller GPU hides the
+ * when the population gives at least 10 spin matrices per SM (3 for a
+ * single spin): a fuller GPU hides the
  * pivot chains, small populations finish sooner inside the move kernel;
  * 2: batched whenever it fits; 0: never. Both pivot as zgefa does
  * and agree to round-off. get reports whether the next move is batched. The
