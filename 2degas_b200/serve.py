@@ -8,7 +8,10 @@ as a qmc2d_system) and then waits until its device footprint
 (`qmc2d_footprint`: walker records, move scratch, tables) fits the free
 share of the HBM budget and a slot is free. Admission is first-fit in
 arrival order: a request that does not fit yet does not hold back later,
-smaller ones.
+smaller ones. Requests whose determinants live in HBM (more than
+HBM_DETS_ABOVE orbitals in a spin) each fill the GPU and are bound by L2
+latency; max_hbm_dets caps how many of them run at once, so that they do
+not evict each other's matrices from L2, while smaller requests fill in.
 
 An admitted request gets its own handle, hence its own CUDA stream, and its
 own host thread. The library's calls release the interpreter lock, so the
@@ -197,17 +200,33 @@ def run_request(p, device=0):
     return dict(energy=mean, error=err, blocks=nb, moves=moves, status=status, block_means=means)
 
 
+# Orbitals per spin above which the library keeps a walker's determinant
+# matrices in HBM instead of shared memory (45 + 45 is the largest shell in
+# shared memory).
+HBM_DETS_ABOVE = 45
+
+
+def hbm_dets(req):
+    return max(req.n_up, req.n_down) > HBM_DETS_ABOVE
+
+
 class Server:
     """Admits requests by HBM footprint and runs the admitted ones together.
 
     hbm_bytes: the device memory the server may hand out; max_slots: the
-    most requests on the device at once. prepare(req, workdir) -> Prepared
+    most requests on the device at once; max_hbm_dets: the most of them with
+    determinants in HBM (None: no cap; 1 by default: on a stream of 12
+    requests from N = 50 to 149 two or more at once lengthened the makespan
+    from 102 to 109-119 s and the median latency from 40 to 63-66 s). prepare(req, workdir) -> Prepared
     and run(prepared, device) -> dict are the host preparation and the
     device run (prepare_request and run_request unless replaced)."""
 
-    def __init__(self, hbm_bytes, max_slots=32, device=0, workdir=None, prepare=None, run=None):
+    def __init__(self, hbm_bytes, max_slots=32, device=0, workdir=None, prepare=None, run=None,
+                 max_hbm_dets=1):
         self.hbm = int(hbm_bytes)
         self.max_slots = max_slots
+        self.max_hbm_dets = max_hbm_dets
+        self.active_hbm_dets = 0
         self.device = device
         self.workdir = workdir or tempfile.mkdtemp(prefix="qmc2d_serve_")
         self.prepare = prepare or prepare_request
@@ -283,6 +302,7 @@ class Server:
             with self.cv:
                 self.used -= p.footprint
                 self.active -= 1
+                self.active_hbm_dets -= int(hbm_dets(r))
                 results[r.rid] = res
                 self.cv.notify_all()
 
@@ -294,10 +314,15 @@ class Server:
                 while admitted:
                     admitted = False
                     for p in sorted(pending, key=lambda p: p.t_arrival):  # first fit
+                        big = hbm_dets(p.req)
+                        if big and self.max_hbm_dets is not None and \
+                                self.active_hbm_dets >= self.max_hbm_dets:
+                            continue
                         if self.active < self.max_slots and self.used + p.footprint <= self.hbm:
                             pending.remove(p)
                             self.used += p.footprint
                             self.active += 1
+                            self.active_hbm_dets += int(big)
                             self.peak_used = max(self.peak_used, self.used)
                             self.peak_active = max(self.peak_active, self.active)
                             th = threading.Thread(target=work, args=(p,), daemon=True)

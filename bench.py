@@ -1004,7 +1004,8 @@ def serve_arm(args, rank, world):
                                           **kw)
     free, total = torch.cuda.mem_get_info()
     budget = int(0.8 * free)
-    srv = serve.Server(budget, max_slots=args.serve_slots)
+    srv = serve.Server(budget, max_slots=args.serve_slots,
+                       max_hbm_dets=args.serve_hbm_dets if args.serve_hbm_dets > 0 else None)
     with Clocks(0) as clk:
         res = srv.serve(stream())
     sm = serve.summary(res)
@@ -1033,6 +1034,7 @@ def serve_arm(args, rank, world):
                    "rs": [1.0, 40.0], "walkers": [512, 4096], "target_ry_per_el": 1e-4,
                    "block_steps": 20, "max_blocks": args.serve_blocks,
                    "hbm_budget_bytes": budget, "slots": args.serve_slots,
+                   "hbm_dets_at_once": args.serve_hbm_dets if args.serve_hbm_dets > 0 else None,
                    "precision": args.precision},
         "serving": {**sm, "peak_active": srv.peak_active, "peak_hbm_bytes": srv.peak_used,
                     "per_request": [dict(rid=r.rid, N=0, status=r.status, latency_s=r.latency,
@@ -1191,6 +1193,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-blocks", type=int, default=100)
     ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--serve-hbm-dets", type=int, default=1,
+                    help="requests with determinants in HBM at once (0: no cap)")
     ap.add_argument("--phases", action="store_true",
                     help="print SM cycles per walker-move of each move-kernel phase instead")
     args = ap.parse_args()

@@ -89,6 +89,35 @@ def test_slots_bound_concurrency():
     assert srv.peak_active == 2 and max(live for _, live, _ in log["concurrent"]) == 2
 
 
+def test_hbm_determinant_requests_capped_while_small_ones_fill_in():
+    prepare, run, log = _fake([1] * 6, dur=0.1)
+    # 0, 2, 4: 81 orbitals per spin (determinants in HBM); 1, 3, 5: 13
+    reqs = [serve.Request(81 if i % 2 == 0 else 13, 81 if i % 2 == 0 else 13, 1.0, rid=i)
+            for i in range(6)]
+    assert [serve.hbm_dets(r) for r in reqs] == [True, False] * 3
+    srv = serve.Server(hbm_bytes=100, max_slots=4, prepare=prepare, run=run, max_hbm_dets=1)
+    live_big = {"n": 0, "max": 0}
+    lock = threading.Lock()
+
+    def run_big(p, device):
+        big = serve.hbm_dets(p.req)
+        with lock:
+            live_big["n"] += big
+            live_big["max"] = max(live_big["max"], live_big["n"])
+        try:
+            return run(p, device)
+        finally:
+            with lock:
+                live_big["n"] -= big
+
+    srv.run_one = run_big
+    res = srv.serve(reqs, realtime=False)
+    assert all(r.status == "done" for r in res)
+    assert live_big["max"] == 1
+    # the small requests ran beside the first large one
+    assert max(live for _, live, _ in log["concurrent"]) >= 2
+
+
 def test_a_failed_run_ends_only_its_request():
     prepare, run, _ = _fake([1, 1, 1])
 
