@@ -49,13 +49,14 @@ METRIC = "walker-moves/sec (DMC with backflow, N=58 r_s=5, 4096 walkers)"
 UNIT = "walker-moves/s"
 # DRAM bytes read per walker by one pairs_kernel + orb_inv_kernel +
 # move_kernel generation, from the ncu capture summarised in
-# profiles/move_kernels_dmc_bf_n58_296w.md (296 walkers, scaled linearly: the
-# walker records and the move scratch, read cold in ncu's replays), plus the
-# move scratch block the pair and orbital kernels write, which reaches DRAM at
-# 4096 walkers (the blocks exceed L2) though not in the 296-walker capture.
-MOVE_DRAM_READ_PER_WALKER = (1.010176e6 + 0.476416e6 + 44.548096e6) / 296
+# profiles/move_kernels_dmc_bf_n58_444w.md (444 walkers, one wave of the
+# move kernel; scaled linearly: the walker records and the move scratch,
+# read cold in ncu's replays), plus the move scratch block the pair and
+# orbital kernels write, which reaches DRAM at 4096 walkers (the blocks
+# exceed L2) though not in the 444-walker capture.
+MOVE_DRAM_READ_PER_WALKER = (1.879296e6 + 0.526080e6 + 71.073536e6) / 444
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum of pairs_kernel + orb_inv_kernel + move_kernel "
-                  "(296 walkers) x walkers/296, + the move scratch written per walker")
+                  "(444 walkers) x walkers/444, + the move scratch written per walker")
 
 
 def move_scratch_bytes(N, nk, ns=()):
