@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(kThreads, kSeq ? 3 : 2) move_kernel(const DevS
     for (int t = 0; t < nt; t++) nd += inv_spin_doubles(S.np[t]);
     prefetch_l2(o + L.inv, nd);
   }
-  if (S.has_bf && !S.bf_zero) prefetch_l2(o + L.pair, 3 * (size_t)N * N);
+  if (S.has_bf && !S.bf_zero) prefetch_l2(o + L.pair, 3 * pair_count(N));
   if (kSeq) {  // read at the write-back (from a 16-byte boundary)
     const size_t e0 = (size_t)w * np, e1 = (e0 + 1) & ~size_t(1);
     prefetch_l2(pop.p + e1, np - (e1 - e0));

@@ -640,7 +640,7 @@ __global__ void __launch_bounds__(kThreads, 2) rmc_det_kernel(const DevSys *sp, 
   const bool pairs_stored = S.has_bf && !S.bf_zero;
   if (pairs_stored) {
     // bring the stored pair values back into L2 before the Jacobian build
-    const size_t bytes = (sizeof(double) * 3 * (size_t)N * N) & ~size_t(15);
+    const size_t bytes = (sizeof(double) * 3 * pair_count(N)) & ~size_t(15);
     const char *base = reinterpret_cast<const char *>(o + L.pair);
     for (size_t b0 = (size_t)tid * 32768; b0 < bytes; b0 += (size_t)kThreads * 32768) {
       const unsigned sz = (unsigned)(bytes - b0 < 32768 ? bytes - b0 : 32768);

@@ -255,10 +255,17 @@ __host__ __device__ inline size_t pair_carve(const DevSys &s, char *base, EvalSm
 // kernel and read by the move kernel of the same step: the proposed
 // configuration, the pair passes' per-particle sums, the proposal's log
 // density, rho_k (both slots), and (backflow) the spline values of every
-// ordered pair (i, j):
-// eta(r_ij), eta'(r_ij)/r_ij and 3 eta'/r + eta'' at [k N^2 + i N + j].
+// pair i < j:
+// eta(r_ij), eta'(r_ij)/r_ij and 3 eta'/r + eta'' at [k P + pair_tri(N, i, j)],
+// P = N (N - 1) / 2 (the values are functions of r_ij alone, computed from
+// the same bits for (i, j) and (j, i), so one triangle serves both orders).
 // A reptile's bead growth also keeps its proposal's drift term (dold) and
 // the free-propagator sum (lng) of get_w_stack (reptation.f:1804-1851).
+__host__ __device__ inline size_t pair_count(int N) { return (size_t)N * (N - 1) / 2; }
+// Row-major upper triangle without the diagonal: (a, b), a < b.
+__host__ __device__ inline size_t pair_tri(int N, int a, int b) {
+  return (size_t)a * (2 * N - a - 1) / 2 + (size_t)(b - a - 1);
+}
 struct MoveScratch {
   int x, g, q, sb, qbd, lap, ltf, vp, wold, dold, lng, rhok, pair;
   size_t inv;  // orb_inv_kernel's output per spin (0: no such region)
@@ -296,7 +303,7 @@ __host__ __device__ inline MoveScratch move_scratch(const DevSys &s, bool with_i
   l.lng = 14 * N + 2;
   l.rhok = 14 * N + 3;
   l.pair = (14 * N + 3 + 4 * (s.nk > 0 ? s.nk : 1) + 3) & ~3;
-  size_t end = (size_t)l.pair + (s.has_bf ? 3 * (size_t)N * N : 0);
+  size_t end = (size_t)l.pair + (s.has_bf ? 3 * pair_count(N) : 0);
   l.inv = 0;
   if (with_inv && orb_inv_fits(s)) {
     end = (end + 1) & ~size_t(1);
@@ -1331,7 +1338,7 @@ __device__ inline void pair_rhok(const DevSys &S, const EvalSmem &m, int t, int 
 //
 // Pair passes A and B: writes m.{ltf, g, lap, vp, G3, S3, q, Sb, qbd} and
 // zeroes m.{gd, lapd, ph2, ph2d}. With pout (backflow), also the backflow
-// spline values of every ordered pair, laid out as in MoveScratch.
+// spline values of every pair i < j, laid out as in MoveScratch.
 // NT threads (a multiple of 32) run the passes; the pair rows (layout
 // RowLayout<R>) are read at `rows`, from shared memory when kSh.
 // R is the precision of the u2 and v2 terms: double, or float with the pair
@@ -1351,7 +1358,7 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
   const int N = S.N;
   const int lane8 = tid & (LG - 1);
   const int per_round = NT / LG;
-  const size_t NN = (size_t)N * N;
+  const size_t NP = pair_count(N);
   constexpr int RS = kSh ? Lay::sstride : Lay::gstride;
   constexpr bool kF64 = sizeof(R) == 8;
   const Knots<R> K(S);
@@ -1432,11 +1439,11 @@ __device__ inline void eval_pairs(const DevSys &S, const EvalSmem &m, long long 
           double w2 = dt * byrd * 3.0 + ddt;
           qbx.add(w2 * rxd);
           qby.add(w2 * ryd);
-          if (pout) {
-            const size_t e = (size_t)i * N + j;
+          if (pout && i < j) {
+            const size_t e = pair_tri(N, i, j);
             pout[e] = t;
-            pout[NN + e] = c;
-            pout[2 * NN + e] = w2;
+            pout[NP + e] = c;
+            pout[2 * NP + e] = w2;
           }
         }
         if (S.has_v2)
@@ -1575,7 +1582,7 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
   };
   const int N = S.N, nt = S.nt;
   const int lane8 = tid & (kGroup - 1);
-  const size_t NN = (size_t)N * N;
+  const size_t NP = pair_count(N);
 
   // ---- backflow Slater determinants (slater_excitations, reptation.f:9967)
   int status = ST_OK;
@@ -1943,10 +1950,10 @@ __device__ inline int eval_det(const DevSys &S, const EvalSmem &m, double *hl, d
               const int jl = jb + l16 + 16 * u, j = f0 + jl;
               pv[u][0] = pv[u][1] = pv[u][2] = 0.0;
               if (pin && valid && jl < ns && j != i) {
-                const size_t e = (size_t)i * N + j;
+                const size_t e = i < j ? pair_tri(N, i, j) : pair_tri(N, j, i);
                 pv[u][0] = __ldg(pin + e);
-                pv[u][1] = __ldg(pin + NN + e);
-                pv[u][2] = __ldg(pin + 2 * NN + e);
+                pv[u][1] = __ldg(pin + NP + e);
+                pv[u][2] = __ldg(pin + 2 * NP + e);
               }
             }
 #pragma unroll

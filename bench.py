@@ -64,7 +64,7 @@ def move_scratch_bytes(N, nk, ns=()):
     ns, the spins' orbital counts, the orbitals-and-inversion region when
     every spin has at most 32 orbitals)."""
     pair = (14 * N + 3 + 4 * max(nk, 1) + 3) & ~3
-    end = pair + 3 * N * N
+    end = pair + 3 * (N * (N - 1) // 2)
     if ns and max(ns) <= 32:
         end = (end + 1) & ~1
         end += sum((2 * n * n + 2 * n * (n | 1) + 2 * n + 2 + 1) & ~1 for n in ns)

@@ -26,13 +26,14 @@ def test_footprint_is_linear_in_walkers_and_counts_every_record(q, n26):
     lib = s.lib
     recs = 2 * (4 * N + nt + np_ + 2) * 8 + (np_ + 1 + 4 + 1) * 8 + 4 + 2 * 8 + 4 * 4 \
         + (4 * N + nt + np_ + 1) * 8 + 8  # + the single-electron sweeps' drift record
-    # the move scratch: per-particle sums, rho_k, (backflow) 3 N^2 pair
-    # values and, for spins of at most 32 orbitals, each spin's orbitals,
-    # inverse, pivots and singular flag (A n^2 and W n (n|1) complex, 2n + 1
-    # doubles, rounded up to even), rounded up to 256 bytes
+    # the move scratch: per-particle sums, rho_k, (backflow) the pair values
+    # of the N (N - 1) / 2 pairs i < j and, for spins of at most 32 orbitals,
+    # each spin's orbitals, inverse, pivots and singular flag (A n^2 and W
+    # n (n|1) complex, 2n + 1 doubles, rounded up to even), rounded up to
+    # 256 bytes
     nk = s.s.nk
     pair = (14 * N + 3 + 4 * max(nk, 1) + 3) & ~3
-    end = pair + 3 * N * N
+    end = pair + 3 * (N * (N - 1) // 2)
     ns = [s.s.np[t] for t in range(nt)]
     if max(ns) <= 32:
         end = (end + 1) & ~1
