@@ -54,7 +54,7 @@ UNIT = "walker-moves/s"
 # read cold in ncu's replays), plus the move scratch block the pair and
 # orbital kernels write, which reaches DRAM at 4096 walkers (the blocks
 # exceed L2) though not in the 444-walker capture.
-MOVE_DRAM_READ_PER_WALKER = (1.879296e6 + 0.526080e6 + 71.073536e6) / 444
+MOVE_DRAM_READ_PER_WALKER = (1.114624e6 + 0.526080e6 + 49.427200e6) / 444
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum of pairs_kernel + orb_inv_kernel + move_kernel "
                   "(444 walkers) x walkers/444, + the move scratch written per walker")
 
