@@ -631,8 +631,8 @@ def config_cpu_baseline(kind, d, cfg, seconds):
 
 
 def config_arm(args, rank, world, local_rank):
-    """BASELINE's configuration 0 (--workload vmc: plain VMC, N = 26 r_s = 1,
-    256 walkers, Gaussian step 0.3 r_s) or 2 (--workload rmc: reptation,
+    """The plain-VMC workload (--workload vmc: N = 26 r_s = 1,
+    256 walkers, Gaussian step 0.3 r_s) or the reptation one (--workload rmc: reptation,
     N = 58 r_s = 10 with u2 + u3 + backflow, 512 reptiles of 200 beads,
     one-bead head moves, tau = 0.01 r_s^2; --rmc-n 26 for the N = 26 deck).
     One step = one VMC step of every walker, or one reptation move of every
